@@ -1,0 +1,435 @@
+"""accel-plus_b200 — Python binding of the B200 tracking engine's C-ABI (include/accel_gpu.h).
+
+The engine itself is libaccelgpu.so (CUDA for sm_100a plus its C++ host layer, built in-tree by
+the Makefile beside this file).  This module is a thin ctypes layer over it, used by the test
+suite and the benchmark; it never computes a tracking result itself, and every call fails
+loudly (AccelError) when the library or a CUDA device is missing.
+
+The directory name carries a hyphen, so import it with importlib:
+
+    accel = importlib.import_module("accel-plus_b200")
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Iterable, Sequence
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libaccelgpu.so")
+
+# ---- constants (mirror include/accel_gpu.h) -------------------------------------------------
+OK, E_INVALID, E_UNSUPPORTED, E_CUDA, E_NOMEM, E_IO, E_TIMEOUT, E_NODEVICE, E_TOO_LARGE = (
+    0, -1, -2, -3, -4, -5, -6, -7, -8)
+DRIFT, QUAD, CORRECTOR, APERTURE, MONITOR, BEND, BENDMPOLE, STRMPOLE, CAVITY = range(1, 10)
+WIGTABLE, IDEALWIG, CRABCAV, RFMULT, TRANSWAKE, MATRIX, SYNCRAD, LONGWAKE = range(10, 18)
+TYPE_NAMES = {DRIFT: "Drift", QUAD: "Quad", CORRECTOR: "Corrector", APERTURE: "Aperture",
+              MONITOR: "Monitor", BEND: "Bend", BENDMPOLE: "BendMPole", STRMPOLE: "StrMPole",
+              CAVITY: "Cavity", WIGTABLE: "WigTable", IDEALWIG: "IdealWig", CRABCAV: "CrabCav",
+              RFMULT: "RFMult", TRANSWAKE: "TransWake", MATRIX: "Matrix", SYNCRAD: "SyncRad",
+              LONGWAKE: "LongWake"}
+MAX_MPOLE = 10
+RAD_OFF, RAD_RAD, RAD_RADQE, RAD_LUMP, RAD_LUMP_DAMP, RAD_LUMP_QE = range(6)
+(F_LENGTH, F_K, F_POLYNOMB, F_POLYNOMA, F_NSLICE, F_MAXNPOLE, F_ANGLE, F_E1, F_E2, F_VOLTAGE,
+ F_FREQUENCY, F_PHIS, F_ENERGY, F_KICKX, F_KICKY, F_XLIM, F_YLIM) = range(1, 18)
+MODE_FUSED, MODE_PLAIN = 0, 1
+LAYOUT_AOS, LAYOUT_SOA = 0, 1
+
+
+class ElemDesc(C.Structure):
+    """accel_elem_desc: one lattice element (field meanings per type in accel_gpu.h)."""
+    _fields_ = [("type", C.c_int32), ("nslice", C.c_int32), ("max_npole", C.c_int32),
+                ("flags", C.c_int32), ("len", C.c_double), ("f", C.c_double * 12),
+                ("poly_a", C.c_double * MAX_MPOLE), ("poly_b", C.c_double * MAX_MPOLE),
+                ("mat", C.c_double * 36), ("famname", C.c_char * 48)]
+
+    @property
+    def name(self) -> str:
+        return self.famname.decode()
+
+    @property
+    def type_name(self) -> str:
+        return TYPE_NAMES.get(self.type, "undefined")
+
+    def copy(self) -> "ElemDesc":
+        d = ElemDesc()
+        C.memmove(C.byref(d), C.byref(self), C.sizeof(ElemDesc))
+        return d
+
+
+class AccelError(RuntimeError):
+    def __init__(self, status: int, where: str, detail: str):
+        super().__init__(f"{where}: status {status} ({detail})")
+        self.status = status
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load libaccelgpu.so; raises if it was not built (there is no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise AccelError(E_UNSUPPORTED, "load", f"{LIB_PATH} is missing: run __graft_entry__.build()")
+    L = C.CDLL(LIB_PATH)
+    P, I, D = C.c_void_p, C.c_int, C.c_double
+    pd = C.POINTER(ElemDesc)
+    sig = {
+        "accel_status_string": (C.c_char_p, [I]),
+        "accel_last_error": (C.c_char_p, []),
+        "accel_version": (I, []),
+        "accel_device_count": (I, [C.POINTER(I)]),
+        "accel_ctx_create": (I, [I, C.POINTER(P)]),
+        "accel_ctx_destroy": (I, [P]),
+        "accel_lattice_read": (I, [C.c_char_p, C.POINTER(pd), C.POINTER(I)]),
+        "accel_lattice_parse": (I, [C.c_char_p, C.POINTER(pd), C.POINTER(I)]),
+        "accel_lattice_write": (I, [C.c_char_p, pd, I, I]),
+        "accel_lattice_free": (None, [pd]),
+        "accel_elem_default": (I, [I, pd]),
+        "accel_line_create": (I, [P, pd, I, C.POINTER(P)]),
+        "accel_line_destroy": (I, [P]),
+        "accel_line_count": (I, [P, C.POINTER(I)]),
+        "accel_line_get_desc": (I, [P, I, pd]),
+        "accel_line_set_field": (I, [P, I, I, I, C.POINTER(D)]),
+        "accel_line_get_field": (I, [P, I, I, I, C.POINTER(D)]),
+        "accel_line_set_flags": (I, [P, I, I, I]),
+        "accel_line_set_energy": (I, [P, D]),
+        "accel_line_setrfphase": (I, [P, C.POINTER(D)]),
+        "accel_line_set_seed": (I, [P, C.c_uint64]),
+        "accel_track": (I, [P, P, I, I, I, I, I, P, I, P]),
+        "accel_track_batched": (I, [P, I, P, P, C.c_int64, I, P, I, P]),
+        "accel_autotune": (I, [P, I, P, P, C.c_int64, C.POINTER(I)]),
+        "accel_set_tile": (I, [P, I, I, I]),
+        "accel_get_tile": (I, [P, C.POINTER(I)]),
+        "accel_m66": (I, [P, I, I, D, D, I, C.POINTER(D)]),
+        "accel_m66_at": (I, [P, I, I, C.POINTER(D), I, D, C.POINTER(D)]),
+        "accel_adjoint_create": (I, [P, I, I, I, P, P, P, I, C.POINTER(P)]),
+        "accel_adjoint_destroy": (I, [P]),
+        "accel_adjoint_forward": (I, [P, P, P]),
+        "accel_adjoint_backward": (I, [P, P, P, P]),
+        "accel_beam_stat": (I, [P, P, I, I, C.POINTER(D), C.POINTER(D), C.POINTER(D), C.POINTER(I)]),
+        "accel_fp64_peak": (I, [P, C.POINTER(D)]),
+        "accel_launch_count": (I, [P, C.POINTER(C.c_int64)]),
+        "accel_profile_enable": (I, [P, I]),
+        "accel_profile_read": (I, [P, C.POINTER(D), C.POINTER(C.c_int64), C.POINTER(D)]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def exported_symbols() -> list[str]:
+    """Every entry point include/accel_gpu.h declares, in declaration order."""
+    import re
+    hdr = os.path.join(os.path.dirname(_HERE), "include", "accel_gpu.h")
+    with open(hdr) as f:
+        text = f.read()
+    return re.findall(r"^\s*(?:const char\*|int|void)\s+(accel_\w+)\s*\(", text, re.M)
+
+
+def _check(status: int, where: str) -> None:
+    if status != OK:
+        L = lib()
+        detail = (L.accel_last_error() or b"").decode() or L.accel_status_string(status).decode()
+        raise AccelError(status, where, detail)
+
+
+def status_string(s: int) -> str:
+    return lib().accel_status_string(s).decode()
+
+
+# ---- lattice files (host only) ------------------------------------------------------------------
+def _take_desc(p, n) -> list[ElemDesc]:
+    out = [p[i].copy() for i in range(n.value)]
+    lib().accel_lattice_free(p)
+    return out
+
+
+def read_lattice(path: str) -> list[ElemDesc]:
+    """Read an Accel+ lattice file (AccelElement::deserialize format)."""
+    p, n = C.POINTER(ElemDesc)(), C.c_int()
+    _check(lib().accel_lattice_read(path.encode(), C.byref(p), C.byref(n)), "accel_lattice_read")
+    return _take_desc(p, n)
+
+
+def parse_lattice(text: str) -> list[ElemDesc]:
+    p, n = C.POINTER(ElemDesc)(), C.c_int()
+    _check(lib().accel_lattice_parse(text.encode(), C.byref(p), C.byref(n)), "accel_lattice_parse")
+    return _take_desc(p, n)
+
+
+def write_lattice(path: str, elems: Sequence[ElemDesc], precision: int = 17) -> None:
+    arr = (ElemDesc * len(elems))(*elems)
+    _check(lib().accel_lattice_write(path.encode(), arr, len(elems), precision), "accel_lattice_write")
+
+
+def elem(type_: int, famname: str = "undefined", length: float = 0.0, **kw) -> ElemDesc:
+    """Build a descriptor with the reference constructor's defaults, then apply keywords:
+    f=[...], poly_a=[...], poly_b=[...], mat=[...], nslice, max_npole, flags."""
+    d = ElemDesc()
+    _check(lib().accel_elem_default(type_, C.byref(d)), "accel_elem_default")
+    d.famname = famname.encode()
+    d.len = length
+    for k, v in kw.items():
+        if k in ("f", "poly_a", "poly_b", "mat"):
+            arr = getattr(d, k)
+            for i, x in enumerate(v):
+                arr[i] = float(x)
+        else:
+            setattr(d, k, v)
+    if type_ in (BEND, BENDMPOLE) and length != 0:
+        d.f[4] = d.f[0] / length
+    return d
+
+
+def desc_array(elems: Sequence[ElemDesc]):
+    return (ElemDesc * len(elems))(*elems)
+
+
+# ---- device objects ---------------------------------------------------------------------------
+def device_count() -> int:
+    n = C.c_int()
+    _check(lib().accel_device_count(C.byref(n)), "accel_device_count")
+    return n.value
+
+
+class Context:
+    """One CUDA device: streams, scratch buffers, tuned tiles (accel_ctx)."""
+
+    def __init__(self, device: int = 0):
+        self.h = C.c_void_p()
+        _check(lib().accel_ctx_create(device, C.byref(self.h)), "accel_ctx_create")
+
+    def close(self):
+        if self.h:
+            lib().accel_ctx_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_tile(self, block=0, seg_turns=0, variant=-1):
+        _check(lib().accel_set_tile(self.h, block, seg_turns, variant), "accel_set_tile")
+
+    def get_tile(self):
+        t = (C.c_int * 3)()
+        _check(lib().accel_get_tile(self.h, t), "accel_get_tile")
+        return tuple(t)
+
+    def fp64_peak(self) -> float:
+        v = C.c_double()
+        _check(lib().accel_fp64_peak(self.h, C.byref(v)), "accel_fp64_peak")
+        return v.value
+
+    def launch_count(self) -> int:
+        v = C.c_int64()
+        _check(lib().accel_launch_count(self.h, C.byref(v)), "accel_launch_count")
+        return v.value
+
+    def profile(self, on: bool):
+        """Issue tracking launches directly with CUDA events around every tracking kernel."""
+        _check(lib().accel_profile_enable(self.h, int(on)), "accel_profile_enable")
+
+    def profile_read(self):
+        """(summed tracking-kernel ms, their launch count, whole-call ms) of the last call."""
+        f, t, n = C.c_double(), C.c_double(), C.c_int64()
+        _check(lib().accel_profile_read(self.h, C.byref(f), C.byref(n), C.byref(t)), "accel_profile_read")
+        return f.value, n.value, t.value
+
+    def beam_stat(self, r, layout=LAYOUT_AOS, n=None):
+        ptr, n = _ptr_and_n(r, n, layout)
+        mean, sig, cross = (C.c_double * 6)(), (C.c_double * 6)(), (C.c_double * 6)()
+        nl = C.c_int()
+        _check(lib().accel_beam_stat(self.h, ptr, layout, n, mean, sig, cross, C.byref(nl)),
+               "accel_beam_stat")
+        return np.array(mean), np.array(sig), np.array(cross), nl.value
+
+
+def _ptr_and_n(r, n=None, layout=LAYOUT_AOS):
+    """Pointer of a numpy array (host) or a torch tensor / object with data_ptr (device)."""
+    if isinstance(r, np.ndarray):
+        if r.dtype != np.float64 or not r.flags.c_contiguous:
+            raise ValueError("state must be a C-contiguous float64 array")
+        ptr = r.ctypes.data
+        size = r.size
+    elif hasattr(r, "data_ptr"):
+        if not r.is_contiguous():
+            raise ValueError("state tensor must be contiguous")
+        ptr = r.data_ptr()
+        size = r.numel()
+    else:
+        raise TypeError("state must be a numpy array or a tensor")
+    if n is None:
+        if size % 6:
+            raise ValueError("state size is not a multiple of 6")
+        n = size // 6
+    return C.c_void_p(ptr), n
+
+
+def _iptr(a):
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        if a.dtype != np.int32 or not a.flags.c_contiguous:
+            raise ValueError("loss array must be C-contiguous int32")
+        return C.c_void_p(a.ctypes.data)
+    return C.c_void_p(a.data_ptr())
+
+
+class Line:
+    """A lattice uploaded to a context (accel_line), with the reference ALine's pass API."""
+
+    def __init__(self, ctx: Context, elems: Sequence[ElemDesc]):
+        self.ctx = ctx
+        self.h = C.c_void_p()
+        arr = desc_array(elems)
+        _check(lib().accel_line_create(ctx.h, arr, len(elems), C.byref(self.h)), "accel_line_create")
+
+    def close(self):
+        if self.h:
+            lib().accel_line_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __len__(self):
+        n = C.c_int()
+        _check(lib().accel_line_count(self.h, C.byref(n)), "accel_line_count")
+        return n.value
+
+    def desc(self, i: int) -> ElemDesc:
+        d = ElemDesc()
+        _check(lib().accel_line_get_desc(self.h, i, C.byref(d)), "accel_line_get_desc")
+        return d
+
+    def descs(self) -> list[ElemDesc]:
+        return [self.desc(i) for i in range(len(self))]
+
+    def set_field(self, idx: int, field: int, value, index: int = 0):
+        v = (C.c_double * 2)(*np.atleast_1d(np.asarray(value, dtype=np.float64))[:2])
+        _check(lib().accel_line_set_field(self.h, idx, field, index, v), "accel_line_set_field")
+
+    def get_field(self, idx: int, field: int, index: int = 0):
+        v = (C.c_double * 2)()
+        _check(lib().accel_line_get_field(self.h, idx, field, index, v), "accel_line_get_field")
+        return v[0] if field not in (F_XLIM, F_YLIM) else (v[0], v[1])
+
+    def set_flags(self, rad=-1, cavity=-1, wake=-1):
+        _check(lib().accel_line_set_flags(self.h, rad, cavity, wake), "accel_line_set_flags")
+
+    def set_energy(self, en: float):
+        _check(lib().accel_line_set_energy(self.h, en), "accel_line_set_energy")
+
+    def setrfphase(self) -> float:
+        v = C.c_double()
+        _check(lib().accel_line_setrfphase(self.h, C.byref(v)), "accel_line_setrfphase")
+        return v.value
+
+    def set_seed(self, seed: int):
+        _check(lib().accel_line_set_seed(self.h, C.c_uint64(seed)), "accel_line_set_seed")
+
+    def track(self, r, nturn: int = 1, st: int = 0, ed: int | None = None, loss=None,
+              mode: int = MODE_FUSED, layout: int = LAYOUT_AOS, stream=None, n=None):
+        """ALine::pass(r, N, nturn) / pass(r, N, st, ed): r is updated in place."""
+        ptr, n = _ptr_and_n(r, n, layout)
+        ed = len(self) if ed is None else ed
+        s = C.c_void_p(stream) if stream is not None else None
+        _check(lib().accel_track(self.h, ptr, layout, n, st, ed, nturn, _iptr(loss), mode, s),
+               "accel_track")
+        return r
+
+    def m66(self, dpp=0.0, delta=1e-8, method=0, st=0, ed=None) -> np.ndarray:
+        m = (C.c_double * 36)()
+        ed = len(self) if ed is None else ed
+        _check(lib().accel_m66(self.h, st, ed, dpp, delta, method, m), "accel_m66")
+        return np.array(m).reshape(6, 6)
+
+    def m66_at(self, r0, method=0, delta=1e-8, st=0, ed=None) -> np.ndarray:
+        m = (C.c_double * 36)()
+        p = (C.c_double * 6)(*[float(x) for x in r0])
+        ed = len(self) if ed is None else ed
+        _check(lib().accel_m66_at(self.h, st, ed, p, method, delta, m), "accel_m66_at")
+        return np.array(m).reshape(6, 6)
+
+
+def _line_array(lines: Sequence[Line]):
+    return (C.c_void_p * len(lines))(*[l.h.value for l in lines])
+
+
+def track_batched(lines: Sequence[Line], part_off: np.ndarray, r_soa, nturn: int, loss=None,
+                  mode: int = MODE_FUSED, stream=None):
+    """Track many lattice instances in one launch; r_soa is a device tensor of 6 x Ntot."""
+    off = np.ascontiguousarray(part_off, dtype=np.int64)
+    ntot = int(off[-1])
+    s = C.c_void_p(stream) if stream is not None else None
+    _check(lib().accel_track_batched(_line_array(lines), len(lines), C.c_void_p(off.ctypes.data),
+                                     C.c_void_p(r_soa.data_ptr()), ntot, nturn, _iptr(loss), mode, s),
+           "accel_track_batched")
+
+
+def autotune(lines: Sequence[Line], part_off: np.ndarray, r_soa) -> tuple:
+    off = np.ascontiguousarray(part_off, dtype=np.int64)
+    t = (C.c_int * 3)()
+    _check(lib().accel_autotune(_line_array(lines), len(lines), C.c_void_p(off.ctypes.data),
+                                C.c_void_p(r_soa.data_ptr()), int(off[-1]), t), "accel_autotune")
+    return tuple(t)
+
+
+class Adjoint:
+    """accel_adjoint_forward / accel_adjoint_backward pair for one line."""
+
+    def __init__(self, line: Line, n: int, nturn: int, ckpt_every: int,
+                 params: Iterable[tuple[int, int, int]]):
+        params = list(params)
+        pe = np.array([p[0] for p in params], dtype=np.int32)
+        pf = np.array([p[1] for p in params], dtype=np.int32)
+        pi = np.array([p[2] for p in params], dtype=np.int32)
+        self._keep = (pe, pf, pi)
+        self.nparam = len(params)
+        self.n = n
+        self.h = C.c_void_p()
+        _check(lib().accel_adjoint_create(line.h, n, nturn, ckpt_every,
+                                          C.c_void_p(pe.ctypes.data), C.c_void_p(pf.ctypes.data),
+                                          C.c_void_p(pi.ctypes.data), self.nparam, C.byref(self.h)),
+               "accel_adjoint_create")
+
+    def close(self):
+        if self.h:
+            lib().accel_adjoint_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def forward(self, r0: np.ndarray) -> np.ndarray:
+        r0 = np.ascontiguousarray(r0, dtype=np.float64)
+        out = np.empty_like(r0)
+        _check(lib().accel_adjoint_forward(self.h, C.c_void_p(r0.ctypes.data),
+                                           C.c_void_p(out.ctypes.data)), "accel_adjoint_forward")
+        return out
+
+    def backward(self, g: np.ndarray):
+        g = np.ascontiguousarray(g, dtype=np.float64)
+        dr0 = np.empty_like(g)
+        dp = np.zeros(max(1, self.nparam))
+        _check(lib().accel_adjoint_backward(self.h, C.c_void_p(g.ctypes.data),
+                                            C.c_void_p(dr0.ctypes.data), C.c_void_p(dp.ctypes.data)),
+               "accel_adjoint_backward")
+        return dr0, dp[: self.nparam]

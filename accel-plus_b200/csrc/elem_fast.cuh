@@ -1,0 +1,349 @@
+// elem_fast.cuh — register-resident element maps for the fused persistent kernel.
+//
+// Same integrators as the reference (atpass.cpp), rearranged for the FP64 pipe:
+//  * the six coordinates live in registers for the whole turn (struct St);
+//  * multipole Horner sums start at the element's highest non-zero coefficient (the reference
+//    always starts at index 9 for StrMPole, accel.cpp:826,837-841, and at MaxNPole-1 for
+//    BendMPole; the leading zero terms add exact zeros for finite coordinates);
+//  * 1/(1+delta) is formed once per element where delta cannot change inside it (no radiation),
+//    and the element's per-slice constants are folded with it;
+//  * the adjacent full-length drifts that end one Yoshida slice and begin the next are merged;
+//  * a*b+c contracts to FMA.
+// None of these changes the map beyond rounding; the parity tests bound the difference.
+#pragma once
+#include <cmath>
+#include "engine.h"
+#include "philox.cuh"
+
+namespace accel {
+namespace fast {
+
+struct St { double x, px, y, py, z, d; };
+
+__device__ __forceinline__ double rcp(double a) { return __drcp_rn(a); }
+
+// fastdrift with NormL = nl and nlh = nl / (2 (1 + delta)) (atpass.cpp:416-428)
+__device__ __forceinline__ void drift(St& s, double nl, double nlh) {
+    double q = fma(s.px, s.px, s.py * s.py);
+    s.x = fma(nl, s.px, s.x);
+    s.y = fma(nl, s.py, s.y);
+    s.z = fma(-nlh, q, s.z);
+}
+
+// straight multipole kick (atpass.cpp:358-414) at compile-time order M
+template <int M, bool SKEW>
+__device__ __forceinline__ void kick(St& s, const double* A, const double* B, double K) {
+    double re = B[M];
+    double im = SKEW ? A[M] : 0.0;
+#pragma unroll
+    for (int i = M - 1; i >= 0; i--) {
+        double nre, nim;
+        if (!SKEW && i == M - 1) {
+            nre = fma(re, s.x, B[i]);
+            nim = re * s.y;
+        } else if (SKEW) {
+            nre = fma(re, s.x, fma(-im, s.y, B[i]));
+            nim = fma(im, s.x, fma(re, s.y, A[i]));
+        } else {
+            nre = fma(re, s.x, fma(-im, s.y, B[i]));
+            nim = fma(im, s.x, re * s.y);
+        }
+        re = nre;
+        im = nim;
+    }
+    s.px = fma(-K, re, s.px);
+    if (SKEW || M > 0) s.py = fma(K, im, s.py);
+}
+
+// Runtime-order kick for orders above the specialised ones.
+__device__ __forceinline__ void kick_n(St& s, const double* A, const double* B, double K, int M) {
+    double re = B[M], im = A[M];
+    for (int i = M - 1; i >= 0; i--) {
+        double nre = fma(re, s.x, fma(-im, s.y, B[i]));
+        im = fma(im, s.x, fma(re, s.y, A[i]));
+        re = nre;
+    }
+    s.px = fma(-K, re, s.px);
+    s.py = fma(K, im, s.py);
+}
+
+// AStrMPole::pass (accel.cpp:800-847), len > 0, effective order M.
+template <int M, bool SKEW>
+__device__ __forceinline__ void strmpole(St& s, const DevElem* __restrict__ e) {
+    double A[M + 1], B[M + 1];
+#pragma unroll
+    for (int i = 0; i <= M; i++) {
+        B[i] = e->v[V_B + i];
+        A[i] = SKEW ? e->v[V_A + i] : 0.0;
+    }
+    const double L1 = e->v[V_L1], L2 = e->v[V_L2], K1 = e->v[V_K1], K2 = e->v[V_K2];
+    const int ns = e->nslice;
+    const double inv = rcp(1.0 + s.d);
+    const double h = 0.5 * inv;
+    const double nl1 = L1 * inv, nl2 = L2 * inv;
+    const double nlh1 = nl1 * h, nlh2 = nl2 * h;
+    drift(s, nl1, nlh1);
+    for (int m = 0; m < ns; m++) {
+        kick<M, SKEW>(s, A, B, K1);
+        drift(s, nl2, nlh2);
+        kick<M, SKEW>(s, A, B, K2);
+        drift(s, nl2, nlh2);
+        kick<M, SKEW>(s, A, B, K1);
+        if (m + 1 < ns) drift(s, 2.0 * nl1, 2.0 * nlh1);
+    }
+    drift(s, nl1, nlh1);
+}
+
+__device__ __noinline__ void strmpole_generic(St& s, const DevElem* __restrict__ e) {
+    double A[ACCEL_MAX_MPOLE], B[ACCEL_MAX_MPOLE];
+    const int M = e->order_eff;
+#pragma unroll
+    for (int i = 0; i < ACCEL_MAX_MPOLE; i++) { A[i] = e->v[V_A + i]; B[i] = e->v[V_B + i]; }
+    const double L1 = e->v[V_L1], L2 = e->v[V_L2], K1 = e->v[V_K1], K2 = e->v[V_K2];
+    const int ns = e->nslice;
+    const double inv = rcp(1.0 + s.d);
+    const double h = 0.5 * inv;
+    const double nl1 = L1 * inv, nl2 = L2 * inv;
+    const double nlh1 = nl1 * h, nlh2 = nl2 * h;
+    drift(s, nl1, nlh1);
+    for (int m = 0; m < ns; m++) {
+        kick_n(s, A, B, K1, M);
+        drift(s, nl2, nlh2);
+        kick_n(s, A, B, K2, M);
+        drift(s, nl2, nlh2);
+        kick_n(s, A, B, K1, M);
+        if (m + 1 < ns) drift(s, 2.0 * nl1, 2.0 * nlh1);
+    }
+    drift(s, nl1, nlh1);
+}
+
+__device__ __forceinline__ void strmpole_dispatch(St& s, const DevElem* __restrict__ e) {
+    const bool skew = (e->flags & STR_SKEW) != 0;
+    switch (e->order_eff + (skew ? 16 : 0)) {
+    case 0: strmpole<0, false>(s, e); break;
+    case 1: strmpole<1, false>(s, e); break;
+    case 2: strmpole<2, false>(s, e); break;
+    case 3: strmpole<3, false>(s, e); break;
+    case 16: strmpole<0, true>(s, e); break;
+    case 17: strmpole<1, true>(s, e); break;
+    case 18: strmpole<2, true>(s, e); break;
+    case 19: strmpole<3, true>(s, e); break;
+    default: strmpole_generic(s, e); break;
+    }
+}
+
+// thin StrMPole (len == 0): one kick of weight 1 at the effective order
+__device__ __forceinline__ void strkick(St& s, const DevElem* __restrict__ e) {
+    double A[ACCEL_MAX_MPOLE], B[ACCEL_MAX_MPOLE];
+#pragma unroll
+    for (int i = 0; i < ACCEL_MAX_MPOLE; i++) { A[i] = e->v[V_A + i]; B[i] = e->v[V_B + i]; }
+    kick_n(s, A, B, 1.0, e->order_eff);
+}
+
+// ---- BendMPole ------------------------------------------------------------------------------
+// hx drift (atpass.cpp:343-355) with delta fixed: a = L/(1+d), b = hL^2/(4(1+d)^2),
+// c = hL/(2(1+d)), dd = L/(2(1+d)^2), g = hL/2
+struct HxCoef { double a, b, c, dd, g; };
+
+__device__ __forceinline__ HxCoef hx_coef(double L, double h, double inv) {
+    HxCoef k;
+    double hs = h * L;
+    k.a = inv * L;
+    k.b = 0.25 * hs * L * inv * inv;
+    k.c = 0.5 * hs * inv;
+    k.dd = 0.5 * L * inv * inv;
+    k.g = 0.5 * hs;
+    return k;
+}
+
+__device__ __forceinline__ void hxdrift(St& s, double h, const HxCoef& k) {
+    double px = s.px, py = s.py;
+    double pxx = px * px, pyy = py * py;
+    double q = pxx + pyy;
+    double hx1 = fma(h, s.x, 1.0);
+    s.x = fma(hx1 * px, k.a, fma(k.b, pxx - pyy, s.x));
+    s.px = fma(-k.c, q, px);
+    s.y = fma(hx1 * k.a * py, fma(px, k.g, 1.0), s.y);
+    s.z = fma(-hx1 * k.dd, q, s.z);
+}
+
+// Horner over B only (bendMPole kicks carry no skew terms), order M
+template <int M>
+__device__ __forceinline__ void horner_b(const St& s, const double* B, double& re, double& im) {
+    re = B[M];
+    im = 0.0;
+#pragma unroll
+    for (int i = M - 1; i >= 0; i--) {
+        double nre, nim;
+        if (i == M - 1) {
+            nre = fma(re, s.x, B[i]);
+            nim = re * s.y;
+        } else {
+            nre = fma(re, s.x, fma(-im, s.y, B[i]));
+            nim = fma(im, s.x, re * s.y);
+        }
+        re = nre;
+        im = nim;
+    }
+}
+
+// Element constants of the curved kick (atpass.cpp:199-235)
+struct BkCoef {
+    double h, K1, K2, c43K2, c3;   // c3 = h/6 K1 - K2/3
+    double cI, cR1, cR2;           // radiation: h(K1 h - K2)/6, -K1 h/2, h(K1 h - K2)/2
+};
+
+__device__ __forceinline__ void bend_kick_core(St& s, const BkCoef& c, double re, double im,
+                                               double L) {
+    double x = s.x, y = s.y;
+    double x2 = x * x, y2 = y * y;
+    double t1 = fma(c.h, x, fma(c.K1, fma(-0.5, y2, x2), c.K2 * x * fma(-4.0 / 3.0, y2, x2)));
+    double a = fma(c.h, t1, fma(-c.h, s.d, re));
+    s.px = fma(-L, a, s.px);
+    double t2 = fma(x * y, fma(c.c43K2, x, c.K1), c.c3 * y2 * y);
+    s.py = fma(L, fma(c.h, t2, im), s.py);
+    s.z = fma(-L * c.h, x, s.z);
+}
+
+// bndthinkickrad (atpass.cpp:255-339); returns the new 1/(1+delta) for the following drift
+template <int M, int RAD>
+__device__ __forceinline__ double bend_kick_rad(St& s, const double* B, const BkCoef& c, double L,
+                                                double crad, double qec, double inv, double gauss) {
+    double re, im;
+    horner_b<M>(s, B, re, im);
+    double x = s.x, y = s.y, y2 = y * y;
+    double xpr = s.px * inv, ypr = s.py * inv;
+    im = fma(c.cI, y2 * y, im);
+    re = fma(y2, fma(c.cR2, x, c.cR1), re);
+    double hx1 = fma(x, c.h, 1.0);
+    double vq = fma(xpr, xpr, ypr * ypr);
+    double vn2 = rcp(fma(hx1, hx1, vq));
+    double by = re + c.h, bx = im;
+    double cr = fma(bx, ypr, -by * xpr);
+    double b2p = fma(by * hx1, by * hx1, fma(bx * hx1, bx * hx1, cr * cr)) * vn2;
+    double opd = 1.0 + s.d;
+    double mean = crad * (opd * opd) * b2p * fma(0.5, vq, hx1) * L;
+    if (RAD == 1) {
+        s.d = s.d - mean;
+    } else {
+        double sig = sqrt(fabs(qec * mean));
+        s.d = s.d - fma(gauss, sig, mean);
+    }
+    double opd2 = 1.0 + s.d;
+    s.px = xpr * opd2;
+    s.py = ypr * opd2;
+    bend_kick_core(s, c, re, im, L);
+    return rcp(opd2);
+}
+
+template <int M>
+__device__ __forceinline__ void bendmpole(St& s, const DevElem* __restrict__ e,
+                                          uint64_t seed, uint32_t pid, uint32_t turn) {
+    double B[M + 1];
+#pragma unroll
+    for (int i = 0; i <= M; i++) B[i] = e->v[V_B + i];
+    const int rad = e->flags;
+    const int ns = e->nslice;
+    BkCoef c;
+    c.h = e->v[V_IRHO];
+    c.K1 = e->v[V_BK1];
+    c.K2 = e->v[V_BK2];
+    c.c43K2 = 4.0 / 3.0 * c.K2;
+    c.c3 = c.h / 6.0 * c.K1 - c.K2 / 3.0;
+    double kh = c.K1 * c.h - c.K2;
+    c.cI = c.h * kh / 6.0;
+    c.cR1 = -c.K1 * c.h / 2.0;
+    c.cR2 = c.h * kh / 2.0;
+    const double L1 = e->v[V_L1], L2 = e->v[V_L2], K1 = e->v[V_K1], K2 = e->v[V_K2];
+    const double psi1 = e->v[V_PSI1], psi2 = e->v[V_PSI2];
+    s.px = fma(s.x, psi1, s.px);
+    s.py = fma(-s.y, psi1, s.py);
+    if (rad == 0) {
+        const double inv = rcp(1.0 + s.d);
+        const HxCoef k1 = hx_coef(L1, c.h, inv), k2 = hx_coef(L2, c.h, inv);
+        for (int m = 0; m < ns; m++) {
+            double re, im;
+            hxdrift(s, c.h, k1);
+            horner_b<M>(s, B, re, im); bend_kick_core(s, c, re, im, K1);
+            hxdrift(s, c.h, k2);
+            horner_b<M>(s, B, re, im); bend_kick_core(s, c, re, im, K2);
+            hxdrift(s, c.h, k2);
+            horner_b<M>(s, B, re, im); bend_kick_core(s, c, re, im, K1);
+            hxdrift(s, c.h, k1);
+        }
+    } else if (rad == 1) {
+        const double crad = e->v[V_CRAD];
+        double inv = rcp(1.0 + s.d);
+        for (int m = 0; m < ns; m++) {
+            hxdrift(s, c.h, hx_coef(L1, c.h, inv));
+            inv = bend_kick_rad<M, 1>(s, B, c, K1, crad, 0.0, inv, 0.0);
+            hxdrift(s, c.h, hx_coef(L2, c.h, inv));
+            inv = bend_kick_rad<M, 1>(s, B, c, K2, crad, 0.0, inv, 0.0);
+            hxdrift(s, c.h, hx_coef(L2, c.h, inv));
+            inv = bend_kick_rad<M, 1>(s, B, c, K1, crad, 0.0, inv, 0.0);
+            hxdrift(s, c.h, hx_coef(L1, c.h, inv));
+        }
+    } else {
+        const double crad = e->v[V_CRAD], qec = e->v[V_QECOEF], SL = e->v[V_SL];
+        const double hs = 0.5 * SL;
+        double inv = rcp(1.0 + s.d);
+        for (int m = 0; m < ns; m++) {
+            hxdrift(s, c.h, hx_coef(hs, c.h, inv));
+            double g = qe_normal(seed, pid, turn, (uint32_t)e->elem, (uint32_t)m);
+            inv = bend_kick_rad<M, 2>(s, B, c, SL, crad, qec, inv, g);
+            hxdrift(s, c.h, hx_coef(hs, c.h, inv));
+        }
+    }
+    s.px = fma(s.x, psi2, s.px);
+    s.py = fma(-s.y, psi2, s.py);
+}
+
+// Orders above 3 are rare in bends: they run the literal map (elem_literal.cuh).
+__device__ __noinline__ void bendmpole_generic(St& s, const DevElem* __restrict__ e,
+                                               uint64_t seed, uint32_t pid, uint32_t turn);
+
+__device__ __forceinline__ void bendmpole_dispatch(St& s, const DevElem* __restrict__ e,
+                                                   uint64_t seed, uint32_t pid, uint32_t turn) {
+    switch (e->order_eff) {
+    case 0: bendmpole<0>(s, e, seed, pid, turn); break;
+    case 1: bendmpole<1>(s, e, seed, pid, turn); break;
+    case 2: bendmpole<2>(s, e, seed, pid, turn); break;
+    case 3: bendmpole<3>(s, e, seed, pid, turn); break;
+    default: bendmpole_generic(s, e, seed, pid, turn); break;
+    }
+}
+
+// ---- other elements ------------------------------------------------------------------------
+__device__ __forceinline__ void drift_elem(St& s, double len) {
+    double inv = rcp(1.0 + s.d);
+    double nl = len * inv;
+    drift(s, nl, nl * 0.5 * inv);
+}
+
+__device__ __forceinline__ void cavity(St& s, const DevElem* __restrict__ e) {
+    const double len = e->v[V_LEN];
+    if (len != 0) drift_elem(s, 0.5 * len);
+    if (e->flags) s.d = fma(e->v[V_NV], sin(fma(e->v[V_KZ], s.z, e->v[V_PHIS])), s.d);
+    if (len != 0) drift_elem(s, 0.5 * len);
+}
+
+__device__ __forceinline__ bool aperture_hit(St& s, const DevElem* __restrict__ e) {
+    const double a = e->v[V_XMIN], b = e->v[V_XMAX], c = e->v[V_YMIN], d = e->v[V_YMAX];
+    if (s.x <= a || s.x >= b || s.y <= c || s.y >= d) {
+        s.z = (double)((s.x <= a) * 1 + (s.x >= b) * 2 + (s.y <= c) * 3 + (s.y >= d) * 4);
+        s.x = __longlong_as_double(0x7ff8000000000000ll);
+        return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void aperture(St& s, const DevElem* __restrict__ e) {
+    if (aperture_hit(s, e)) return;
+    if (e->v[V_LEN] != 0) {
+        drift_elem(s, e->v[V_LEN]);
+        aperture_hit(s, e);
+    }
+}
+
+}  // namespace fast
+}  // namespace accel

@@ -1,0 +1,99 @@
+// engine.h — internal declarations shared by the host C++ and the CUDA translation units.
+#pragma once
+#include <cstdint>
+#include <cstddef>
+#include <string>
+#include <vector>
+#include <mutex>
+#include <atomic>
+#include "accel_gpu.h"
+
+namespace accel {
+
+// ------------------------------------------------------------------------------------------
+// Device element record.  One 384-byte record per element, 128-byte aligned, so an element
+// spans exactly three L1/L2 lines.  Lines are "compiled" from accel_elem_desc on the host:
+// every parameter-only expression the reference evaluates per particle (slice lengths, Yoshida
+// weights, irho*tan(e), CRAD, ...) is evaluated once here with the reference's operation order,
+// so the values are bit-identical to what the reference computes inside its loops.
+// ------------------------------------------------------------------------------------------
+enum DevOp : int32_t {
+    OP_NOP = 0,        // Monitor, zero-length markers
+    OP_DRIFT = 1,
+    OP_STRMPOLE = 2,   // len > 0: Yoshida slices
+    OP_STRKICK = 3,    // StrMPole with len == 0: one thin kick (accel.cpp:824-827)
+    OP_BENDMPOLE = 4,
+    OP_QUAD = 5,
+    OP_BEND = 6,
+    OP_CAVITY = 7,
+    OP_APERTURE = 8,
+    OP_CORRECTOR = 9,
+    OP_MATRIX = 10,
+    OP_SYNCRAD = 11,
+    OP_TRANSWAKE = 12, // collective: never inside a fused range
+    OP_LONGWAKE = 13,  // collective: never inside a fused range
+};
+
+struct alignas(128) DevElem {
+    int32_t op;
+    int32_t nslice;
+    int32_t order_eff;  // highest non-zero multipole index (exact Horner start for finite input)
+    int32_t order_lit;  // the order the reference loops from (9 for StrMPole, MaxNPole-1 bends)
+    int32_t flags;      // rad flag, on/off, skew-present bit (STR_SKEW)
+    int32_t elem;       // element index in the line
+    int32_t pad0, pad1;
+    double v[44];
+};
+static_assert(sizeof(DevElem) == 384, "DevElem must be 384 bytes");
+
+// payload slots
+enum : int {
+    V_LEN = 0,
+    // StrMPole / BendMPole
+    V_L1 = 1, V_L2 = 2, V_K1 = 3, V_K2 = 4, V_SL = 5,
+    V_IRHO = 6, V_PSI1 = 7,
+    V_A = 8,       // A[0..9] at v[8..17]
+    V_B = 18,      // B[0..9] at v[18..27]
+    V_PSI2 = 28, V_CRAD = 29, V_QECOEF = 30, V_BK1 = 31, V_BK2 = 32, V_ENERGY = 33,
+    // Quad
+    V_QK = 1,
+    // Bend
+    V_THETA = 1, V_GRD = 2, V_BIRHO = 3, V_BPSI1 = 4, V_BPSI2 = 5,
+    // Cavity
+    V_NV = 1, V_TF = 2, V_PHIS = 3, V_KZ = 4,
+    // Aperture
+    V_XMIN = 1, V_XMAX = 2, V_YMIN = 3, V_YMAX = 4,
+    // Corrector
+    V_KX = 1, V_KY = 2,
+    // Matrix
+    V_MAT = 8,     // 36 values v[8..43]
+    // SyncRad
+    V_ALFX = 1, V_ALFY = 2, V_ALFZ = 3, V_SX = 4, V_SY = 5, V_SZ = 6, V_SIGX = 7, V_SIGY = 8,
+    V_SIGD = 9,
+    // LongWake / TransWake keep their descriptor fields in v[1..12]
+    V_W = 1,
+};
+
+enum : int32_t { STR_SKEW = 1 << 8 };
+
+// ------------------------------------------------------------------------------------------
+// Host-side error plumbing
+// ------------------------------------------------------------------------------------------
+void set_error(const std::string& msg);
+int fail(int status, const std::string& msg);
+
+// lattice I/O (lattice_io.cpp)
+int parse_lattice(const std::string& text, std::vector<accel_elem_desc>& out, std::string& err);
+std::string format_lattice(const accel_elem_desc* e, int n, int precision);
+void default_desc(int type, accel_elem_desc* d);
+const char* type_name(int type);
+int type_from_name(const std::string& s);
+
+// compile descriptors to device records (compile.cpp)
+int compile_line(const accel_elem_desc* d, int n, std::vector<DevElem>& out, std::string& err);
+bool is_collective(int type);
+bool is_supported(int type);
+// Algorithmic flop count per particle-turn (model: add/sub/mul/div = 1 at the effective order)
+double model_flops(const accel_elem_desc* d, int n);
+
+}  // namespace accel

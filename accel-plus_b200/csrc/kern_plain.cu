@@ -1,0 +1,91 @@
+// kern_plain.cu — the plain per-element FP64 kernel and the transfer-matrix kernels.
+//
+// Built with --fmad=false: every product and sum rounds on its own, as on the x86-64 host, and
+// the element maps keep the reference's operand order (elem_literal.cuh).  One launch per
+// element per turn, one thread per particle, state in HBM (SoA): this is the straightforward GPU
+// form of AccelElement::pass, the comparator the fused kernel is measured against.
+#include <cuda_runtime.h>
+#include <cstdint>
+#include "kernels.h"
+#include "elem_literal.cuh"
+
+namespace accel {
+
+__global__ void __launch_bounds__(256) k_plain_elem(const TrackParams P, int e,
+                                                    const int32_t* __restrict__ turn_ctr) {
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t n = P.ntot;
+    if (p >= n) return;
+    double* __restrict__ st = P.st;
+    double r[6];
+    r[0] = st[p];
+    if (r[0] != r[0]) return;
+    r[1] = st[n + p]; r[2] = st[2 * n + p]; r[3] = st[3 * n + p]; r[4] = st[4 * n + p]; r[5] = st[5 * n + p];
+    const int inst = P.pinst ? P.pinst[p] : 0;
+    const DevElem& el = P.tables[(P.tbl_off ? P.tbl_off[inst] : 0) + e];
+    lit::QeSource q{P.seed, (uint32_t)p, (uint32_t)((P.rng_base ? *P.rng_base : 0) + P.rng_turn0 + *turn_ctr), (uint32_t)el.elem, 0u};
+    lit::pass<double>(el, r, q);
+    st[p] = r[0]; st[n + p] = r[1]; st[2 * n + p] = r[2];
+    st[3 * n + p] = r[3]; st[4 * n + p] = r[4]; st[5 * n + p] = r[5];
+}
+
+void launch_plain_elem(const TrackParams& p, int e, const int32_t* turn_ctr, cudaStream_t s) {
+    if (p.ntot <= 0) return;
+    k_plain_elem<<<(unsigned)((p.ntot + 255) / 256), 256, 0, s>>>(p, e, turn_ctr);
+}
+
+// End of a turn: the per-turn NaN scan of trackDA (aline.cpp:646-659), then the turn counter.
+__global__ void k_plain_turn_end(const TrackParams P, const int32_t* __restrict__ turn_ctr) {
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= P.ntot) return;
+    if (P.loss_turn[p] < 0 && P.st[p] != P.st[p]) P.loss_turn[p] = P.turn0 + *turn_ctr;
+}
+__global__ void k_inc(int32_t* c) { *c += 1; }
+
+void launch_plain_turn_end(const TrackParams& p, int32_t* turn_ctr, cudaStream_t s) {
+    if (p.ntot > 0) k_plain_turn_end<<<(unsigned)((p.ntot + 255) / 256), 256, 0, s>>>(p, turn_ctr);
+    k_inc<<<1, 1, 0, s>>>(turn_ctr);
+}
+
+// One-turn matrix.  method 0: exact tangent map — the literal maps on Dual<6> seeded with the
+// identity; method 1: twelve particles at +/-delta, m_ij = (r+_i - r-_i)/2/delta (aline.cpp:900-927).
+__global__ void k_m66_exact(const DevElem* __restrict__ tbl, int e0, int e1, const double* r0, double* m) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    Dual<6> r[6];
+    for (int i = 0; i < 6; i++) {
+        r[i] = Dual<6>(r0[i]);
+        r[i].d[i] = 1.0;
+    }
+    lit::QeSource q{0, 0, 0, 0, 0};
+    for (int e = e0; e < e1; e++) lit::pass<Dual<6>>(tbl[e], r, q);
+    for (int i = 0; i < 6; i++)
+        for (int j = 0; j < 6; j++) m[6 * i + j] = r[i].d[j];
+}
+
+__global__ void k_m66_fd(const DevElem* __restrict__ tbl, int e0, int e1, const double* r0,
+                         double delta, double* m) {
+    __shared__ double rr[12][6];
+    const int j = threadIdx.x;
+    if (j < 12) {
+        double r[6];
+        for (int k = 0; k < 6; k++) r[k] = r0[k];
+        if (j < 6) r[j] = r0[j] + delta;
+        else r[j - 6] = r0[j - 6] - delta;
+        lit::QeSource q{0, 0, 0, 0, 0};
+        for (int e = e0; e < e1; e++) lit::pass<double>(tbl[e], r, q);
+        for (int k = 0; k < 6; k++) rr[j][k] = r[k];
+    }
+    __syncthreads();
+    if (j < 36) {
+        int row = j / 6, col = j % 6;
+        m[j] = (rr[col][row] - rr[col + 6][row]) / 2.0 / delta;
+    }
+}
+
+void launch_m66(const DevElem* tbl, int e0, int e1, const double* r0_dev, double delta, int method,
+                double* m_dev, cudaStream_t s) {
+    if (method == 0) k_m66_exact<<<1, 32, 0, s>>>(tbl, e0, e1, r0_dev, m_dev);
+    else k_m66_fd<<<1, 64, 0, s>>>(tbl, e0, e1, r0_dev, delta, m_dev);
+}
+
+}  // namespace accel

@@ -1,0 +1,85 @@
+// kernels.h — launch interface of the CUDA translation units (host-callable).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "engine.h"
+
+namespace accel {
+
+// Particle state is SoA: coordinate k of particle p at st[k * ntot + p].
+struct TrackParams {
+    const DevElem* tables;   // concatenated element tables
+    const int32_t* tbl_off;  // [ninst] record offset of each instance's table (nullptr: 0)
+    const int32_t* pinst;    // [ntot] instance of each particle (nullptr: all 0)
+    double* st;              // SoA state
+    int64_t ntot;
+    int32_t* loss_turn;      // [ntot]; -1 alive
+    const int32_t* live;     // live list (fused) — entries index st
+    const int32_t* nlive;    // device count of live entries
+    int32_t* chunk_ctr;      // fused: atomic chunk counter, zero at launch
+    int32_t* err;            // error word (bounded waits)
+    int e0, e1;              // element range
+    int nturn;               // turns in this launch (fused)
+    int turn0;               // turn index (loss record) of the launch's first turn
+    const int32_t* turn_dev; // device turn counter added to turn0 and rng_turn0 (may be null)
+    int rng_turn0;           // turn offset fed to the QE counter
+    const int32_t* rng_base; // device: QE turn base of the line (advanced per call)
+    uint64_t seed;
+};
+
+// ---- fused (kern_fused.cu) ----------------------------------------------------------------
+constexpr int kNumFusedVariants = 6;
+struct VariantInfo { int block; int min_blocks; };
+VariantInfo fused_variant_info(int v);
+int fused_blocks_per_sm(int variant);                     // occupancy at the variant's block
+void launch_fused(const TrackParams& p, int variant, int grid, cudaStream_t s);
+// Stable compaction; live_in == live_out (in place) is allowed.  Resets the chunk counter and
+// adds `turns` to the device turn counter.
+void launch_compact(const int32_t* live_in, const int32_t* nin, const double* x, int32_t* live_out,
+                    int32_t* nout, int32_t* chunk_ctr, int32_t* turn_ctr, int turns, cudaStream_t s);
+void launch_init_live(const double* x, int64_t n, int32_t* loss_turn, int32_t* live, int32_t* nlive,
+                      int32_t* chunk_ctr, int init_loss, cudaStream_t s);
+void launch_aos_to_soa(const double* aos, double* soa, int64_t n, cudaStream_t s);
+void launch_soa_to_aos(const double* soa, double* aos, int64_t n, cudaStream_t s);
+void launch_fill_i32(int32_t* p, int32_t v, int64_t n, cudaStream_t s);
+void launch_copy_i32(const int32_t* src, int32_t* dst, int64_t n, cudaStream_t s);
+// collective elements on the live list (one instance only)
+void launch_longwake(const TrackParams& p, const DevElem* e_dev, const DevElem& e_host,
+                     double* scratch, int32_t* iscratch, cudaStream_t s);
+void launch_transwake(const TrackParams& p, const DevElem* e_dev, const DevElem& e_host,
+                      double* xsnap, cudaStream_t s);
+size_t longwake_scratch_doubles(int nbins);
+// moments of live particles: out[0..5] mean, [6..11] sigma, [12..17] cross, [18] nlive
+void launch_beam_stat(const double* st, int64_t n, double* partial, int nblk, double* out,
+                      cudaStream_t s);
+int beam_stat_blocks(int64_t n);
+double fp64_peak_run(int sm_count, cudaStream_t s, float* ms_out);
+
+// ---- plain (kern_plain.cu) ----------------------------------------------------------------
+void launch_plain_elem(const TrackParams& p, int e, const int32_t* turn_ctr, cudaStream_t s);
+void launch_plain_turn_end(const TrackParams& p, int32_t* turn_ctr, cudaStream_t s);
+// exact tangent map (Dual<6>) / central differences through [e0, e1) of one table
+void launch_m66(const DevElem* tbl, int e0, int e1, const double* r0_dev, double delta, int method,
+                double* m_dev, cudaStream_t s);
+
+// ---- adjoint (kern_adjoint.cu) ------------------------------------------------------------
+struct AdjParams {
+    const DevElem* tbl;
+    int ne;
+    int64_t n;
+    double* st;          // SoA state being advanced (forward / recompute)
+    double* lam;         // SoA adjoint
+    double* tape;        // [ne][6][n] element-input states of one turn
+    double* pgrad_part;  // [nblocks][nparam] per-block partial parameter gradients
+    const int32_t* pslot;   // [ne] slot of this element's first parameter, -1 none
+    const int32_t* pkind;   // [nparam] field kind
+    const int32_t* pindex;  // [nparam] multipole index
+    int nparam;
+    int32_t* err;
+};
+void launch_adj_turn_forward(const AdjParams& a, cudaStream_t s);      // st advanced one turn
+void launch_adj_turn_backward(const AdjParams& a, cudaStream_t s);     // uses st = turn input
+void launch_adj_reduce(const double* part, int nblk, int nparam, double* out, cudaStream_t s);
+int adj_blocks(int64_t n);
+
+}  // namespace accel

@@ -1,0 +1,81 @@
+// runtime.h — host-side objects behind the opaque C-ABI handles.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <utility>
+#include <vector>
+#include "engine.h"
+#include "kernels.h"
+
+namespace accel {
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    int ensure(size_t nbytes);  // grow-only; contents are not preserved on growth
+    void release();
+};
+
+struct GraphKey {
+    std::vector<int64_t> v;
+    bool operator<(const GraphKey& o) const { return v < o.v; }
+    bool operator==(const GraphKey& o) const { return v == o.v; }
+};
+using BatchKey = GraphKey;
+
+struct GraphEntry {
+    cudaGraphExec_t exec[4] = {nullptr, nullptr, nullptr, nullptr};  // pre, body, tail, post
+    int part_launches[4] = {0, 0, 0, 0};  // this library's kernels per launch of each part
+    ~GraphEntry();
+};
+
+int line_sync(struct ::accel_line* L);
+int desc_set_field(accel_elem_desc& d, int field, int index, const double* v);
+int desc_get_field(const accel_elem_desc& d, int field, int index, double* v);
+void apply_flags(accel_elem_desc* d, int n, int rad_flag, int cavity_on, int wake_on);
+void launch_rng_advance(int32_t* base, int nturn, cudaStream_t s);
+
+}  // namespace accel
+
+struct accel_ctx {
+    int device = 0;
+    int sm_count = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::mutex mu;
+    accel::DevBuf state, aos, loss, live0, cnt, tables, tbl_off, pinst, scratch, iscratch,
+        probe_state;
+    int tile_variant = -1;  // -1: tuned or default
+    int tile_seg = 0;       // 0: tuned or default
+    int bps[accel::kNumFusedVariants] = {0};
+    std::map<accel::GraphKey, std::unique_ptr<accel::GraphEntry>> graphs;
+    std::map<accel::GraphKey, std::pair<int, int>> tuned;  // -> (variant, seg)
+    accel::BatchKey batch_key;
+    int64_t launches = 0;
+    bool profile = false;                  // direct launches with events (accel_profile_enable)
+    std::vector<cudaEvent_t> prof_events;  // [begin, end] per tracking launch, then whole call
+    ~accel_ctx();
+};
+
+struct accel_line {
+    accel_ctx* ctx = nullptr;
+    std::vector<accel_elem_desc> desc;
+    std::vector<accel::DevElem> host_tbl;
+    accel::DevBuf d_tbl;
+    accel::DevBuf d_rng;  // [0]: QE turn base, advanced by every tracking call
+    bool dirty = true;
+    int64_t version = 0;
+    uint64_t seed = 0x5EED5EEDull;
+};
+
+namespace accel {
+inline GraphKey tune_key(::accel_line* const* lines, int ninst, int64_t ntot, int /*nturn*/) {
+    GraphKey k;
+    k.v = {(int64_t)(intptr_t)lines[0], lines[0]->version, (int64_t)ninst, ntot};
+    return k;
+}
+}  // namespace accel

@@ -1,0 +1,244 @@
+/*
+ * accel_gpu.h — C-ABI of the B200 tracking engine for Accel+ storage-ring lattices.
+ *
+ * Every entry point is `extern "C"`, returns an int status (ACCEL_OK == 0, negative on error),
+ * takes plain pointers and sizes, and never throws.  Particle state follows the reference's
+ * convention: six doubles per particle [x, px, y, py, z, delta]; a lost particle has x = NaN and
+ * an aperture code in z (reference accel.cpp:350-354).
+ *
+ * Pointers flagged "host or device" are classified with cudaPointerGetAttributes: device memory
+ * is used in place on the given stream; host memory is staged through the library's device
+ * buffers and copied back before the call returns.
+ *
+ * Reference interfaces replaced (paths inside the reference project, src/lib/accel/):
+ *   AccelElement::pass(double*, int)            accel.h:70        -> accel_track (st, ed range)
+ *   ALine::pass(double*, int, unsigned, unsigned) accel.h:625      -> accel_track (nturn = 1)
+ *   ALine::pass(double*, int), pass(.., nturn)  accel.h:626-627   -> accel_track
+ *   ALine::trackDA                              accel.h:628       -> accel_track (loss turns) + host
+ *   ALine::trackMA                              accel.h:630       -> accel_track_batched (start offsets)
+ *   ALine::getm66                               accel.h:635-637   -> accel_m66
+ *   ALine::deserialize / AccelElement::create   accel.h:68,607    -> accel_lattice_read
+ *   ALine::serialize                            accel.h:606       -> accel_lattice_write
+ *   AccelElement::setfield / getfield           accel.h:71-72     -> accel_line_set_field / get_field
+ *   ALine::set_rad_onoff / set_cavity_onoff /
+ *         set_wake_onoff / setenergy            accel.h:613-618   -> accel_line_set_flags / set_energy
+ *   ALine::setrfphase()                         accel.h:615       -> accel_line_setrfphase
+ *   calc_beam_stat                              utility.h:63      -> accel_beam_stat
+ */
+#ifndef ACCEL_GPU_H
+#define ACCEL_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------------------------ */
+#define ACCEL_OK               0
+#define ACCEL_E_INVALID       -1  /* bad argument, size or element parameter                   */
+#define ACCEL_E_UNSUPPORTED   -2  /* element type or mode the engine does not implement       */
+#define ACCEL_E_CUDA          -3  /* a CUDA runtime call failed (message via accel_last_error) */
+#define ACCEL_E_NOMEM         -4  /* device or host allocation failed                          */
+#define ACCEL_E_IO            -5  /* lattice file could not be opened or parsed                */
+#define ACCEL_E_TIMEOUT       -6  /* a bounded device wait ran out (kernel returned early)      */
+#define ACCEL_E_NODEVICE      -7  /* no CUDA device visible                                    */
+#define ACCEL_E_TOO_LARGE     -8  /* request exceeds a documented fixed capacity               */
+
+/* ---- element types: the names of the reference's type registry (accel.cpp:25-43) ---------- */
+#define ACCEL_DRIFT      1
+#define ACCEL_QUAD       2
+#define ACCEL_CORRECTOR  3
+#define ACCEL_APERTURE   4
+#define ACCEL_MONITOR    5
+#define ACCEL_BEND       6
+#define ACCEL_BENDMPOLE  7
+#define ACCEL_STRMPOLE   8
+#define ACCEL_CAVITY     9
+#define ACCEL_WIGTABLE  10   /* parsed, tracking returns ACCEL_E_UNSUPPORTED */
+#define ACCEL_IDEALWIG  11   /* parsed, tracking returns ACCEL_E_UNSUPPORTED */
+#define ACCEL_CRABCAV   12   /* parsed, tracking returns ACCEL_E_UNSUPPORTED */
+#define ACCEL_RFMULT    13   /* parsed, tracking returns ACCEL_E_UNSUPPORTED */
+#define ACCEL_TRANSWAKE 14
+#define ACCEL_MATRIX    15
+#define ACCEL_SYNCRAD   16
+#define ACCEL_LONGWAKE  17   /* no reference counterpart: longitudinal broadband-resonator wake */
+
+#define ACCEL_MAX_MPOLE  10  /* reference MAX_MPOLE, accel.h:48 */
+
+/* radiation flag values (reference accel.h:577-582) */
+#define ACCEL_RAD_OFF        0
+#define ACCEL_RAD_RAD        1
+#define ACCEL_RAD_RADQE      2
+#define ACCEL_RAD_LUMP       3
+#define ACCEL_RAD_LUMP_DAMP  4
+#define ACCEL_RAD_LUMP_QE    5
+
+/*
+ * Host-side element descriptor.  One per lattice element, in ring order.  Scalar fields live in
+ * f[] with a per-type meaning:
+ *   DRIFT      —
+ *   QUAD       f0 K
+ *   CORRECTOR  f0 KickX, f1 KickY
+ *   APERTURE   f0 xmin, f1 xmax, f2 ymin, f3 ymax
+ *   MONITOR    f0 Interval, f1 Ratio            (a no-op on the device)
+ *   BEND       f0 BendingAngle, f1 e1, f2 e2, f3 K, f4 irho
+ *   BENDMPOLE  f0 BendingAngle, f1 e1, f2 e2, f3 energy [MeV], f4 irho; poly_b; max_npole; nslice
+ *   STRMPOLE   poly_a, poly_b; max_npole; nslice
+ *   CAVITY     f0 Voltage [MV], f1 Frequency [Hz], f2 Phis [rad], f3 Energy [MeV]
+ *   TRANSWAKE  f0 Energy, f1 Charge [nC], f2 WakeX, f3 FreqX [GHz], f4 Qx, f5 WakeY, f6 FreqY, f7 Qy
+ *   MATRIX     mat[36] row-major
+ *   SYNCRAD    f0 Energy, f1 U0, f2 Jx, f3 Jy, f4 EmitX, f5 EmitY, f6 SigDelta, f7 BetaX, f8 BetaY
+ *   LONGWAKE   f0 Energy [MeV], f1 Charge [nC], f2 Rs [Ohm], f3 fr [Hz], f4 Q, f5 nbins
+ * irho is kept as its own field because the reference only refreshes it when BendingAngle is set
+ * (accel.h:170, accel.cpp:497,581), not when Length changes.
+ * flags: BENDMPOLE / SYNCRAD radiation flag (ACCEL_RAD_*), CAVITY / TRANSWAKE / LONGWAKE on-off.
+ */
+typedef struct accel_elem_desc {
+    int32_t type;
+    int32_t nslice;
+    int32_t max_npole;
+    int32_t flags;
+    double  len;
+    double  f[12];
+    double  poly_a[ACCEL_MAX_MPOLE];
+    double  poly_b[ACCEL_MAX_MPOLE];
+    double  mat[36];
+    char    famname[48];
+} accel_elem_desc;
+
+/* field ids for accel_line_set_field / get_field (the reference's setfield names) */
+#define ACCEL_F_LENGTH       1
+#define ACCEL_F_K            2
+#define ACCEL_F_POLYNOMB     3   /* index = order n */
+#define ACCEL_F_POLYNOMA     4   /* index = order n */
+#define ACCEL_F_NSLICE       5
+#define ACCEL_F_MAXNPOLE     6
+#define ACCEL_F_ANGLE        7   /* BendingAngle: also refreshes irho, as the reference does */
+#define ACCEL_F_E1           8
+#define ACCEL_F_E2           9
+#define ACCEL_F_VOLTAGE     10
+#define ACCEL_F_FREQUENCY   11
+#define ACCEL_F_PHIS        12
+#define ACCEL_F_ENERGY      13
+#define ACCEL_F_KICKX       14
+#define ACCEL_F_KICKY       15
+#define ACCEL_F_XLIM        16   /* two values */
+#define ACCEL_F_YLIM        17   /* two values */
+
+/* track modes */
+#define ACCEL_MODE_FUSED  0  /* persistent batched kernel: registers across turns, compaction */
+#define ACCEL_MODE_PLAIN  1  /* one launch per element, state in HBM, reference operation order */
+
+/* state layouts */
+#define ACCEL_LAYOUT_AOS  0  /* r[6*i + k]  (the reference's layout) */
+#define ACCEL_LAYOUT_SOA  1  /* r[k*N + i]                            */
+
+typedef struct accel_ctx  accel_ctx;   /* one per CUDA device: streams, scratch, tuned tiles */
+typedef struct accel_line accel_line;  /* a lattice uploaded to one context                */
+
+/* ---- library / context ------------------------------------------------------------------- */
+const char* accel_status_string(int status);
+const char* accel_last_error(void);              /* thread-local detail of the last failure   */
+int  accel_version(void);
+int  accel_device_count(int* n);
+int  accel_ctx_create(int device, accel_ctx** out);
+int  accel_ctx_destroy(accel_ctx* ctx);
+
+/* ---- lattice files (host only; no GPU needed) ----------------------------------------------
+ * accel_lattice_read follows AccelElement::deserialize (accel.cpp:67-133) and the per-type
+ * create() readers; it allocates *elems with malloc (free with accel_lattice_free).          */
+int  accel_lattice_read(const char* path, accel_elem_desc** elems, int* n);
+int  accel_lattice_parse(const char* text, accel_elem_desc** elems, int* n);
+int  accel_lattice_write(const char* path, const accel_elem_desc* elems, int n, int precision);
+void accel_lattice_free(accel_elem_desc* elems);
+int  accel_elem_default(int type, accel_elem_desc* out);   /* the reference's default ctor */
+
+/* ---- lines -------------------------------------------------------------------------------- */
+int  accel_line_create(accel_ctx* ctx, const accel_elem_desc* elems, int n, accel_line** out);
+int  accel_line_destroy(accel_line* line);
+int  accel_line_count(const accel_line* line, int* n);
+int  accel_line_get_desc(const accel_line* line, int idx, accel_elem_desc* out);
+int  accel_line_set_field(accel_line* line, int idx, int field, int index, const double* value);
+int  accel_line_get_field(const accel_line* line, int idx, int field, int index, double* value);
+int  accel_line_set_flags(accel_line* line, int rad_flag, int cavity_on, int wake_on);
+int  accel_line_set_energy(accel_line* line, double energy_mev);
+int  accel_line_setrfphase(accel_line* line, double* phis_out);      /* ALine::setrfphase() */
+int  accel_line_set_seed(accel_line* line, uint64_t seed);           /* Philox key for QE     */
+
+/*
+ * Track N particles through elements [st, ed) for nturn turns (ALine::pass semantics: a full turn
+ * when st == 0 and ed == n).  r: 6N doubles, host or device, in `layout`.  loss_turn (optional,
+ * host or device, N int32): -1 for survivors, else the 0-based turn in which x became NaN, which is
+ * what the reference's per-turn NaN scan in trackDA records (aline.cpp:646-659).
+ * stream: a cudaStream_t (NULL = the context's own stream).
+ */
+int  accel_track(accel_line* line, double* r, int layout, int N, int st, int ed, int nturn,
+                 int32_t* loss_turn, int mode, void* stream);
+
+/*
+ * Batched tracking: `ninst` lines (same context) tracked in one persistent launch.  Particles are
+ * grouped by instance: instance i owns particles [part_off[i], part_off[i+1]) of the SoA arrays
+ * r_soa (6 x Ntot doubles, k-major, device memory).  All lines must have the same element count.
+ */
+int  accel_track_batched(accel_line* const* lines, int ninst, const int64_t* part_off,
+                         double* r_soa, int64_t ntot, int nturn, int32_t* loss_turn,
+                         int mode, void* stream);
+
+/* Autotuner control: tile = {block, turns per segment (compaction cadence), variant} */
+int  accel_autotune(accel_line* const* lines, int ninst, const int64_t* part_off,
+                    const double* r_soa, int64_t ntot, int* tile_out3);
+int  accel_set_tile(accel_ctx* ctx, int block, int seg_turns, int variant);  /* 0s = auto */
+int  accel_get_tile(accel_ctx* ctx, int* tile_out3);
+
+/*
+ * One-turn (or [st, ed)) 6x6 transfer matrix around the point (0,0,0,0,0,dpp) (row-major m[36]).
+ * method 0: exact tangent map (forward-mode derivative through every element pass);
+ * method 1: central differences with step delta, as ALine::getm66 (aline.cpp:900-927).
+ */
+int  accel_m66(accel_line* line, int st, int ed, double dpp, double delta, int method,
+               double* m66);
+/* Same, around an arbitrary 6D point r0 (e.g. a closed orbit). */
+int  accel_m66_at(accel_line* line, int st, int ed, const double* r0, int method, double delta,
+                  double* m66);
+
+/*
+ * Reverse-mode (adjoint) pair.  Parameters are (element index, field, index) triples
+ * (ACCEL_F_POLYNOMB/A of StrMPole, ACCEL_F_K of Quad).
+ * accel_adjoint_forward tracks r0 (host or device, AoS, N particles) for nturn turns, keeping a
+ * checkpoint of the state every `ckpt_every` turns on the device, and writes r_final.
+ * accel_adjoint_backward takes dL/dr_final (AoS, 6N) and returns dL/dr0 (AoS, 6N) and
+ * dL/dparams (nparam), recomputing each segment from its checkpoint.
+ */
+typedef struct accel_adjoint accel_adjoint;
+int  accel_adjoint_create(accel_line* line, int N, int nturn, int ckpt_every,
+                          const int32_t* param_elem, const int32_t* param_field,
+                          const int32_t* param_index, int nparam, accel_adjoint** out);
+int  accel_adjoint_destroy(accel_adjoint* adj);
+int  accel_adjoint_forward(accel_adjoint* adj, const double* r0, double* r_final);
+int  accel_adjoint_backward(accel_adjoint* adj, const double* dl_drfinal, double* dl_dr0,
+                            double* dl_dparams);
+
+/* Beam moments of live particles (calc_beam_stat, utility.cpp:387-438): mean[6], sigma[6],
+ * cross[6] = <xx'>,<yy'>,<x d>,<x' d>,<y z>,<y' z>; returns the live count in *nlive.       */
+int  accel_beam_stat(accel_ctx* ctx, const double* r, int layout, int N, double* mean,
+                     double* sigma, double* cross, int* nlive);
+
+/* Device FP64 FMA throughput micro-benchmark (TFLOP/s, FMA = 2 flops). */
+int  accel_fp64_peak(accel_ctx* ctx, double* tflops);
+
+/* Number of this library's kernels launched since the context was created. */
+int  accel_launch_count(accel_ctx* ctx, int64_t* count);
+
+/* Measurement hook.  When on, every fused-kernel launch inside a tracking graph is bracketed by
+ * CUDA events recorded on the stream it runs on; accel_profile_read synchronizes the context's
+ * stream and returns, for the most recent tracking call, the summed device time of those
+ * launches, their count, and the call's whole device time. */
+int  accel_profile_enable(accel_ctx* ctx, int on);
+int  accel_profile_read(accel_ctx* ctx, double* fused_ms, int64_t* fused_launches, double* total_ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ACCEL_GPU_H */

@@ -1,0 +1,115 @@
+"""The C-ABI library on the host: it loads, exports every entry point the header declares, reads
+and writes the reference's lattice format, and reports errors by status without a GPU."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+
+def test_library_exports_every_declared_symbol(A):
+    lib = A.lib()
+    declared = A.exported_symbols()
+    assert len(declared) >= 35
+    missing = [s for s in declared if not hasattr(lib, s)]
+    assert not missing, missing
+
+
+def test_status_strings(A):
+    for s in (A.OK, A.E_INVALID, A.E_UNSUPPORTED, A.E_CUDA, A.E_NOMEM, A.E_IO, A.E_TIMEOUT,
+              A.E_NODEVICE, A.E_TOO_LARGE):
+        assert A.status_string(s) and A.status_string(s) != "unknown status"
+
+
+def test_lattice_roundtrip_bit_exact(A, LT, tmp_path):
+    for ring in (LT.config1_ring(), LT.config2_ring()):
+        p = str(tmp_path / "x.lat")
+        A.write_lattice(p, ring)
+        back = A.read_lattice(p)
+        assert len(back) == len(ring)
+        for a, b in zip(ring, back):
+            # the file carries no run-time switches (radiation, cavity on/off), only parameters
+            assert (a.type, a.nslice, a.max_npole, a.len, a.name) == (b.type, b.nslice, b.max_npole, b.len, b.name)
+            for f in ("f", "poly_a", "poly_b", "mat"):
+                assert bytes(getattr(a, f)) == bytes(getattr(b, f)), (a.name, f)
+
+
+def test_lattice_reader_grammar(A):
+    text = """
+    ! a comment line
+    QF1  : StrMPole 0.25 3
+        0 1.2 0
+        0 0 0
+    D1 :  Drift 2.0
+    B1:   BendMPole 1.0 0.1 0.01 0.02 2
+        0.0 0.5
+    RF :  Cavity 0 3.2 476e6 0.26 3000
+    AP :  Aperture 0 -0.05 0.05 -0.04 0.04
+    M  : Matrix 0
+      1 0 0 0 0 0
+      0 1 0 0 0 0
+      0 0 1 0 0 0
+      0 0 0 1 0 0
+      0 0 0 0 1 0
+      0 0 0 0 0 1
+    MON : Monitor 0 0 -2
+    RETURN
+    X : Drift 9
+    """
+    e = A.parse_lattice(text)
+    assert [d.type_name for d in e] == ["StrMPole", "Drift", "BendMPole", "Cavity", "Aperture", "Matrix", "Monitor"]
+    assert e[0].max_npole == 3 and e[0].poly_b[1] == 1.2 and e[0].nslice == 10
+    assert e[2].f[0] == 0.1 and e[2].f[4] == 0.1 / 1.0 and e[2].poly_b[1] == 0.5 and e[2].f[3] == 3000
+    assert e[3].flags == 1  # a Cavity is constructed on; the Lattice block switches it off
+    assert list(e[4].f[:4]) == [-0.05, 0.05, -0.04, 0.04]
+    assert e[6].f[0] == 1 and e[6].f[1] == 0.1  # interval clamped to 1, ratio < 0 -> 0.1
+
+
+def test_lattice_reader_errors(A):
+    with pytest.raises(A.AccelError) as ei:
+        A.parse_lattice("Q : Quadrupole 0.3 1.0\n")
+    assert ei.value.status == A.E_IO
+    with pytest.raises(A.AccelError) as ei:
+        A.parse_lattice("B : BendMPole 1.0 0.1 0 0 11\n 1 2 3\n")
+    assert ei.value.status == A.E_IO
+    with pytest.raises(A.AccelError) as ei:
+        A.read_lattice("/nonexistent/lattice.lat")
+    assert ei.value.status == A.E_IO
+
+
+@pytest.mark.skipif(not __import__("oracle").ref_available(), reason="reference library not built here")
+def test_reader_agrees_with_reference_deserialize(A, O, LT):
+    """Every element's fields as the reference's own deserialize+getfield see them."""
+    path = os.path.join(LT.GOLDEN_DIR, "dba18.lat")
+    mine = A.read_lattice(path)
+    ref = O.RefLine(path)
+    assert len(ref) == len(mine)
+    for i, d in enumerate(mine):
+        assert ref.get_field(i, "Length") == d.len
+        if d.type == A.STRMPOLE:
+            for n in range(d.max_npole):
+                assert ref.get_poly(i, n) == d.poly_b[n]
+                assert ref.get_poly(i, n, skew=True) == d.poly_a[n]
+        if d.type == A.CAVITY:
+            assert ref.get_field(i, "Voltage") == d.f[0]
+            assert ref.get_field(i, "Frequency") == d.f[1]
+            assert ref.get_field(i, "Phis") == d.f[2]
+
+
+def test_no_device_is_an_error_not_a_fallback(A):
+    if A.device_count() > 0:
+        pytest.skip("a device is present")
+    with pytest.raises(A.AccelError) as ei:
+        A.Context(0)
+    assert ei.value.status == A.E_NODEVICE
+
+
+def test_model_flops_match_survey_formula(A, LT):
+    """Config-1 FODO: 32 x [2 quads (m=1) + 2 sextupoles (m=2) + 2 bends (m=0) + 4 drifts]."""
+    ring = LT.config1_ring()
+    per_cell = 2 * 10 * (52 + 3 * 12) + 2 * 10 * (52 + 3 * 20) + 2 * (10 * (184 + 3 * 44) + 8) + 4 * 14
+    assert LT.flops_per_turn(ring) == 32 * per_cell

@@ -1,0 +1,251 @@
+"""GPU parity: the engine's kernels, through the C-ABI, against the reference's golden outputs and
+the CPU oracle on the same seeded inputs.
+
+Tolerances (FP64):
+  plain kernel (reference operation order, no FMA): bit-identical for every element whose map has
+      no per-particle transcendental; within 1e-14 relative where CUDA's sin/cos/sinh/cosh/exp
+      enter (linear Quad and Bend, Cavity, TransWake);
+  fused kernel (FMA, merged drifts, effective Horner order): within 1e-12 relative after one turn
+      and 1e-9 after 1,000 turns on regular orbits; loss turns identical.
+"Relative" is per coordinate, scaled by that coordinate's RMS over the live particles.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import rel_err, same_bits
+
+pytestmark = pytest.mark.gpu
+
+TRANSCENDENTAL = {"quad_f", "quad_d", "bend", "bend_neg", "cavity", "transwake"}
+
+
+def _flags(line, A, name):
+    if name == "cavity":
+        line.set_flags(cavity=1)
+    if name == "bendm_rad":
+        line.set_flags(rad=1)
+    if name == "transwake":
+        line.set_flags(wake=1)
+    if name == "syncrad_damp":
+        line.set_flags(rad=A.RAD_LUMP_DAMP)
+
+
+@pytest.mark.parametrize("mode", ["plain", "fused"])
+def test_elements_against_reference(A, ctx, G, MG, mode):
+    m = A.MODE_PLAIN if mode == "plain" else A.MODE_FUSED
+    for name, elems in MG.element_cases().items():
+        line = A.Line(ctx, elems)
+        _flags(line, A, name)
+        r = G["elem_in"].copy()
+        line.track(r, 1, mode=m)
+        ref = G[f"elem_{name}"]
+        if mode == "plain" and name not in TRANSCENDENTAL:
+            assert same_bits(r, ref), name
+        elif mode == "plain":
+            assert rel_err(r, ref) < 1e-14, name
+        else:
+            assert rel_err(r, ref) < 1e-12, (name, rel_err(r, ref))
+        assert np.array_equal(np.isnan(r[:, 0]), np.isnan(ref[:, 0])), name
+
+
+def test_plain_fodo_bit_exact(A, ctx, G, LT):
+    line = A.Line(ctx, LT.config1_ring())
+    for turns, key in ((1, "fodo_t1"), (100, "fodo_t100")):
+        r = G["fodo_in"].copy()
+        line.track(r, turns, mode=A.MODE_PLAIN)
+        assert same_bits(r, G[key]), key
+
+
+def test_fused_fodo_tolerance(A, ctx, G, LT):
+    line = A.Line(ctx, LT.config1_ring())
+    r = G["fodo_in"].copy()
+    line.track(r, 1)
+    assert rel_err(r, G["fodo_t1"]) < 1e-12
+    r = G["fodo_in"].copy()
+    line.track(r, 100)
+    assert rel_err(r, G["fodo_t100"]) < 1e-10
+
+
+def test_fused_config1_1000_turns(A, ctx, O, LT):
+    """Config 1 (FODO, uniform x in +-5 mm, y in +-2 mm), 1,000 turns: fused GPU vs the oracle."""
+    ring = LT.config1_ring()
+    p = LT.config1_particles()[:256].copy()
+    ref = p.copy()
+    lt_ref = O.port_track(ring, ref, 1000, nthreads=8)
+    line = A.Line(ctx, ring)
+    r = p.copy()
+    lt = np.empty(len(r), dtype=np.int32)
+    line.track(r, 1000, loss=lt)
+    assert np.array_equal(lt, lt_ref)
+    assert rel_err(r, ref) < 1e-9
+
+
+@pytest.mark.parametrize("mode", ["plain", "fused"])
+def test_dba_grid_loss_turns(A, ctx, G, LT, mode):
+    """Config 2 ring (radiation + cavity on): loss turns of a DA grid identical to the reference."""
+    m = A.MODE_PLAIN if mode == "plain" else A.MODE_FUSED
+    line = A.Line(ctx, LT.config2_ring())
+    r = G["dba_grid_in"].copy()
+    lt = np.empty(len(r), dtype=np.int32)
+    line.track(r, 200, loss=lt, mode=m)
+    assert np.array_equal(lt, G["dba_grid_loss"])
+    live = lt < 0
+    assert live.any()
+    tol = 0 if mode == "plain" else 1e-10
+    assert rel_err(r, G["dba_grid_out"]) <= tol
+    # lost particles carry the reference's aperture code in z and NaN in x
+    lost = ~live
+    assert np.all(np.isnan(r[lost, 0]))
+    codes = G["dba_grid_out"][lost, 4]
+    assert np.array_equal(r[lost, 4], codes)
+
+
+@pytest.mark.parametrize("mode", ["plain", "fused"])
+def test_batched_error_copies(A, ctx, G, LT, mode):
+    """Config-3 style: error-seeded copies with uneven grids tracked in one batched launch."""
+    import torch
+    m = A.MODE_PLAIN if mode == "plain" else A.MODE_FUSED
+    base = LT.config2_ring()
+    rings = [LT.error_copy(base, k) for k in range(2)]
+    grids = [G["c3_0_in"], G["c3_1_in"]]
+    extra = LT.error_copy(base, 7)
+    rings.append(extra)
+    grids.append(LT.da_grid(7, 3))
+    lines = [A.Line(ctx, r) for r in rings]
+    off = np.zeros(len(grids) + 1, dtype=np.int64)
+    off[1:] = np.cumsum([g.shape[0] for g in grids])
+    aos = np.concatenate(grids)
+    soa = torch.tensor(aos.T.copy(), device="cuda", dtype=torch.float64).contiguous()
+    loss = torch.empty(len(aos), device="cuda", dtype=torch.int32)
+    A.track_batched(lines, off, soa, 100, loss=loss, mode=m)
+    torch.cuda.synchronize()
+    out = soa.cpu().numpy().T.copy()
+    lt = loss.cpu().numpy()
+    for k in (0, 1):
+        s = slice(off[k], off[k + 1])
+        assert np.array_equal(lt[s], G[f"c3_{k}_loss"]), k
+        if mode == "plain":
+            assert same_bits(out[s], G[f"c3_{k}_out"])
+        else:
+            assert rel_err(out[s], G[f"c3_{k}_out"]) < 1e-10
+    # the third copy against the oracle
+    import oracle as O
+    r3 = grids[2].copy()
+    lt3 = O.port_track(rings[2], r3, 100)
+    s = slice(off[2], off[3])
+    assert np.array_equal(lt[s], lt3)
+    assert rel_err(out[s], r3) < 1e-10
+
+
+def test_m66_fd_matches_getm66_and_exact_is_close(A, ctx, G, LT):
+    line = A.Line(ctx, LT.config1_ring())
+    fd = line.m66(method=1, delta=1e-8)
+    assert same_bits(fd, G["fodo_m66"])  # the FD path is the reference's getm66 on the GPU
+    ex = line.m66(method=0)
+    assert np.max(np.abs(ex - fd)) < 1e-6 * max(1.0, np.max(np.abs(fd)))
+    # exact map is symplectic: M^T J M = J in the transverse 4x4 block
+    J = np.zeros((4, 4))
+    J[0, 1] = J[2, 3] = 1
+    J[1, 0] = J[3, 2] = -1
+    m4 = ex[:4, :4]
+    assert np.max(np.abs(m4.T @ J @ m4 - J)) < 1e-12
+
+
+def test_setrfphase_matches_reference(A, ctx, G, LT):
+    """ALine::setrfphase on the GPU (plain kernel, radiation on): the reference's phase, bit for bit."""
+    line = A.Line(ctx, A.read_lattice(f"{LT.GOLDEN_DIR}/dba18.lat"))
+    assert line.setrfphase() == G["dba_phis"][0]
+
+
+def test_range_pass_and_layouts(A, ctx, O, G, LT):
+    """pass(r, N, st, ed) on a sub-range, AoS and SoA, host and device pointers."""
+    import torch
+    ring = LT.config1_ring()
+    line = A.Line(ctx, ring)
+    p = G["fodo_in"].copy()
+    ref = p.copy()
+    O.port_pass_line(ring, ref, 17, 211)
+    r = p.copy()
+    line.track(r, 1, st=17, ed=211, mode=A.MODE_PLAIN)
+    assert same_bits(r, ref)
+    soa = np.ascontiguousarray(p.T)
+    line.track(soa, 1, st=17, ed=211, mode=A.MODE_PLAIN, layout=A.LAYOUT_SOA, n=len(p))
+    assert same_bits(soa.T, ref)
+    dev = torch.tensor(p, device="cuda")
+    line.track(dev, 1, st=17, ed=211, mode=A.MODE_PLAIN)
+    torch.cuda.synchronize()
+    assert same_bits(dev.cpu().numpy(), ref)
+
+
+def test_beam_stat_matches_calc_beam_stat(A, ctx, O, G):
+    r = G["dba_grid_out"].copy()
+    mean, sig, cross, nl = ctx.beam_stat(r)
+    m2, s2, c2, n2 = O.port_beam_stat(r)
+    assert nl == n2
+    assert np.allclose(mean, m2, rtol=1e-12, atol=1e-18)
+    assert np.allclose(sig, s2, rtol=1e-12, atol=1e-18)
+    assert np.allclose(cross, c2, rtol=1e-10, atol=1e-20)
+
+
+def test_longwake_against_oracle(A, ctx, O, LT):
+    rng = np.random.default_rng(11)
+    n = 4096
+    r = np.zeros((n, 6))
+    r[:, 0] = rng.normal(0, 1e-4, n)
+    r[:, 4] = rng.normal(0, 3e-3, n)
+    r[:, 5] = rng.normal(0, 1e-3, n)
+    r[::97, 0] = np.nan  # a few lost particles are skipped
+    elems = [LT.longwake_elem()]
+    ref = r.copy()
+    O.port_track(elems, ref, 1, loss=False)
+    line = A.Line(ctx, elems)
+    out = r.copy()
+    line.track(out, 1)
+    assert np.array_equal(np.isnan(out[:, 0]), np.isnan(ref[:, 0]))
+    d_ref, d = ref[:, 5] - r[:, 5], out[:, 5] - r[:, 5]
+    live = ~np.isnan(r[:, 0])
+    assert np.max(np.abs(d[live] - d_ref[live])) < 1e-12 * np.max(np.abs(d_ref[live]))
+    assert np.max(np.abs(d_ref[live])) > 0
+
+
+def test_errors_are_statuses(A, ctx):
+    wig = A.elem(A.IDEALWIG, "W", 1.0)
+    line = A.Line(ctx, [wig])
+    r = np.zeros((4, 6))
+    with pytest.raises(A.AccelError) as ei:
+        line.track(r, 1)
+    assert ei.value.status == A.E_UNSUPPORTED
+    line2 = A.Line(ctx, [A.elem(A.DRIFT, "D", 1.0)])
+    with pytest.raises(A.AccelError) as ei:
+        line2.track(r, 1, st=0, ed=5)
+    assert ei.value.status == A.E_INVALID
+
+
+def test_autotune_and_launch_count(A, ctx, LT):
+    import torch
+    base = LT.config2_ring()
+    rings = [LT.error_copy(base, k) for k in range(3)]
+    grids = [LT.da_grid(11, 5), LT.da_grid(13, 7), LT.da_grid(9, 9)]
+    lines = [A.Line(ctx, r) for r in rings]
+    off = np.zeros(4, dtype=np.int64)
+    off[1:] = np.cumsum([g.shape[0] for g in grids])
+    aos = np.concatenate(grids)
+    soa0 = torch.tensor(aos.T.copy(), device="cuda").contiguous()
+    ctx.set_tile(0, 16, 0)
+    a = soa0.clone()
+    la = torch.empty(len(aos), device="cuda", dtype=torch.int32)
+    n0 = ctx.launch_count()
+    A.track_batched(lines, off, a, 50, loss=la)
+    torch.cuda.synchronize()
+    assert ctx.launch_count() > n0
+    ctx.set_tile(0, 0, -1)
+    tile = A.autotune(lines, off, soa0)
+    assert tile[0] in (64, 128, 256) and tile[1] > 0
+    b = soa0.clone()
+    lb = torch.empty(len(aos), device="cuda", dtype=torch.int32)
+    A.track_batched(lines, off, b, 50, loss=lb)
+    torch.cuda.synchronize()
+    assert torch.equal(la, lb)
+    assert rel_err(a.cpu().numpy().T, b.cpu().numpy().T) < 1e-13
