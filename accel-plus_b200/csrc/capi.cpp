@@ -303,8 +303,9 @@ static int run_core(accel_ctx* C, const CoreReq& q, cudaStream_t user) {
         if (C->bps[q.variant] <= 0) return fail(ACCEL_E_CUDA, "fused kernel cannot be resident");
     }
     const Plan plan = make_plan(q, has_collective(q.lines[0], q.e0, q.e1));
-    // order after the user's prior work, run on the private stream, order the user's stream after
-    if (user && user != C->stream) {
+    // order after the caller's prior work on `user`, run on the private stream, then order the
+    // caller's stream after ours (user may be 0, the legacy default stream)
+    if (user != C->stream) {
         CK(cudaEventRecord(C->ev0, user));
         CK(cudaStreamWaitEvent(C->stream, C->ev0, 0));
     }
@@ -367,7 +368,7 @@ static int run_core(accel_ctx* C, const CoreReq& q, cudaStream_t user) {
         C->launches += g->part_launches[PART_PRE] + (int64_t)plan.nbody * g->part_launches[PART_BODY] +
                        (plan.tail ? g->part_launches[PART_TAIL] : 0) + g->part_launches[PART_POST];
     }
-    if (user && user != C->stream) {
+    if (user != C->stream) {
         CK(cudaEventRecord(C->ev1, C->stream));
         CK(cudaStreamWaitEvent(user, C->ev1, 0));
     }
@@ -595,7 +596,7 @@ int accel_track(accel_line* L, double* r, int layout, int N, int st, int ed, int
         }
         return ACCEL_OK;
     }
-    cudaStream_t user = stream ? (cudaStream_t)stream : C->stream;
+    cudaStream_t user = (cudaStream_t)stream;  // NULL: the legacy default stream
     const bool rdev = is_device_ptr(r);
     const bool ldev = loss_turn ? is_device_ptr(loss_turn) : false;
     const size_t nb = sizeof(double) * 6 * (size_t)N;
@@ -716,7 +717,7 @@ int accel_track_batched(accel_line* const* lines, int ninst, const int64_t* part
     if (!is_device_ptr(r_soa)) return fail(ACCEL_E_INVALID, "r_soa must be device memory");
     if (loss_turn && !is_device_ptr(loss_turn)) return fail(ACCEL_E_INVALID, "loss_turn must be device memory");
     if (ntot == 0 || nturn == 0) return ACCEL_OK;
-    cudaStream_t user = stream ? (cudaStream_t)stream : C->stream;
+    cudaStream_t user = (cudaStream_t)stream;  // NULL: the legacy default stream
     if ((s = C->loss.ensure(sizeof(int32_t) * (size_t)ntot))) return s;
     CoreReq q{};
     q.lines = lines;
@@ -769,7 +770,7 @@ int accel_autotune(accel_line* const* lines, int ninst, const int64_t* part_off,
         q.seg = seg;
         q.nturn = turns;
         CK(cudaMemcpyAsync(q.st, r_soa, nb, cudaMemcpyDeviceToDevice, C->stream));
-        int st2 = run_core(C, q, C->stream);  // builds (untimed) graph on first use
+        int st2 = run_core(C, q, C->stream);  // builds the (untimed) graphs on first use
         if (st2) return st2;
         CK(cudaMemcpyAsync(q.st, r_soa, nb, cudaMemcpyDeviceToDevice, C->stream));
         cudaEvent_t a, b;

@@ -177,9 +177,10 @@ int compile_line(const accel_elem_desc* d, int n, std::vector<DevElem>& out, std
             r.flags = e.flags ? 1 : 0;
             break;
         default:
-            err = std::string("element ") + e.famname + " of type " + type_name(e.type) +
-                  " is not supported by the tracking engine";
-            return ACCEL_E_UNSUPPORTED;
+            // parsed and kept (the line can be read, edited and written back); tracking through
+            // it is refused by the C-ABI with ACCEL_E_UNSUPPORTED before any launch
+            r.op = OP_NOP;
+            break;
         }
     }
     return ACCEL_OK;

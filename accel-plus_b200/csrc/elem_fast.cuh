@@ -20,6 +20,12 @@ namespace fast {
 
 struct St { double x, px, y, py, z, d; };
 
+// Elements and multipole orders outside the specialised paths run the literal map through one
+// out-of-line call that takes and returns the state by value (defined in kern_fused.cu), so the
+// hot path's state never has its address taken and stays in registers.
+__device__ __noinline__ St rare_elem(St s, const DevElem* __restrict__ e, uint64_t seed,
+                                     uint32_t pid, uint32_t turn);
+
 __device__ __forceinline__ double rcp(double a) { return __drcp_rn(a); }
 
 // fastdrift with NormL = nl and nlh = nl / (2 (1 + delta)) (atpass.cpp:416-428)
@@ -55,18 +61,6 @@ __device__ __forceinline__ void kick(St& s, const double* A, const double* B, do
     if (SKEW || M > 0) s.py = fma(K, im, s.py);
 }
 
-// Runtime-order kick for orders above the specialised ones.
-__device__ __forceinline__ void kick_n(St& s, const double* A, const double* B, double K, int M) {
-    double re = B[M], im = A[M];
-    for (int i = M - 1; i >= 0; i--) {
-        double nre = fma(re, s.x, fma(-im, s.y, B[i]));
-        im = fma(im, s.x, fma(re, s.y, A[i]));
-        re = nre;
-    }
-    s.px = fma(-K, re, s.px);
-    s.py = fma(K, im, s.py);
-}
-
 // AStrMPole::pass (accel.cpp:800-847), len > 0, effective order M.
 template <int M, bool SKEW>
 __device__ __forceinline__ void strmpole(St& s, const DevElem* __restrict__ e) {
@@ -94,29 +88,6 @@ __device__ __forceinline__ void strmpole(St& s, const DevElem* __restrict__ e) {
     drift(s, nl1, nlh1);
 }
 
-__device__ __noinline__ void strmpole_generic(St& s, const DevElem* __restrict__ e) {
-    double A[ACCEL_MAX_MPOLE], B[ACCEL_MAX_MPOLE];
-    const int M = e->order_eff;
-#pragma unroll
-    for (int i = 0; i < ACCEL_MAX_MPOLE; i++) { A[i] = e->v[V_A + i]; B[i] = e->v[V_B + i]; }
-    const double L1 = e->v[V_L1], L2 = e->v[V_L2], K1 = e->v[V_K1], K2 = e->v[V_K2];
-    const int ns = e->nslice;
-    const double inv = rcp(1.0 + s.d);
-    const double h = 0.5 * inv;
-    const double nl1 = L1 * inv, nl2 = L2 * inv;
-    const double nlh1 = nl1 * h, nlh2 = nl2 * h;
-    drift(s, nl1, nlh1);
-    for (int m = 0; m < ns; m++) {
-        kick_n(s, A, B, K1, M);
-        drift(s, nl2, nlh2);
-        kick_n(s, A, B, K2, M);
-        drift(s, nl2, nlh2);
-        kick_n(s, A, B, K1, M);
-        if (m + 1 < ns) drift(s, 2.0 * nl1, 2.0 * nlh1);
-    }
-    drift(s, nl1, nlh1);
-}
-
 __device__ __forceinline__ void strmpole_dispatch(St& s, const DevElem* __restrict__ e) {
     const bool skew = (e->flags & STR_SKEW) != 0;
     switch (e->order_eff + (skew ? 16 : 0)) {
@@ -128,16 +99,8 @@ __device__ __forceinline__ void strmpole_dispatch(St& s, const DevElem* __restri
     case 17: strmpole<1, true>(s, e); break;
     case 18: strmpole<2, true>(s, e); break;
     case 19: strmpole<3, true>(s, e); break;
-    default: strmpole_generic(s, e); break;
+    default: s = rare_elem(s, e, 0, 0, 0); break;
     }
-}
-
-// thin StrMPole (len == 0): one kick of weight 1 at the effective order
-__device__ __forceinline__ void strkick(St& s, const DevElem* __restrict__ e) {
-    double A[ACCEL_MAX_MPOLE], B[ACCEL_MAX_MPOLE];
-#pragma unroll
-    for (int i = 0; i < ACCEL_MAX_MPOLE; i++) { A[i] = e->v[V_A + i]; B[i] = e->v[V_B + i]; }
-    kick_n(s, A, B, 1.0, e->order_eff);
 }
 
 // ---- BendMPole ------------------------------------------------------------------------------
@@ -298,10 +261,6 @@ __device__ __forceinline__ void bendmpole(St& s, const DevElem* __restrict__ e,
     s.py = fma(-s.y, psi2, s.py);
 }
 
-// Orders above 3 are rare in bends: they run the literal map (elem_literal.cuh).
-__device__ __noinline__ void bendmpole_generic(St& s, const DevElem* __restrict__ e,
-                                               uint64_t seed, uint32_t pid, uint32_t turn);
-
 __device__ __forceinline__ void bendmpole_dispatch(St& s, const DevElem* __restrict__ e,
                                                    uint64_t seed, uint32_t pid, uint32_t turn) {
     switch (e->order_eff) {
@@ -309,7 +268,7 @@ __device__ __forceinline__ void bendmpole_dispatch(St& s, const DevElem* __restr
     case 1: bendmpole<1>(s, e, seed, pid, turn); break;
     case 2: bendmpole<2>(s, e, seed, pid, turn); break;
     case 3: bendmpole<3>(s, e, seed, pid, turn); break;
-    default: bendmpole_generic(s, e, seed, pid, turn); break;
+    default: s = rare_elem(s, e, seed, pid, turn); break;
     }
 }
 

@@ -26,21 +26,15 @@ __device__ __forceinline__ bool nan_(double v) { return v != v; }
 __device__ __forceinline__ double qnan() { return __longlong_as_double(0x7ff8000000000000ll); }
 }  // namespace
 
-// Rare elements (Quad, Bend, Corrector, Matrix, SyncRad, high-order bends) run the literal map.
-__device__ __noinline__ void generic_elem(fast::St& s, const DevElem* __restrict__ e, uint64_t seed,
-                                          uint32_t pid, uint32_t turn) {
+// Rare elements (thin and high-order multipoles, Quad, Bend, Corrector, Matrix, SyncRad) run the
+// literal map out of line; the state goes in and out by value.
+__device__ __noinline__ fast::St fast::rare_elem(fast::St s, const DevElem* __restrict__ e,
+                                                 uint64_t seed, uint32_t pid, uint32_t turn) {
     double r[6] = {s.x, s.px, s.y, s.py, s.z, s.d};
     lit::QeSource q{seed, pid, turn, (uint32_t)e->elem, 0u};
     lit::pass<double>(*e, r, q);
-    s.x = r[0]; s.px = r[1]; s.y = r[2]; s.py = r[3]; s.z = r[4]; s.d = r[5];
+    return fast::St{r[0], r[1], r[2], r[3], r[4], r[5]};
 }
-
-namespace fast {
-__device__ __noinline__ void bendmpole_generic(St& s, const DevElem* __restrict__ e, uint64_t seed,
-                                               uint32_t pid, uint32_t turn) {
-    generic_elem(s, e, seed, pid, turn);
-}
-}  // namespace fast
 
 __device__ __forceinline__ void fused_elem(fast::St& s, const DevElem* __restrict__ e, uint64_t seed,
                                            uint32_t pid, uint32_t turn) {
@@ -48,13 +42,13 @@ __device__ __forceinline__ void fused_elem(fast::St& s, const DevElem* __restric
     case OP_NOP: break;
     case OP_DRIFT: fast::drift_elem(s, e->v[V_LEN]); break;
     case OP_STRMPOLE: fast::strmpole_dispatch(s, e); break;
-    case OP_STRKICK: fast::strkick(s, e); break;
+    case OP_STRKICK: s = fast::rare_elem(s, e, seed, pid, turn); break;
     case OP_BENDMPOLE: fast::bendmpole_dispatch(s, e, seed, pid, turn); break;
     case OP_CAVITY: fast::cavity(s, e); break;
     case OP_APERTURE: fast::aperture(s, e); break;
     case OP_TRANSWAKE:
     case OP_LONGWAKE: break;  // collective: the host never puts one inside a fused range
-    default: generic_elem(s, e, seed, pid, turn); break;
+    default: s = fast::rare_elem(s, e, seed, pid, turn); break;
     }
 }
 

@@ -50,6 +50,10 @@ def parse():
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--small", action="store_true",
                     help="profiling case: 16 copies, 20 turns, one step (for ncu)")
+    ap.add_argument("--variant", type=int, default=-1, help="force a fused-kernel variant (skips autotuning)")
+    ap.add_argument("--seg", type=int, default=0, help="force turns per segment")
+    ap.add_argument("--engine-only", action="store_true",
+                    help="only the fused engine timing: no plain, e2e, CPU legs (profiling runs)")
     return ap.parse_args()
 
 
@@ -223,6 +227,8 @@ def engine_arm(args):
     if args.small:
         args.copies, args.turns, args.steps, args.warmup = 16, 20, 1, 1
         args.no_plain = args.no_cpu = args.no_e2e = True
+    if args.engine_only:
+        args.no_plain = args.no_cpu = args.no_e2e = True
 
     rings, off, aos, sizes = workload(args.copies, rank)
     ntot = int(off[-1])
@@ -258,7 +264,10 @@ def engine_arm(args):
         A.track_batched(lines, off, state, args.turns, loss=loss, mode=mode, stream=stream)
 
     tile = None
-    if not args.no_autotune:
+    if args.variant >= 0 or args.seg > 0:
+        ctx.set_tile(0, max(0, args.seg), args.variant)
+        tile = ctx.get_tile()
+    elif not args.no_autotune:
         tile = A.autotune(lines, off, soa0)
     for k in range(args.warmup):
         step(k=k)

@@ -172,7 +172,8 @@ int  accel_line_set_seed(accel_line* line, uint64_t seed);           /* Philox k
  * when st == 0 and ed == n).  r: 6N doubles, host or device, in `layout`.  loss_turn (optional,
  * host or device, N int32): -1 for survivors, else the 0-based turn in which x became NaN, which is
  * what the reference's per-turn NaN scan in trackDA records (aline.cpp:646-659).
- * stream: a cudaStream_t (NULL = the context's own stream).
+ * stream: a cudaStream_t; NULL is the legacy default stream.  The work runs on the context's own
+ * stream, ordered after the caller's prior work on `stream` and before its later work.
  */
 int  accel_track(accel_line* line, double* r, int layout, int N, int st, int ed, int nturn,
                  int32_t* loss_turn, int mode, void* stream);
