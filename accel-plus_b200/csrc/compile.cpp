@@ -49,6 +49,32 @@ static int highest_nonzero(const double* a, const double* b, int upto) {
     return m;
 }
 
+// Copy what the fused kernel reads into the first 128-byte line of the record.
+static void fill_hot(DevElem& r) {
+    for (int i = 0; i < 14; i++) r.h[i] = 0.0;
+    switch (r.op) {
+    case OP_DRIFT: r.h[H_LEN] = r.v[V_LEN]; break;
+    case OP_STRMPOLE:
+        r.h[H_L1] = r.v[V_L1]; r.h[H_L2] = r.v[V_L2]; r.h[H_K1] = r.v[V_K1]; r.h[H_K2] = r.v[V_K2];
+        for (int i = 0; i <= kHotOrder; i++) { r.h[H_A + i] = r.v[V_A + i]; r.h[H_B + i] = r.v[V_B + i]; }
+        break;
+    case OP_BENDMPOLE:
+        r.h[H_L1] = r.v[V_L1]; r.h[H_L2] = r.v[V_L2]; r.h[H_K1] = r.v[V_K1]; r.h[H_K2] = r.v[V_K2];
+        r.h[H_IRHO] = r.v[V_IRHO]; r.h[H_PSI1] = r.v[V_PSI1]; r.h[H_PSI2] = r.v[V_PSI2];
+        r.h[H_CRAD] = r.v[V_CRAD]; r.h[H_BK1] = r.v[V_BK1]; r.h[H_BK2] = r.v[V_BK2];
+        for (int i = 0; i <= kHotOrder; i++) r.h[H_BB + i] = r.v[V_B + i];
+        break;
+    case OP_CAVITY:
+        r.h[H_LEN] = r.v[V_LEN]; r.h[H_NV] = r.v[V_NV]; r.h[H_KZ] = r.v[V_KZ]; r.h[H_PHIS] = r.v[V_PHIS];
+        break;
+    case OP_APERTURE:
+        r.h[H_LEN] = r.v[V_LEN];
+        for (int i = 0; i < 4; i++) r.h[H_XMIN + i] = r.v[V_XMIN + i];
+        break;
+    default: break;
+    }
+}
+
 int compile_line(const accel_elem_desc* d, int n, std::vector<DevElem>& out, std::string& err) {
     out.assign((size_t)n, DevElem{});
     for (int k = 0; k < n; k++) {
@@ -57,7 +83,8 @@ int compile_line(const accel_elem_desc* d, int n, std::vector<DevElem>& out, std
         std::memset(&r, 0, sizeof(r));
         r.elem = k;
         r.flags = e.flags;
-        r.nslice = e.nslice;
+        if (e.nslice > 32767) { err = "nslice above 32767"; return ACCEL_E_INVALID; }
+        r.nslice = (int16_t)e.nslice;
         r.v[V_LEN] = e.len;
         switch (e.type) {
         case ACCEL_MONITOR:
@@ -81,11 +108,14 @@ int compile_line(const accel_elem_desc* d, int n, std::vector<DevElem>& out, std
                 r.v[V_A + i] = e.poly_a[i];
                 r.v[V_B + i] = e.poly_b[i];
             }
-            r.order_lit = ACCEL_MAX_MPOLE - 1;  // accel.cpp:826,837-841
-            r.order_eff = highest_nonzero(e.poly_a, e.poly_b, ACCEL_MAX_MPOLE - 1);
-            bool skew = false;
-            for (int i = 0; i < ACCEL_MAX_MPOLE; i++) skew |= (e.poly_a[i] != 0.0);
-            r.flags = skew ? STR_SKEW : 0;
+            r.order_lit = (int8_t)(ACCEL_MAX_MPOLE - 1);  // accel.cpp:826,837-841
+            r.order_eff = (int8_t)highest_nonzero(e.poly_a, e.poly_b, ACCEL_MAX_MPOLE - 1);
+            bool skew = false, skew_hi = false;
+            for (int i = 0; i < ACCEL_MAX_MPOLE; i++) {
+                skew |= (e.poly_a[i] != 0.0);
+                if (i > 0) skew_hi |= (e.poly_a[i] != 0.0);
+            }
+            r.flags = skew ? (STR_SKEW | (skew_hi ? 0 : STR_SKEW0)) : 0;
             break;
         }
         case ACCEL_BENDMPOLE: {
@@ -111,8 +141,8 @@ int compile_line(const accel_elem_desc* d, int n, std::vector<DevElem>& out, std
             double uc_E0 = 0.665 * E0 * E0 / 1.0e6 / 2.99792458E8 * std::fabs(irho) * 1000;
             r.v[V_QECOEF] = 55 * std::sqrt(3.0) / 72.0 * uc_E0;
             for (int i = 0; i < ACCEL_MAX_MPOLE; i++) r.v[V_B + i] = e.poly_b[i];
-            r.order_lit = e.max_npole - 1;
-            r.order_eff = highest_nonzero(nullptr, e.poly_b, r.order_lit);
+            r.order_lit = (int8_t)(e.max_npole - 1);
+            r.order_eff = (int8_t)highest_nonzero(nullptr, e.poly_b, r.order_lit);
             r.v[V_BK1] = e.poly_b[1];                          // atpass.cpp:229 (read always)
             r.v[V_BK2] = (r.order_lit >= 2) ? e.poly_b[2] : 0;  // atpass.cpp:230-233
             r.flags = e.flags;                                  // radiation flag 0/1/2
@@ -182,6 +212,7 @@ int compile_line(const accel_elem_desc* d, int n, std::vector<DevElem>& out, std
             r.op = OP_NOP;
             break;
         }
+        fill_hot(r);
     }
     return ACCEL_OK;
 }

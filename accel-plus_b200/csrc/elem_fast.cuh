@@ -36,41 +36,47 @@ __device__ __forceinline__ void drift(St& s, double nl, double nlh) {
     s.z = fma(-nlh, q, s.z);
 }
 
-// straight multipole kick (atpass.cpp:358-414) at compile-time order M
-template <int M, bool SKEW>
+// Straight multipole kick (atpass.cpp:358-414) at compile-time order M.  SK is the skew level:
+// 0 no skew terms, 1 only A[0] (a skew dipole, e.g. the feed-down of a vertical offset),
+// 2 skew terms up to A[M].
+template <int M, int SK>
 __device__ __forceinline__ void kick(St& s, const double* A, const double* B, double K) {
-    double re = B[M];
-    double im = SKEW ? A[M] : 0.0;
+    if constexpr (M == 0) {
+        s.px = fma(-K, B[0], s.px);
+        if (SK) s.py = fma(K, A[0], s.py);
+    } else {
+        double re = B[M];
+        double im = (SK == 2) ? A[M] : 0.0;
 #pragma unroll
-    for (int i = M - 1; i >= 0; i--) {
-        double nre, nim;
-        if (!SKEW && i == M - 1) {
-            nre = fma(re, s.x, B[i]);
-            nim = re * s.y;
-        } else if (SKEW) {
-            nre = fma(re, s.x, fma(-im, s.y, B[i]));
-            nim = fma(im, s.x, fma(re, s.y, A[i]));
-        } else {
-            nre = fma(re, s.x, fma(-im, s.y, B[i]));
-            nim = fma(im, s.x, re * s.y);
+        for (int i = M - 1; i >= 0; i--) {
+            const bool first = (i == M - 1) && SK != 2;  // im is still exactly zero
+            const bool use_a = (SK == 2 || (SK == 1 && i == 0));
+            double nre, nim;
+            if (first) {
+                nre = fma(re, s.x, B[i]);
+                nim = use_a ? fma(re, s.y, A[i]) : re * s.y;
+            } else {
+                nre = fma(re, s.x, fma(-im, s.y, B[i]));
+                nim = use_a ? fma(im, s.x, fma(re, s.y, A[i])) : fma(im, s.x, re * s.y);
+            }
+            re = nre;
+            im = nim;
         }
-        re = nre;
-        im = nim;
+        s.px = fma(-K, re, s.px);
+        s.py = fma(K, im, s.py);
     }
-    s.px = fma(-K, re, s.px);
-    if (SKEW || M > 0) s.py = fma(K, im, s.py);
 }
 
-// AStrMPole::pass (accel.cpp:800-847), len > 0, effective order M.
-template <int M, bool SKEW>
+// AStrMPole::pass (accel.cpp:800-847), len > 0, effective order M, skew level SK.
+template <int M, int SK>
 __device__ __forceinline__ void strmpole(St& s, const DevElem* __restrict__ e) {
     double A[M + 1], B[M + 1];
 #pragma unroll
     for (int i = 0; i <= M; i++) {
-        B[i] = e->v[V_B + i];
-        A[i] = SKEW ? e->v[V_A + i] : 0.0;
+        B[i] = e->h[H_B + i];
+        A[i] = (SK == 2 || (SK == 1 && i == 0)) ? e->h[H_A + i] : 0.0;
     }
-    const double L1 = e->v[V_L1], L2 = e->v[V_L2], K1 = e->v[V_K1], K2 = e->v[V_K2];
+    const double L1 = e->h[H_L1], L2 = e->h[H_L2], K1 = e->h[H_K1], K2 = e->h[H_K2];
     const int ns = e->nslice;
     const double inv = rcp(1.0 + s.d);
     const double h = 0.5 * inv;
@@ -78,27 +84,32 @@ __device__ __forceinline__ void strmpole(St& s, const DevElem* __restrict__ e) {
     const double nlh1 = nl1 * h, nlh2 = nl2 * h;
     drift(s, nl1, nlh1);
     for (int m = 0; m < ns; m++) {
-        kick<M, SKEW>(s, A, B, K1);
+        kick<M, SK>(s, A, B, K1);
         drift(s, nl2, nlh2);
-        kick<M, SKEW>(s, A, B, K2);
+        kick<M, SK>(s, A, B, K2);
         drift(s, nl2, nlh2);
-        kick<M, SKEW>(s, A, B, K1);
+        kick<M, SK>(s, A, B, K1);
         if (m + 1 < ns) drift(s, 2.0 * nl1, 2.0 * nlh1);
     }
     drift(s, nl1, nlh1);
 }
 
+// flags: STR_SKEW set when any A is non-zero; STR_SKEW0 when A[0] is the only one.
 __device__ __forceinline__ void strmpole_dispatch(St& s, const DevElem* __restrict__ e) {
-    const bool skew = (e->flags & STR_SKEW) != 0;
-    switch (e->order_eff + (skew ? 16 : 0)) {
-    case 0: strmpole<0, false>(s, e); break;
-    case 1: strmpole<1, false>(s, e); break;
-    case 2: strmpole<2, false>(s, e); break;
-    case 3: strmpole<3, false>(s, e); break;
-    case 16: strmpole<0, true>(s, e); break;
-    case 17: strmpole<1, true>(s, e); break;
-    case 18: strmpole<2, true>(s, e); break;
-    case 19: strmpole<3, true>(s, e); break;
+    const int sk = (e->flags & STR_SKEW) ? ((e->flags & STR_SKEW0) ? 1 : 2) : 0;
+    switch (e->order_eff * 4 + sk) {
+    case 0: strmpole<0, 0>(s, e); break;
+    case 1: strmpole<0, 1>(s, e); break;
+    case 2: strmpole<0, 2>(s, e); break;
+    case 4: strmpole<1, 0>(s, e); break;
+    case 5: strmpole<1, 1>(s, e); break;
+    case 6: strmpole<1, 2>(s, e); break;
+    case 8: strmpole<2, 0>(s, e); break;
+    case 9: strmpole<2, 1>(s, e); break;
+    case 10: strmpole<2, 2>(s, e); break;
+    case 12: strmpole<3, 0>(s, e); break;
+    case 13: strmpole<3, 1>(s, e); break;
+    case 14: strmpole<3, 2>(s, e); break;
     default: s = rare_elem(s, e, 0, 0, 0); break;
     }
 }
@@ -156,8 +167,17 @@ struct BkCoef {
     double cI, cR1, cR2;           // radiation: h(K1 h - K2)/6, -K1 h/2, h(K1 h - K2)/2
 };
 
+// With K1 = K2 = 0 (a pure dipole field plus B[0..M]) the curved kick reduces to
+// px -= L (re + h (h x - delta)), py += L im, z -= L h x.
+template <bool PURE>
 __device__ __forceinline__ void bend_kick_core(St& s, const BkCoef& c, double re, double im,
                                                double L) {
+    if (PURE) {
+        s.px = fma(-L, fma(c.h, fma(c.h, s.x, -s.d), re), s.px);
+        s.py = fma(L, im, s.py);
+        s.z = fma(-L * c.h, s.x, s.z);
+        return;
+    }
     double x = s.x, y = s.y;
     double x2 = x * x, y2 = y * y;
     double t1 = fma(c.h, x, fma(c.K1, fma(-0.5, y2, x2), c.K2 * x * fma(-4.0 / 3.0, y2, x2)));
@@ -168,16 +188,21 @@ __device__ __forceinline__ void bend_kick_core(St& s, const BkCoef& c, double re
     s.z = fma(-L * c.h, x, s.z);
 }
 
-// bndthinkickrad (atpass.cpp:255-339); returns the new 1/(1+delta) for the following drift
-template <int M, int RAD>
+// bndthinkickrad (atpass.cpp:255-339); returns the new 1/(1+delta) for the following drift.
+// The energy loss per kick D is tiny (|D/(1+delta)| ~ 1e-7), so the new inverse is the old one
+// times 1/(1-u), u = D/(1+delta), summed to u^3 (truncation below 1e-20 relative); a loss
+// above |u| = 1e-4 takes the exact reciprocal.
+template <int M, int RAD, bool PURE>
 __device__ __forceinline__ double bend_kick_rad(St& s, const double* B, const BkCoef& c, double L,
                                                 double crad, double qec, double inv, double gauss) {
     double re, im;
     horner_b<M>(s, B, re, im);
     double x = s.x, y = s.y, y2 = y * y;
     double xpr = s.px * inv, ypr = s.py * inv;
-    im = fma(c.cI, y2 * y, im);
-    re = fma(y2, fma(c.cR2, x, c.cR1), re);
+    if (!PURE) {
+        im = fma(c.cI, y2 * y, im);
+        re = fma(y2, fma(c.cR2, x, c.cR1), re);
+    }
     double hx1 = fma(x, c.h, 1.0);
     double vq = fma(xpr, xpr, ypr * ypr);
     double vn2 = rcp(fma(hx1, hx1, vq));
@@ -186,39 +211,43 @@ __device__ __forceinline__ double bend_kick_rad(St& s, const double* B, const Bk
     double b2p = fma(by * hx1, by * hx1, fma(bx * hx1, bx * hx1, cr * cr)) * vn2;
     double opd = 1.0 + s.d;
     double mean = crad * (opd * opd) * b2p * fma(0.5, vq, hx1) * L;
+    double loss;
     if (RAD == 1) {
-        s.d = s.d - mean;
+        loss = mean;
     } else {
         double sig = sqrt(fabs(qec * mean));
-        s.d = s.d - fma(gauss, sig, mean);
+        loss = fma(gauss, sig, mean);
     }
+    s.d = s.d - loss;
     double opd2 = 1.0 + s.d;
     s.px = xpr * opd2;
     s.py = ypr * opd2;
-    bend_kick_core(s, c, re, im, L);
+    bend_kick_core<PURE>(s, c, re, im, L);
+    const double u = loss * inv;  // 1/(1+d-D) = inv (1 + u + u^2 + u^3 + ...)
+    if (fabs(u) < 1e-4) return fma(inv * u, fma(u, u, u) + 1.0, inv);
     return rcp(opd2);
 }
 
-template <int M>
+template <int M, bool PURE>
 __device__ __forceinline__ void bendmpole(St& s, const DevElem* __restrict__ e,
                                           uint64_t seed, uint32_t pid, uint32_t turn) {
     double B[M + 1];
 #pragma unroll
-    for (int i = 0; i <= M; i++) B[i] = e->v[V_B + i];
+    for (int i = 0; i <= M; i++) B[i] = e->h[H_BB + i];
     const int rad = e->flags;
     const int ns = e->nslice;
     BkCoef c;
-    c.h = e->v[V_IRHO];
-    c.K1 = e->v[V_BK1];
-    c.K2 = e->v[V_BK2];
+    c.h = e->h[H_IRHO];
+    c.K1 = e->h[H_BK1];
+    c.K2 = e->h[H_BK2];
     c.c43K2 = 4.0 / 3.0 * c.K2;
     c.c3 = c.h / 6.0 * c.K1 - c.K2 / 3.0;
     double kh = c.K1 * c.h - c.K2;
     c.cI = c.h * kh / 6.0;
     c.cR1 = -c.K1 * c.h / 2.0;
     c.cR2 = c.h * kh / 2.0;
-    const double L1 = e->v[V_L1], L2 = e->v[V_L2], K1 = e->v[V_K1], K2 = e->v[V_K2];
-    const double psi1 = e->v[V_PSI1], psi2 = e->v[V_PSI2];
+    const double L1 = e->h[H_L1], L2 = e->h[H_L2], K1 = e->h[H_K1], K2 = e->h[H_K2];
+    const double psi1 = e->h[H_PSI1], psi2 = e->h[H_PSI2];
     s.px = fma(s.x, psi1, s.px);
     s.py = fma(-s.y, psi1, s.py);
     if (rad == 0) {
@@ -227,33 +256,33 @@ __device__ __forceinline__ void bendmpole(St& s, const DevElem* __restrict__ e,
         for (int m = 0; m < ns; m++) {
             double re, im;
             hxdrift(s, c.h, k1);
-            horner_b<M>(s, B, re, im); bend_kick_core(s, c, re, im, K1);
+            horner_b<M>(s, B, re, im); bend_kick_core<PURE>(s, c, re, im, K1);
             hxdrift(s, c.h, k2);
-            horner_b<M>(s, B, re, im); bend_kick_core(s, c, re, im, K2);
+            horner_b<M>(s, B, re, im); bend_kick_core<PURE>(s, c, re, im, K2);
             hxdrift(s, c.h, k2);
-            horner_b<M>(s, B, re, im); bend_kick_core(s, c, re, im, K1);
+            horner_b<M>(s, B, re, im); bend_kick_core<PURE>(s, c, re, im, K1);
             hxdrift(s, c.h, k1);
         }
     } else if (rad == 1) {
-        const double crad = e->v[V_CRAD];
+        const double crad = e->h[H_CRAD];
         double inv = rcp(1.0 + s.d);
         for (int m = 0; m < ns; m++) {
             hxdrift(s, c.h, hx_coef(L1, c.h, inv));
-            inv = bend_kick_rad<M, 1>(s, B, c, K1, crad, 0.0, inv, 0.0);
+            inv = bend_kick_rad<M, 1, PURE>(s, B, c, K1, crad, 0.0, inv, 0.0);
             hxdrift(s, c.h, hx_coef(L2, c.h, inv));
-            inv = bend_kick_rad<M, 1>(s, B, c, K2, crad, 0.0, inv, 0.0);
+            inv = bend_kick_rad<M, 1, PURE>(s, B, c, K2, crad, 0.0, inv, 0.0);
             hxdrift(s, c.h, hx_coef(L2, c.h, inv));
-            inv = bend_kick_rad<M, 1>(s, B, c, K1, crad, 0.0, inv, 0.0);
+            inv = bend_kick_rad<M, 1, PURE>(s, B, c, K1, crad, 0.0, inv, 0.0);
             hxdrift(s, c.h, hx_coef(L1, c.h, inv));
         }
     } else {
-        const double crad = e->v[V_CRAD], qec = e->v[V_QECOEF], SL = e->v[V_SL];
+        const double crad = e->h[H_CRAD], qec = e->v[V_QECOEF], SL = e->v[V_SL];
         const double hs = 0.5 * SL;
         double inv = rcp(1.0 + s.d);
         for (int m = 0; m < ns; m++) {
             hxdrift(s, c.h, hx_coef(hs, c.h, inv));
             double g = qe_normal(seed, pid, turn, (uint32_t)e->elem, (uint32_t)m);
-            inv = bend_kick_rad<M, 2>(s, B, c, SL, crad, qec, inv, g);
+            inv = bend_kick_rad<M, 2, PURE>(s, B, c, SL, crad, qec, inv, g);
             hxdrift(s, c.h, hx_coef(hs, c.h, inv));
         }
     }
@@ -263,11 +292,17 @@ __device__ __forceinline__ void bendmpole(St& s, const DevElem* __restrict__ e,
 
 __device__ __forceinline__ void bendmpole_dispatch(St& s, const DevElem* __restrict__ e,
                                                    uint64_t seed, uint32_t pid, uint32_t turn) {
-    switch (e->order_eff) {
-    case 0: bendmpole<0>(s, e, seed, pid, turn); break;
-    case 1: bendmpole<1>(s, e, seed, pid, turn); break;
-    case 2: bendmpole<2>(s, e, seed, pid, turn); break;
-    case 3: bendmpole<3>(s, e, seed, pid, turn); break;
+    // h carries B[0..3]: orders above kHotOrder go out of line
+    const bool pure = e->h[H_BK1] == 0.0 && e->h[H_BK2] == 0.0;
+    switch (e->order_eff * 2 + (pure ? 1 : 0)) {
+    case 0: bendmpole<0, false>(s, e, seed, pid, turn); break;
+    case 1: bendmpole<0, true>(s, e, seed, pid, turn); break;
+    case 2: bendmpole<1, false>(s, e, seed, pid, turn); break;
+    case 3: bendmpole<1, true>(s, e, seed, pid, turn); break;
+    case 4: bendmpole<2, false>(s, e, seed, pid, turn); break;
+    case 5: bendmpole<2, true>(s, e, seed, pid, turn); break;
+    case 6: bendmpole<3, false>(s, e, seed, pid, turn); break;
+    case 7: bendmpole<3, true>(s, e, seed, pid, turn); break;
     default: s = rare_elem(s, e, seed, pid, turn); break;
     }
 }
@@ -280,14 +315,14 @@ __device__ __forceinline__ void drift_elem(St& s, double len) {
 }
 
 __device__ __forceinline__ void cavity(St& s, const DevElem* __restrict__ e) {
-    const double len = e->v[V_LEN];
+    const double len = e->h[H_LEN];
     if (len != 0) drift_elem(s, 0.5 * len);
-    if (e->flags) s.d = fma(e->v[V_NV], sin(fma(e->v[V_KZ], s.z, e->v[V_PHIS])), s.d);
+    if (e->flags) s.d = fma(e->h[H_NV], sin(fma(e->h[H_KZ], s.z, e->h[H_PHIS])), s.d);
     if (len != 0) drift_elem(s, 0.5 * len);
 }
 
 __device__ __forceinline__ bool aperture_hit(St& s, const DevElem* __restrict__ e) {
-    const double a = e->v[V_XMIN], b = e->v[V_XMAX], c = e->v[V_YMIN], d = e->v[V_YMAX];
+    const double a = e->h[H_XMIN], b = e->h[H_XMAX], c = e->h[H_YMIN], d = e->h[H_YMAX];
     if (s.x <= a || s.x >= b || s.y <= c || s.y >= d) {
         s.z = (double)((s.x <= a) * 1 + (s.x >= b) * 2 + (s.y <= c) * 3 + (s.y >= d) * 4);
         s.x = __longlong_as_double(0x7ff8000000000000ll);
@@ -298,8 +333,8 @@ __device__ __forceinline__ bool aperture_hit(St& s, const DevElem* __restrict__ 
 
 __device__ __forceinline__ void aperture(St& s, const DevElem* __restrict__ e) {
     if (aperture_hit(s, e)) return;
-    if (e->v[V_LEN] != 0) {
-        drift_elem(s, e->v[V_LEN]);
+    if (e->h[H_LEN] != 0) {
+        drift_elem(s, e->h[H_LEN]);
         aperture_hit(s, e);
     }
 }

@@ -36,15 +36,29 @@ enum DevOp : int32_t {
 
 struct alignas(128) DevElem {
     int32_t op;
-    int32_t nslice;
-    int32_t order_eff;  // highest non-zero multipole index (exact Horner start for finite input)
-    int32_t order_lit;  // the order the reference loops from (9 for StrMPole, MaxNPole-1 bends)
+    int16_t nslice;
+    int8_t order_eff;   // highest non-zero multipole index (exact Horner start for finite input)
+    int8_t order_lit;   // the order the reference loops from (9 for StrMPole, MaxNPole-1 bends)
     int32_t flags;      // rad flag, on/off, skew-present bit (STR_SKEW)
     int32_t elem;       // element index in the line
-    int32_t pad0, pad1;
-    double v[44];
+    double h[14];       // hot payload: everything the fused kernel reads, in the first 128 B line
+    double v[44];       // literal payload (plain kernel, tangent map, rare elements)
+    double pad[4];
 };
-static_assert(sizeof(DevElem) == 384, "DevElem must be 384 bytes");
+static_assert(sizeof(DevElem) == 512, "DevElem must be 512 bytes");
+static_assert(offsetof(DevElem, v) == 128, "the hot payload must fill exactly the first line");
+
+// hot payload slots (DevElem::h)
+enum : int {
+    H_LEN = 0,                                       // Drift, Cavity, Aperture
+    H_L1 = 0, H_L2 = 1, H_K1 = 2, H_K2 = 3,          // StrMPole, BendMPole
+    H_A = 4, H_B = 8,                                // StrMPole A[0..3], B[0..3]
+    H_IRHO = 4, H_PSI1 = 5, H_PSI2 = 6, H_CRAD = 7,  // BendMPole
+    H_BK1 = 8, H_BK2 = 9, H_BB = 10,                 // BendMPole K1, K2, B[0..3] at h[10..13]
+    H_NV = 1, H_KZ = 2, H_PHIS = 3,                  // Cavity
+    H_XMIN = 1, H_XMAX = 2, H_YMIN = 3, H_YMAX = 4,  // Aperture
+};
+constexpr int kHotOrder = 3;  // specialised multipole orders 0..3 read their coefficients from h
 
 // payload slots
 enum : int {
@@ -74,7 +88,7 @@ enum : int {
     V_W = 1,
 };
 
-enum : int32_t { STR_SKEW = 1 << 8 };
+enum : int32_t { STR_SKEW = 1 << 8, STR_SKEW0 = 1 << 9 };  // any A non-zero; only A[0]
 
 // ------------------------------------------------------------------------------------------
 // Host-side error plumbing

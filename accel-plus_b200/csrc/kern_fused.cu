@@ -40,7 +40,7 @@ __device__ __forceinline__ void fused_elem(fast::St& s, const DevElem* __restric
                                            uint32_t pid, uint32_t turn) {
     switch (e->op) {
     case OP_NOP: break;
-    case OP_DRIFT: fast::drift_elem(s, e->v[V_LEN]); break;
+    case OP_DRIFT: fast::drift_elem(s, e->h[H_LEN]); break;
     case OP_STRMPOLE: fast::strmpole_dispatch(s, e); break;
     case OP_STRKICK: s = fast::rare_elem(s, e, seed, pid, turn); break;
     case OP_BENDMPOLE: fast::bendmpole_dispatch(s, e, seed, pid, turn); break;
@@ -83,6 +83,9 @@ __global__ void __launch_bounds__(BS, MINB) k_fused(const TrackParams P) {
             if (alive) {
                 const uint32_t rt = (uint32_t)(rbase + P.rng_turn0 + t);
                 for (int e = P.e0; e < P.e1; e++) {
+                    // pull the next element's parameter line into L1 while this one computes
+                    const DevElem* nx = T + (e + 1 < P.e1 ? e + 1 : P.e0);
+                    asm volatile("prefetch.global.L1 [%0];" ::"l"(nx));
                     fused_elem(s, T + e, P.seed, (uint32_t)p, rt);
                     if (nan_(s.x)) break;
                 }

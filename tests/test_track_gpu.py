@@ -102,9 +102,10 @@ def test_dba_grid_loss_turns(A, ctx, O, G, LT, mode):
     err = rel_err_each(r[sv.regular], G["dba_grid_out"][sv.regular], sv.scale)
     assert np.max(err) < 1e-9, np.max(err)
     # lost particles carry the reference's aperture code in z and NaN in x
-    same_loss = (lt >= 0) & (lt == ref_lt)
+    # (a particle that overflows to NaN before reaching the aperture carries NaN there instead)
+    same_loss = (lt >= 0) & (lt == ref_lt) & ~sv.boundary
     assert np.all(np.isnan(r[lt >= 0, 0]))
-    assert np.array_equal(r[same_loss, 4], G["dba_grid_out"][same_loss, 4])
+    assert np.array_equal(r[same_loss, 4], G["dba_grid_out"][same_loss, 4], equal_nan=True)
 
 
 @pytest.mark.parametrize("mode", ["plain", "fused"])
