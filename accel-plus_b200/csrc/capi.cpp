@@ -140,7 +140,7 @@ struct CoreReq {
     int64_t ntot;
     int32_t* loss;
     int e0, e1, nturn, mode;
-    int variant, seg;
+    int variant, seg, sched;
     bool probe;  // autotuning probe: no RNG advance bookkeeping
 };
 
@@ -203,6 +203,7 @@ static int emit_part(accel_ctx* C, const CoreReq& q, int part, int turns, cudaSt
     P.rng_base = (int32_t*)L0->d_rng.p;
     P.turn0 = 0;
     P.rng_turn0 = 0;
+    P.sched = q.sched;
     if (part == PART_PRE) {
         launch_init_live(q.st, q.ntot, q.loss, live, cnt + 0, cnt + 2, 1, s);
         launch_fill_i32(cnt + 3, 0, 1, s);
@@ -335,7 +336,7 @@ static int run_core(accel_ctx* C, const CoreReq& q, cudaStream_t user) {
     } else {
         GraphKey key;
         key.v = {(int64_t)q.mode, (int64_t)q.ninst, q.ntot, (int64_t)q.e0, (int64_t)q.e1, (int64_t)q.nturn,
-                 (int64_t)q.variant, (int64_t)plan.seg, (int64_t)(intptr_t)q.st, (int64_t)(intptr_t)q.loss,
+                 (int64_t)q.variant, (int64_t)plan.seg, (int64_t)q.sched, (int64_t)(intptr_t)q.st, (int64_t)(intptr_t)q.loss,
                  (int64_t)(intptr_t)q.tables, (int64_t)(intptr_t)q.tbl_off, (int64_t)(intptr_t)q.pinst,
                  (int64_t)q.probe, (int64_t)(intptr_t)C->live0.p, (int64_t)(intptr_t)C->cnt.p,
                  (int64_t)(intptr_t)C->scratch.p, (int64_t)(intptr_t)C->iscratch.p};
@@ -375,9 +376,10 @@ static int run_core(accel_ctx* C, const CoreReq& q, cudaStream_t user) {
     return ACCEL_OK;
 }
 
-static void default_tile(accel_ctx* C, int& variant, int& seg) {
+static void default_tile(accel_ctx* C, int& variant, int& seg, int& sched) {
     variant = C->tile_variant >= 0 ? C->tile_variant : 0;
     seg = C->tile_seg > 0 ? C->tile_seg : 16;
+    sched = C->tile_sched >= 0 ? C->tile_sched : 0;
 }
 
 // ------------------------------------------------------------------------------------------
@@ -630,9 +632,11 @@ int accel_track(accel_line* L, double* r, int layout, int N, int st, int ed, int
     q.e1 = ed;
     q.nturn = nturn;
     q.mode = mode;
-    default_tile(C, q.variant, q.seg);
+    default_tile(C, q.variant, q.seg, q.sched);
     auto tk = C->tuned.find(tune_key(lines, 1, N, nturn));
-    if (tk != C->tuned.end() && C->tile_variant < 0) { q.variant = tk->second.first; q.seg = tk->second.second; }
+    if (tk != C->tuned.end() && C->tile_variant < 0) {
+        q.variant = tk->second[0]; q.seg = tk->second[1]; q.sched = tk->second[2];
+    }
     if ((s = run_core(C, q, user))) return s;
     if (dev_in) launch_soa_to_aos(soa, dev_in, N, user);
     if (!rdev) {
@@ -730,9 +734,11 @@ int accel_track_batched(accel_line* const* lines, int ninst, const int64_t* part
     q.e1 = (int)lines[0]->desc.size();
     q.nturn = nturn;
     q.mode = mode;
-    default_tile(C, q.variant, q.seg);
+    default_tile(C, q.variant, q.seg, q.sched);
     auto tk = C->tuned.find(tune_key(lines, ninst, ntot, nturn));
-    if (tk != C->tuned.end() && C->tile_variant < 0) { q.variant = tk->second.first; q.seg = tk->second.second; }
+    if (tk != C->tuned.end() && C->tile_variant < 0) {
+        q.variant = tk->second[0]; q.seg = tk->second[1]; q.sched = tk->second[2];
+    }
     if ((s = run_core(C, q, user))) return s;
     CK(cudaGetLastError());
     return ACCEL_OK;
@@ -765,9 +771,10 @@ int accel_autotune(accel_line* const* lines, int ninst, const int64_t* part_off,
     q.e1 = (int)lines[0]->desc.size();
     q.mode = ACCEL_MODE_FUSED;
     q.probe = true;
-    auto time_it = [&](int variant, int seg, int turns, float* ms) -> int {
+    auto time_it = [&](int variant, int seg, int sched, int turns, float* ms) -> int {
         q.variant = variant;
         q.seg = seg;
+        q.sched = sched;
         q.nturn = turns;
         CK(cudaMemcpyAsync(q.st, r_soa, nb, cudaMemcpyDeviceToDevice, C->stream));
         int st2 = run_core(C, q, C->stream);  // builds the (untimed) graphs on first use
@@ -785,26 +792,27 @@ int accel_autotune(accel_line* const* lines, int ninst, const int64_t* part_off,
         cudaEventDestroy(b);
         return st2;
     };
-    int best_v = 0;
+    int best_v = 0, best_sched = 0;
     float best = 1e30f;
-    for (int v = 0; v < kNumFusedVariants; v++) {
-        float ms = 0;
-        if ((s = time_it(v, 4, 4, &ms))) return s;
-        if (ms < best) { best = ms; best_v = v; }
-    }
+    for (int sched = 0; sched < kNumSched; sched++)
+        for (int v = 0; v < kNumFusedVariants; v++) {
+            float ms = 0;
+            if ((s = time_it(v, 4, sched, 4, &ms))) return s;
+            if (ms < best) { best = ms; best_v = v; best_sched = sched; }
+        }
     int best_seg = 16;
     best = 1e30f;
-    for (int seg : {2, 8, 32, 128}) {
+    for (int seg : {1, 2, 4, 8, 32}) {
         float ms = 0;
-        if ((s = time_it(best_v, seg, 128, &ms))) return s;
+        if ((s = time_it(best_v, seg, best_sched, 64, &ms))) return s;
         if (ms < best * 0.98f) { best = ms; best_seg = seg; }
     }
     C->graphs.clear();
-    C->tuned[tune_key(lines, ninst, ntot, -1)] = {best_v, best_seg};
+    C->tuned[tune_key(lines, ninst, ntot, -1)] = {best_v, best_seg, best_sched};
     if (tile_out3) {
         tile_out3[0] = fused_variant_info(best_v).block;
         tile_out3[1] = best_seg;
-        tile_out3[2] = best_v;
+        tile_out3[2] = best_v + 100 * best_sched;
     }
     return ACCEL_OK;
 }
@@ -812,7 +820,10 @@ int accel_autotune(accel_line* const* lines, int ninst, const int64_t* part_off,
 int accel_set_tile(accel_ctx* C, int block, int seg_turns, int variant) {
     if (!C) return fail(ACCEL_E_INVALID, "NULL ctx");
     std::lock_guard<std::mutex> lk(C->mu);
-    if (variant >= kNumFusedVariants) return fail(ACCEL_E_INVALID, "variant out of range");
+    int sched = -1;
+    if (variant >= 100) { sched = variant / 100; variant %= 100; }
+    if (variant >= kNumFusedVariants || sched >= kNumSched) return fail(ACCEL_E_INVALID, "variant out of range");
+    C->tile_sched = sched;
     if (variant < 0 && block > 0) {
         for (int v = 0; v < kNumFusedVariants; v++)
             if (fused_variant_info(v).block == block) { variant = v; break; }
@@ -825,11 +836,11 @@ int accel_set_tile(accel_ctx* C, int block, int seg_turns, int variant) {
 
 int accel_get_tile(accel_ctx* C, int* t) {
     if (!C || !t) return fail(ACCEL_E_INVALID, "NULL argument");
-    int v, s;
-    default_tile(C, v, s);
+    int v, s, sc;
+    default_tile(C, v, s, sc);
     t[0] = fused_variant_info(v).block;
     t[1] = s;
-    t[2] = v;
+    t[2] = v + 100 * sc;
     return ACCEL_OK;
 }
 

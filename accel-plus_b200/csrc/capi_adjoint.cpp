@@ -1,11 +1,263 @@
-// capi_adjoint.cpp — adjoint C-ABI (filled in with the adjoint pair).
+// capi_adjoint.cpp — the forward/backward C-ABI pair of the adjoint.
+//
+// accel_adjoint_forward tracks N particles for nturn turns (literal maps, effective Horner order),
+// keeping the state at every ckpt_every-th turn.  accel_adjoint_backward then walks the segments
+// last to first: recompute the segment's turn-start states from its checkpoint, and reverse its
+// turns last to first (kern_adjoint.cu).  Memory on the device: (nseg + K + ne + 3) x 6 x N
+// doubles for checkpoints, the turn tape, the element tape, state, adjoint and scratch.
+//
+// Parameters are (element, field, index) triples: StrMPole PolynomB/PolynomA[index] (field K on a
+// StrMPole is PolynomB[1]), Quad K.  The line must be free of radiation, quantum excitation and
+// wake elements (their maps are not differentiated): ACCEL_E_UNSUPPORTED otherwise.
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <numeric>
+#include <string>
+#include <vector>
+#include "adjoint_params.h"
 #include "engine.h"
+#include "kernels.h"
 #include "runtime.h"
+
 using namespace accel;
-struct accel_adjoint { int dummy; };
-extern "C" {
-int accel_adjoint_create(accel_line*, int, int, int, const int32_t*, const int32_t*, const int32_t*, int, accel_adjoint**) { return fail(ACCEL_E_UNSUPPORTED, "adjoint not built"); }
-int accel_adjoint_destroy(accel_adjoint*) { return ACCEL_OK; }
-int accel_adjoint_forward(accel_adjoint*, const double*, double*) { return fail(ACCEL_E_UNSUPPORTED, "adjoint not built"); }
-int accel_adjoint_backward(accel_adjoint*, const double*, double*, double*) { return fail(ACCEL_E_UNSUPPORTED, "adjoint not built"); }
+
+#define CK(call)                                                                               \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess)                                                                 \
+            return fail(ACCEL_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));     \
+    } while (0)
+
+namespace {
+constexpr int kMaxAdjParams = 2048;
+
+bool dev_ptr(const void* p) {
+    cudaPointerAttributes a;
+    if (!p || cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
 }
+}  // namespace
+
+struct accel_adjoint {
+    accel_line* line = nullptr;
+    int n = 0, nturn = 0, every = 1, nseg = 0, ne = 0, nparam = 0;
+    std::vector<int> order;  // caller's parameter j -> sorted position
+    std::vector<int32_t> pfirst, pcount, pkind, pindex;
+    DevBuf st, lam, aos, tape, ckpt, turn_tape, part, meta, final_x, grad;
+    bool have_forward = false;
+    ~accel_adjoint() {
+        for (DevBuf* b : {&st, &lam, &aos, &tape, &ckpt, &turn_tape, &part, &meta, &final_x, &grad}) b->release();
+    }
+};
+
+static AdjParams params_of(accel_adjoint* J) {
+    AdjParams a{};
+    a.tbl = (const DevElem*)J->line->d_tbl.p;
+    a.ne = J->ne;
+    a.n = J->n;
+    a.st = (double*)J->st.p;
+    a.lam = (double*)J->lam.p;
+    a.tape = (double*)J->tape.p;
+    a.pgrad_part = (double*)J->part.p;
+    int32_t* m = (int32_t*)J->meta.p;
+    a.pfirst = m;
+    a.pcount = m + J->ne;
+    a.pkind = m + 2 * J->ne;
+    a.pindex = m + 2 * J->ne + std::max(1, J->nparam);
+    a.nparam = J->nparam;
+    return a;
+}
+
+extern "C" {
+
+int accel_adjoint_create(accel_line* L, int N, int nturn, int every, const int32_t* pe,
+                         const int32_t* pf, const int32_t* pi, int nparam, accel_adjoint** out) {
+    if (!L || !out || N <= 0 || nturn <= 0 || every <= 0 || nparam < 0) return fail(ACCEL_E_INVALID, "bad argument");
+    if (nparam > 0 && (!pe || !pf || !pi)) return fail(ACCEL_E_INVALID, "parameter arrays are NULL");
+    if (nparam > kMaxAdjParams) return fail(ACCEL_E_TOO_LARGE, "more than 2048 parameters");
+    accel_ctx* C = L->ctx;
+    std::lock_guard<std::mutex> lk(C->mu);
+    CK(cudaSetDevice(C->device));
+    int s = line_sync(L);
+    if (s) return s;
+    const int ne = (int)L->desc.size();
+    for (int k = 0; k < ne; k++) {
+        const accel_elem_desc& d = L->desc[k];
+        if (!is_supported(d.type)) return fail(ACCEL_E_UNSUPPORTED, std::string("element ") + d.famname + " is not implemented");
+        if (is_collective(d.type)) return fail(ACCEL_E_UNSUPPORTED, "the adjoint does not differentiate wake elements");
+        if (d.type == ACCEL_BENDMPOLE && d.flags != 0) return fail(ACCEL_E_UNSUPPORTED, "the adjoint needs radiation off");
+        if (d.type == ACCEL_SYNCRAD && d.flags != 0) return fail(ACCEL_E_UNSUPPORTED, "the adjoint needs SyncRad off");
+    }
+    std::unique_ptr<accel_adjoint> J(new accel_adjoint());
+    J->line = L;
+    J->n = N;
+    J->nturn = nturn;
+    J->every = every;
+    J->nseg = (nturn + every - 1) / every;
+    J->ne = ne;
+    J->nparam = nparam;
+    // parameters, stably sorted by element
+    struct P { int elem, kind, index, orig; };
+    std::vector<P> ps;
+    for (int j = 0; j < nparam; j++) {
+        const int e = pe[j];
+        if (e < 0 || e >= ne) return fail(ACCEL_E_INVALID, "parameter element out of range");
+        const accel_elem_desc& d = L->desc[e];
+        P p{e, 0, pi[j], j};
+        if (d.type == ACCEL_STRMPOLE && (pf[j] == ACCEL_F_POLYNOMB || pf[j] == ACCEL_F_POLYNOMA)) {
+            if (pi[j] < 0 || pi[j] >= ACCEL_MAX_MPOLE) return fail(ACCEL_E_INVALID, "multipole index outside 0..9");
+            p.kind = pf[j] == ACCEL_F_POLYNOMB ? adj::PK_B : adj::PK_A;
+        } else if (d.type == ACCEL_STRMPOLE && pf[j] == ACCEL_F_K) {
+            p.kind = adj::PK_B;
+            p.index = 1;
+        } else if (d.type == ACCEL_QUAD && pf[j] == ACCEL_F_K) {
+            p.kind = adj::PK_QUADK;
+            p.index = 0;
+        } else {
+            return fail(ACCEL_E_UNSUPPORTED, std::string("no gradient for this field of ") + d.famname);
+        }
+        ps.push_back(p);
+    }
+    std::stable_sort(ps.begin(), ps.end(), [](const P& a, const P& b) { return a.elem < b.elem; });
+    J->order.assign((size_t)nparam, 0);
+    J->pfirst.assign((size_t)ne, 0);
+    J->pcount.assign((size_t)ne, 0);
+    for (int j = 0; j < nparam; j++) {
+        J->order[(size_t)ps[(size_t)j].orig] = j;
+        J->pkind.push_back(ps[(size_t)j].kind);
+        J->pindex.push_back(ps[(size_t)j].index);
+        J->pcount[(size_t)ps[(size_t)j].elem]++;
+    }
+    for (int e = 0, acc = 0; e < ne; e++) {
+        J->pfirst[(size_t)e] = acc;
+        acc += J->pcount[(size_t)e];
+        if (J->pcount[(size_t)e] > adj::kMaxParamsPerElem)
+            return fail(ACCEL_E_TOO_LARGE, "more than 4 parameters on one element");
+    }
+    // a StrMPole parameter beyond the element's effective order still needs its Horner terms:
+    // the gradient of B_n at a zero coefficient is the derivative of the zero term
+    for (const P& p : ps) {
+        if (p.kind == adj::PK_QUADK) continue;
+        DevElem& r = L->host_tbl[(size_t)p.elem];
+        if (p.index > r.order_eff) {
+            r.order_eff = (int8_t)p.index;
+            if (p.kind == adj::PK_A) r.flags |= STR_SKEW, r.flags &= ~STR_SKEW0;
+        }
+    }
+    CK(cudaMemcpy(L->d_tbl.p, L->host_tbl.data(), L->host_tbl.size() * sizeof(DevElem), cudaMemcpyHostToDevice));
+    const size_t s6 = sizeof(double) * 6 * (size_t)N;
+    int nblk = adj_blocks(N);
+    if ((s = J->st.ensure(s6)) || (s = J->lam.ensure(s6)) || (s = J->aos.ensure(s6)) ||
+        (s = J->tape.ensure(s6 * (size_t)ne)) || (s = J->ckpt.ensure(s6 * (size_t)J->nseg)) ||
+        (s = J->turn_tape.ensure(s6 * (size_t)std::min(every, nturn))) ||
+        (s = J->part.ensure(sizeof(double) * (size_t)std::max(1, nblk * nparam))) ||
+        (s = J->meta.ensure(sizeof(int32_t) * (size_t)(2 * ne + 2 * std::max(1, nparam)))) ||
+        (s = J->final_x.ensure(sizeof(double) * (size_t)N)) ||
+        (s = J->grad.ensure(sizeof(double) * (size_t)std::max(1, nparam))))
+        return s;
+    std::vector<int32_t> meta((size_t)(2 * ne + 2 * std::max(1, nparam)), 0);
+    std::copy(J->pfirst.begin(), J->pfirst.end(), meta.begin());
+    std::copy(J->pcount.begin(), J->pcount.end(), meta.begin() + ne);
+    std::copy(J->pkind.begin(), J->pkind.end(), meta.begin() + 2 * ne);
+    std::copy(J->pindex.begin(), J->pindex.end(), meta.begin() + 2 * ne + std::max(1, nparam));
+    CK(cudaMemcpy(J->meta.p, meta.data(), meta.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+    *out = J.release();
+    return ACCEL_OK;
+}
+
+int accel_adjoint_destroy(accel_adjoint* J) {
+    if (!J) return ACCEL_OK;
+    std::lock_guard<std::mutex> lk(J->line->ctx->mu);
+    cudaSetDevice(J->line->ctx->device);
+    cudaStreamSynchronize(J->line->ctx->stream);
+    J->line->dirty = true;  // the table was widened for parameter orders; rebuild on next use
+    delete J;
+    return ACCEL_OK;
+}
+
+int accel_adjoint_forward(accel_adjoint* J, const double* r0, double* r_final) {
+    if (!J || !r0 || !r_final) return fail(ACCEL_E_INVALID, "NULL argument");
+    accel_ctx* C = J->line->ctx;
+    std::lock_guard<std::mutex> lk(C->mu);
+    CK(cudaSetDevice(C->device));
+    if (J->line->dirty) return fail(ACCEL_E_INVALID, "the line changed after accel_adjoint_create");
+    cudaStream_t s = C->stream;
+    const size_t s6 = sizeof(double) * 6 * (size_t)J->n;
+    const double* in = r0;
+    if (!dev_ptr(r0)) {
+        CK(cudaMemcpyAsync(J->aos.p, r0, s6, cudaMemcpyHostToDevice, s));
+        in = (const double*)J->aos.p;
+    }
+    launch_aos_to_soa(in, (double*)J->st.p, J->n, s);
+    AdjParams a = params_of(J);
+    launch_adj_forward(a, (double*)J->ckpt.p, J->nturn, J->every, s);
+    CK(cudaMemcpyAsync(J->final_x.p, J->st.p, sizeof(double) * (size_t)J->n, cudaMemcpyDeviceToDevice, s));
+    launch_soa_to_aos((const double*)J->st.p, (double*)J->aos.p, J->n, s);
+    C->launches += 3;
+    if (dev_ptr(r_final)) CK(cudaMemcpyAsync(r_final, J->aos.p, s6, cudaMemcpyDeviceToDevice, s));
+    else CK(cudaMemcpyAsync(r_final, J->aos.p, s6, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    CK(cudaGetLastError());
+    J->have_forward = true;
+    return ACCEL_OK;
+}
+
+int accel_adjoint_backward(accel_adjoint* J, const double* g, double* dr0, double* dp) {
+    if (!J || !g || !dr0 || (!dp && J->nparam > 0)) return fail(ACCEL_E_INVALID, "NULL argument");
+    if (!J->have_forward) return fail(ACCEL_E_INVALID, "call accel_adjoint_forward first");
+    accel_ctx* C = J->line->ctx;
+    std::lock_guard<std::mutex> lk(C->mu);
+    CK(cudaSetDevice(C->device));
+    cudaStream_t s = C->stream;
+    const size_t s6 = sizeof(double) * 6 * (size_t)J->n;
+    const double* in = g;
+    if (!dev_ptr(g)) {
+        CK(cudaMemcpyAsync(J->aos.p, g, s6, cudaMemcpyHostToDevice, s));
+        in = (const double*)J->aos.p;
+    }
+    launch_aos_to_soa(in, (double*)J->lam.p, J->n, s);
+    const int nblk = adj_blocks(J->n);
+    if (J->nparam > 0) CK(cudaMemsetAsync(J->part.p, 0, sizeof(double) * (size_t)nblk * J->nparam, s));
+    AdjParams a = params_of(J);
+    int64_t launches = 1;
+    for (int seg = J->nseg - 1; seg >= 0; seg--) {
+        const int t0 = seg * J->every;
+        const int nt = std::min(J->every, J->nturn - t0);
+        const double* ck = (const double*)J->ckpt.p + (size_t)seg * 6 * J->n;
+        launch_adj_recompute(a, ck, (double*)J->turn_tape.p, nt, s);
+        launches++;
+        for (int j = nt - 1; j >= 0; j--) {
+            launch_adj_turn_reverse(a, (const double*)J->turn_tape.p + (size_t)j * 6 * J->n,
+                                    (const double*)J->final_x.p, s);
+            launches++;
+        }
+    }
+    launch_soa_to_aos((const double*)J->lam.p, (double*)J->aos.p, J->n, s);
+    launches++;
+    if (dev_ptr(dr0)) CK(cudaMemcpyAsync(dr0, J->aos.p, s6, cudaMemcpyDeviceToDevice, s));
+    else CK(cudaMemcpyAsync(dr0, J->aos.p, s6, cudaMemcpyDeviceToHost, s));
+    if (J->nparam > 0) {
+        launch_adj_reduce((const double*)J->part.p, nblk, J->nparam, (double*)J->grad.p, s);
+        launches++;
+        std::vector<double> sorted((size_t)J->nparam);
+        CK(cudaMemcpyAsync(sorted.data(), J->grad.p, sizeof(double) * J->nparam, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        std::vector<double> outv((size_t)J->nparam);
+        for (int j = 0; j < J->nparam; j++) outv[(size_t)j] = sorted[(size_t)J->order[(size_t)j]];
+        if (dev_ptr(dp)) CK(cudaMemcpy(dp, outv.data(), sizeof(double) * J->nparam, cudaMemcpyHostToDevice));
+        else std::memcpy(dp, outv.data(), sizeof(double) * J->nparam);
+    }
+    CK(cudaStreamSynchronize(s));
+    CK(cudaGetLastError());
+    C->launches += launches;
+    return ACCEL_OK;
+}
+
+}  // extern "C"

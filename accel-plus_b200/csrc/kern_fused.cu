@@ -60,10 +60,21 @@ __global__ void __launch_bounds__(BS, MINB) k_fused(const TrackParams P) {
     const int tbase = P.turn_dev ? *P.turn_dev : 0;
     const int rbase = (P.rng_base ? *P.rng_base : 0) + tbase;
     double* __restrict__ st = P.st;
+    // sched 1: this block owns chunks [c0, c1) of the live list, its warps stride through them
+    const int nchunk = (nlive + 31) / 32;
+    const int per_block = (nchunk + gridDim.x - 1) / gridDim.x;
+    const int c0 = blockIdx.x * per_block, c1 = min(nchunk, c0 + per_block);
+    int cnext = c0 + (threadIdx.x >> 5);
     for (;;) {
         int base = 0;
-        if (lane == 0) base = atomicAdd(P.chunk_ctr, 32);
-        base = __shfl_sync(FULL, base, 0);
+        if (P.sched == 0) {
+            if (lane == 0) base = atomicAdd(P.chunk_ctr, 32);
+            base = __shfl_sync(FULL, base, 0);
+        } else {
+            if (cnext >= c1) break;
+            base = cnext * 32;
+            cnext += BS / 32;
+        }
         if (base >= nlive) break;
         const int idx = base + lane;
         const bool have = idx < nlive;

@@ -23,12 +23,15 @@ struct TrackParams {
     int turn0;               // turn index (loss record) of the launch's first turn
     const int32_t* turn_dev; // device turn counter added to turn0 and rng_turn0 (may be null)
     int rng_turn0;           // turn offset fed to the QE counter
+    int sched;               // fused: 0 chunks pulled per warp from an atomic counter,
+                             //        1 contiguous live-list range per block (L1 keeps fewer tables)
     const int32_t* rng_base; // device: QE turn base of the line (advanced per call)
     uint64_t seed;
 };
 
 // ---- fused (kern_fused.cu) ----------------------------------------------------------------
 constexpr int kNumFusedVariants = 6;
+constexpr int kNumSched = 2;
 struct VariantInfo { int block; int min_blocks; };
 VariantInfo fused_variant_info(int v);
 int fused_blocks_per_sm(int variant);                     // occupancy at the variant's block
@@ -67,19 +70,20 @@ struct AdjParams {
     const DevElem* tbl;
     int ne;
     int64_t n;
-    double* st;          // SoA state being advanced (forward / recompute)
-    double* lam;         // SoA adjoint
-    double* tape;        // [ne][6][n] element-input states of one turn
-    double* pgrad_part;  // [nblocks][nparam] per-block partial parameter gradients
-    const int32_t* pslot;   // [ne] slot of this element's first parameter, -1 none
-    const int32_t* pkind;   // [nparam] field kind
+    double* st;             // SoA state being advanced
+    double* lam;            // SoA adjoint
+    double* tape;           // [ne][6][n] element-input states of one turn
+    double* pgrad_part;     // [nblocks][nparam] per-block parameter-gradient rows
+    const int32_t* pfirst;  // [ne] first parameter of each element (sorted by element)
+    const int32_t* pcount;  // [ne] parameters of each element
+    const int32_t* pkind;   // [nparam] adj::ParamKind
     const int32_t* pindex;  // [nparam] multipole index
     int nparam;
-    int32_t* err;
 };
-void launch_adj_turn_forward(const AdjParams& a, cudaStream_t s);      // st advanced one turn
-void launch_adj_turn_backward(const AdjParams& a, cudaStream_t s);     // uses st = turn input
-void launch_adj_reduce(const double* part, int nblk, int nparam, double* out, cudaStream_t s);
 int adj_blocks(int64_t n);
+void launch_adj_forward(const AdjParams& a, double* ckpt, int nturn, int every, cudaStream_t s);
+void launch_adj_recompute(const AdjParams& a, const double* ck, double* turn_tape, int nt, cudaStream_t s);
+void launch_adj_turn_reverse(const AdjParams& a, const double* r_start, const double* final_x, cudaStream_t s);
+void launch_adj_reduce(const double* part, int nblk, int nparam, double* out, cudaStream_t s);
 
 }  // namespace accel

@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <array>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -51,9 +52,10 @@ struct accel_ctx {
         probe_state;
     int tile_variant = -1;  // -1: tuned or default
     int tile_seg = 0;       // 0: tuned or default
+    int tile_sched = -1;    // -1: tuned or default
     int bps[accel::kNumFusedVariants] = {0};
     std::map<accel::GraphKey, std::unique_ptr<accel::GraphEntry>> graphs;
-    std::map<accel::GraphKey, std::pair<int, int>> tuned;  // -> (variant, seg)
+    std::map<accel::GraphKey, std::array<int, 3>> tuned;  // -> (variant, seg, sched)
     accel::BatchKey batch_key;
     int64_t launches = 0;
     bool profile = false;                  // direct launches with events (accel_profile_enable)

@@ -375,7 +375,9 @@ def engine_arm(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": config_dict(args, off, aos), "roofline": roofline, "cpu_baseline": cpu,
             "e2e": e2e, "gpu_launches": int(launches), "clocks": clk, "plain": plain,
-            "tile": {"block": tile[0], "seg_turns": tile[1], "variant": tile[2]} if tile else None,
+            "tile": {"block": tile[0], "seg_turns": tile[1], "variant": tile[2] % 100,
+                     "sched": ["atomic chunks per warp", "contiguous range per block"][tile[2] // 100]}
+                    if tile else None,
             "particle_turns_per_step": total_pt,
             "survivors": int((loss_np < 0).sum()),
         }

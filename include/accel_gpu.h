@@ -187,7 +187,9 @@ int  accel_track_batched(accel_line* const* lines, int ninst, const int64_t* par
                          double* r_soa, int64_t ntot, int nturn, int32_t* loss_turn,
                          int mode, void* stream);
 
-/* Autotuner control: tile = {block, turns per segment (compaction cadence), variant} */
+/* Autotuner control: tile = {block, turns per segment (compaction cadence), variant}, where
+ * variant = register-cap variant + 100 x scheduling mode (0: chunks of 32 particles pulled per
+ * warp from an atomic counter; 1: a contiguous live-list range per block). */
 int  accel_autotune(accel_line* const* lines, int ninst, const int64_t* part_off,
                     const double* r_soa, int64_t ntot, int* tile_out3);
 int  accel_set_tile(accel_ctx* ctx, int block, int seg_turns, int variant);  /* 0s = auto */
