@@ -214,7 +214,7 @@ int  accel_m66_at(accel_line* line, int st, int ed, const double* r0, int method
  * accel_adjoint_backward takes dL/dr_final (AoS, 6N) and returns dL/dr0 (AoS, 6N) and
  * dL/dparams (nparam), recomputing each segment from its checkpoint.
  */
-typedef struct accel_adjoint accel_adjoint;
+typedef struct accel_adjoint accel_adjoint;  /* destroy before its line; lines before their ctx */
 int  accel_adjoint_create(accel_line* line, int N, int nturn, int ckpt_every,
                           const int32_t* param_elem, const int32_t* param_field,
                           const int32_t* param_index, int nparam, accel_adjoint** out);
