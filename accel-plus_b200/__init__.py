@@ -13,7 +13,6 @@ from __future__ import annotations
 
 import ctypes as C
 import os
-import weakref
 from typing import Iterable, Sequence
 
 import numpy as np
@@ -206,13 +205,11 @@ class Context:
 
     def __init__(self, device: int = 0):
         self.h = C.c_void_p()
-        self._children = weakref.WeakSet()
         _check(lib().accel_ctx_create(device, C.byref(self.h)), "accel_ctx_create")
 
     def close(self):
-        """Destroy the context; lines created on it are closed first."""
-        for ch in list(self._children):
-            ch.close()
+        """Release the context handle.  The library keeps it alive for lines still open on it, so
+        handles may be closed (or garbage-collected) in any order."""
         if self.h:
             lib().accel_ctx_destroy(self.h)
             self.h = C.c_void_p()
@@ -295,17 +292,13 @@ class Line:
     """A lattice uploaded to a context (accel_line), with the reference ALine's pass API."""
 
     def __init__(self, ctx: Context, elems: Sequence[ElemDesc]):
-        self.ctx = ctx  # the context outlives its lines
+        self.ctx = ctx
         self.h = C.c_void_p()
-        self._children = weakref.WeakSet()
         arr = desc_array(elems)
         _check(lib().accel_line_create(ctx.h, arr, len(elems), C.byref(self.h)), "accel_line_create")
-        ctx._children.add(self)
 
     def close(self):
-        """Destroy the line; adjoints built on it are closed first."""
-        for ch in list(self._children):
-            ch.close()
+        """Release the line handle (the library keeps it for adjoints still open on it)."""
         if self.h:
             lib().accel_line_destroy(self.h)
             self.h = C.c_void_p()
@@ -411,13 +404,12 @@ class Adjoint:
         self._keep = (pe, pf, pi)
         self.nparam = len(params)
         self.n = n
-        self.line = line  # the line outlives its adjoints
+        self.line = line
         self.h = C.c_void_p()
         _check(lib().accel_adjoint_create(line.h, n, nturn, ckpt_every,
                                           C.c_void_p(pe.ctypes.data), C.c_void_p(pf.ctypes.data),
                                           C.c_void_p(pi.ctypes.data), self.nparam, C.byref(self.h)),
                "accel_adjoint_create")
-        line._children.add(self)
 
     def close(self):
         if self.h:

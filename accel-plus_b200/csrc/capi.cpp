@@ -436,11 +436,37 @@ int accel_ctx_create(int device, accel_ctx** out) {
     return ACCEL_OK;
 }
 
-int accel_ctx_destroy(accel_ctx* C) {
-    if (!C) return ACCEL_OK;
+}  // extern "C"
+
+namespace accel {
+void ctx_unref(accel_ctx* C) {
+    if (C->refs.fetch_sub(1) != 1) return;
     cudaSetDevice(C->device);
     cudaStreamSynchronize(C->stream);
     delete C;
+}
+
+void line_unref(accel_line* L) {
+    if (L->refs.fetch_sub(1) != 1) return;
+    accel_ctx* C = L->ctx;
+    {
+        std::lock_guard<std::mutex> lk(C->mu);
+        cudaSetDevice(C->device);
+        cudaStreamSynchronize(C->stream);
+        C->graphs.clear();
+        L->d_tbl.release();
+        L->d_rng.release();
+        delete L;
+    }
+    ctx_unref(C);
+}
+}  // namespace accel
+
+extern "C" {
+
+int accel_ctx_destroy(accel_ctx* C) {
+    if (!C) return ACCEL_OK;
+    accel::ctx_unref(C);
     return ACCEL_OK;
 }
 
@@ -498,19 +524,14 @@ int accel_line_create(accel_ctx* C, const accel_elem_desc* elems, int n, accel_l
     std::lock_guard<std::mutex> lk(C->mu);
     int s = line_sync(L.get());
     if (s) return s;
+    C->refs.fetch_add(1);
     *out = L.release();
     return ACCEL_OK;
 }
 
 int accel_line_destroy(accel_line* L) {
     if (!L) return ACCEL_OK;
-    std::lock_guard<std::mutex> lk(L->ctx->mu);
-    cudaSetDevice(L->ctx->device);
-    cudaStreamSynchronize(L->ctx->stream);
-    L->ctx->graphs.clear();
-    L->d_tbl.release();
-    L->d_rng.release();
-    delete L;
+    accel::line_unref(L);
     return ACCEL_OK;
 }
 

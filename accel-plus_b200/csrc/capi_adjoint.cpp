@@ -168,17 +168,22 @@ int accel_adjoint_create(accel_line* L, int N, int nturn, int every, const int32
     std::copy(J->pkind.begin(), J->pkind.end(), meta.begin() + 2 * ne);
     std::copy(J->pindex.begin(), J->pindex.end(), meta.begin() + 2 * ne + std::max(1, nparam));
     CK(cudaMemcpy(J->meta.p, meta.data(), meta.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+    L->refs.fetch_add(1);
     *out = J.release();
     return ACCEL_OK;
 }
 
 int accel_adjoint_destroy(accel_adjoint* J) {
     if (!J) return ACCEL_OK;
-    std::lock_guard<std::mutex> lk(J->line->ctx->mu);
-    cudaSetDevice(J->line->ctx->device);
-    cudaStreamSynchronize(J->line->ctx->stream);
-    J->line->dirty = true;  // the table was widened for parameter orders; rebuild on next use
-    delete J;
+    accel_line* L = J->line;
+    {
+        std::lock_guard<std::mutex> lk(L->ctx->mu);
+        cudaSetDevice(L->ctx->device);
+        cudaStreamSynchronize(L->ctx->stream);
+        L->dirty = true;  // the table was widened for parameter orders; rebuild on next use
+        delete J;
+    }
+    accel::line_unref(L);
     return ACCEL_OK;
 }
 

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <array>
+#include <atomic>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -42,7 +43,11 @@ void launch_rng_advance(int32_t* base, int nturn, cudaStream_t s);
 
 }  // namespace accel
 
+// Handles are reference counted so that they may be destroyed in any order: a context counts
+// its live lines, a line its live adjoints, and each is released when its own destroy has been
+// called and its last child is gone.
 struct accel_ctx {
+    std::atomic<int> refs{1};
     int device = 0;
     int sm_count = 0;
     cudaStream_t stream = nullptr;
@@ -64,6 +69,7 @@ struct accel_ctx {
 };
 
 struct accel_line {
+    std::atomic<int> refs{1};
     accel_ctx* ctx = nullptr;
     std::vector<accel_elem_desc> desc;
     std::vector<accel::DevElem> host_tbl;
@@ -80,4 +86,9 @@ inline GraphKey tune_key(::accel_line* const* lines, int ninst, int64_t ntot, in
     k.v = {(int64_t)(intptr_t)lines[0], lines[0]->version, (int64_t)ninst, ntot};
     return k;
 }
+}  // namespace accel
+
+namespace accel {
+void ctx_unref(accel_ctx* C);   // drop one reference; the last one frees the context
+void line_unref(accel_line* L);  // drop one reference; the last one frees the line and unrefs its context
 }  // namespace accel

@@ -143,6 +143,8 @@ const char* accel_status_string(int status);
 const char* accel_last_error(void);              /* thread-local detail of the last failure   */
 int  accel_version(void);
 int  accel_device_count(int* n);
+/* Handles are released in any order: a context with live lines (or a line with live adjoints)
+ * stays usable by those children and is freed when the last of them is destroyed.           */
 int  accel_ctx_create(int device, accel_ctx** out);
 int  accel_ctx_destroy(accel_ctx* ctx);
 
@@ -214,7 +216,7 @@ int  accel_m66_at(accel_line* line, int st, int ed, const double* r0, int method
  * accel_adjoint_backward takes dL/dr_final (AoS, 6N) and returns dL/dr0 (AoS, 6N) and
  * dL/dparams (nparam), recomputing each segment from its checkpoint.
  */
-typedef struct accel_adjoint accel_adjoint;  /* destroy before its line; lines before their ctx */
+typedef struct accel_adjoint accel_adjoint;  /* holds its line (and context) until destroyed */
 int  accel_adjoint_create(accel_line* line, int N, int nturn, int ckpt_every,
                           const int32_t* param_elem, const int32_t* param_field,
                           const int32_t* param_index, int nparam, accel_adjoint** out);

@@ -1,7 +1,10 @@
 """The adjoint pair on the GPU: gradients of L = sum over surviving particles of (x^2 + y^2) after
 n turns, with respect to the initial coordinates and multipole strengths, against central finite
-differences of the CPU oracle (h = 1e-6), and the one-turn Jacobian from six adjoint seeds against
-the exact tangent map.  Tolerance: 1e-6 relative (the finite-difference error itself is ~1e-9)."""
+differences of the CPU oracle, and the one-turn Jacobian from six adjoint seeds against the exact
+tangent map.  Tolerance: 1e-6 relative.  The differences are Richardson-extrapolated central
+differences: steps of 1e-6 of a coordinate's spread, and 1e-3 of a strength (a sextupole's gradient
+is a small sum of cancelling terms, which round-off in the tracked loss would swamp at tiny steps;
+at 1e-3 the extrapolated difference converges to 1e-7 relative)."""
 from __future__ import annotations
 
 import numpy as np
@@ -61,7 +64,8 @@ def test_adjoint_against_finite_differences(A, ctx, O, LT, ringname):
     ref = r0.copy()
     O.port_track(ring, ref, nturn, loss=False)
     scale = np.sqrt(np.mean(ref ** 2, axis=0)) + 1e-30
-    assert np.max(np.abs(rf - ref) / scale) < 1e-12  # the adjoint's forward is the reference map
+    # the adjoint's forward is the reference map (FMA-contracted, so not bit-identical)
+    assert np.max(np.abs(rf - ref) / scale) < 1e-10
     dr0, dp = adj.backward(grad_final(rf))
     h = 1e-6
     # initial coordinates: particles are independent, so perturb one particle at a time
@@ -83,7 +87,7 @@ def test_adjoint_against_finite_differences(A, ctx, O, LT, ringname):
             arr = rr[e].poly_b if fld == A.F_POLYNOMB else rr[e].poly_a
             arr[idx] += dv * step
             return loss_of(O, rr, r0, nturn)
-        fd = richardson(f, h) / step
+        fd = richardson(f, 1e-3) / step
         assert abs(dp[j] - fd) <= 1e-6 * max(abs(fd), 1e-9), (j, dp[j], fd)
 
 
@@ -113,3 +117,28 @@ def test_adjoint_rejects_radiation_and_bad_params(A, ctx, LT):
     with pytest.raises(A.AccelError) as ei:
         A.Adjoint(line4, 4, 2, 1, [(drift, A.F_POLYNOMB, 2)])
     assert ei.value.status == A.E_UNSUPPORTED
+
+
+def test_handles_released_in_any_order(A, ctx, LT):
+    """Context, line and adjoint destroyed parent-first through the C-ABI: each parent stays alive
+    until its last child is gone, so the children still work and nothing is freed twice."""
+    import ctypes as C
+    L = A.lib()
+    c = C.c_void_p()
+    assert L.accel_ctx_create(0, C.byref(c)) == 0
+    ring = LT.config4_ring()
+    arr = (A.ElemDesc * len(ring))(*ring)
+    ln = C.c_void_p()
+    assert L.accel_line_create(c, arr, len(ring), C.byref(ln)) == 0
+    adj = C.c_void_p()
+    z = np.zeros(1, dtype=np.int32)
+    assert L.accel_adjoint_create(ln, 4, 2, 1, C.c_void_p(z.ctypes.data), C.c_void_p(z.ctypes.data),
+                                  C.c_void_p(z.ctypes.data), 0, C.byref(adj)) == 0
+    assert L.accel_ctx_destroy(c) == 0
+    r = np.zeros((4, 6))
+    r[:, 0] = 1e-4
+    assert L.accel_line_destroy(ln) == 0
+    out = np.empty_like(r)
+    assert L.accel_adjoint_forward(adj, C.c_void_p(r.ctypes.data), C.c_void_p(out.ctypes.data)) == 0
+    assert np.all(np.isfinite(out)) and np.any(out != r)
+    assert L.accel_adjoint_destroy(adj) == 0

@@ -1,0 +1,106 @@
+"""The input-deck interpreter `accel+gpu` against the reference's own `accel+` on the same decks.
+
+The reference's outputs are committed fixtures (tests/golden/<deck>.ref.out, written by
+make_deck_golden.py).  Both programs print with six significant digits, so the comparison is line by
+line: the words must be identical and every number equal within 2e-5 relative (1e-12 absolute for
+values that are round-off around zero).  Dynamic- and momentum-aperture boundaries are decided by a
+lost / survived verdict that may flip for a particle on the chaotic edge; there a ray radius may
+differ by one scan step and the area by the one triangle it changes.
+"""
+from __future__ import annotations
+
+import os
+import re
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+EXE = os.path.join(ROOT, "accel-plus_b200", "accel+gpu")
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+DECKS = os.path.join(ROOT, "tests", "decks")
+NUM = re.compile(r"[-+]?(?:\d+\.?\d*|\.\d+)(?:[eE][-+]?\d+)?")
+
+
+def run_deck(name):
+    out = subprocess.run([EXE, os.path.join(DECKS, name + ".in")], cwd=ROOT, capture_output=True,
+                         text=True, timeout=600)
+    assert out.returncode == 0, out.stdout[-2000:] + out.stderr[-2000:]
+    return [l for l in out.stdout.splitlines() if not l.startswith("#UTC")]
+
+
+def split(line):
+    nums = [float(m) for m in NUM.findall(line)]
+    return NUM.sub("#", line).split(), nums
+
+
+def close(a, b, rel=2e-5, abs_=1e-12):
+    return abs(a - b) <= max(rel * max(abs(a), abs(b)), abs_)
+
+
+def compare(mine, ref):
+    assert len(mine) == len(ref), "\n".join(mine[-20:])
+    block, step = None, None
+    for lm, lr in zip(mine, ref):
+        wm, nm = split(lm)
+        wr, nr = split(lr)
+        assert wm == wr and len(nm) == len(nr), (lm, lr)
+        if lr.startswith("$$$") or lr.startswith("*****"):
+            block = lr
+        if lr.startswith("#") and len(nr) == 7:  # track_DA: xmin xmax ymax nray nstep nturn neg
+            step = ("da", (nr[1] - nr[0]) / (nr[4] - 1))
+        if lr.startswith("#") and len(nr) == 5:  # track_MA: nmoni nstep nturn dppmin dppmax
+            step = ("ma", (nr[4] - nr[3]) / nr[1])
+        if all(close(a, b) for a, b in zip(nm, nr)):
+            continue
+        if block and block.startswith("$$$DA-profile") and step and step[0] == "da":
+            if lr.startswith("$$$DA"):
+                assert close(nm[-1], nr[-1], rel=0.05), (lm, lr)
+            else:
+                rm, rr = (nm[0] ** 2 + nm[1] ** 2) ** 0.5, (nr[0] ** 2 + nr[1] ** 2) ** 0.5
+                assert abs(rm - rr) <= 1.01 * step[1], (lm, lr)
+            continue
+        if block and block.startswith("$$$MA") and step and step[0] == "ma":
+            if lr.startswith("$$$MA"):
+                assert close(nm[-1], nr[-1], rel=0.2), (lm, lr)
+            else:
+                assert all(abs(a - b) <= 1.01 * step[1] for a, b in zip(nm, nr)), (lm, lr)
+            continue
+        raise AssertionError(f"numbers differ:\n mine: {lm}\n ref:  {lr}")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("deck", ["dba_deck", "fodo_deck"])
+def test_deck_matches_reference(deck):
+    with open(os.path.join(GOLDEN, deck + ".ref.out")) as f:
+        ref = [l for l in f.read().splitlines() if not l.startswith("#UTC")]
+    compare(run_deck(deck), ref)
+
+
+def test_deck_compare_accepts_reference_against_itself():
+    """The comparison's own logic, on the golden outputs alone (no GPU)."""
+    for deck in ("dba_deck", "fodo_deck"):
+        with open(os.path.join(GOLDEN, deck + ".ref.out")) as f:
+            ref = f.read().splitlines()
+        compare(ref, ref)
+        bent = list(ref)
+        i = next(k for k, l in enumerate(bent) if l.startswith("Tunes"))
+        bent[i] = bent[i].replace("0.", "0.9", 1)
+        with pytest.raises(AssertionError):
+            compare(bent, ref)
+
+
+def test_deck_without_device_fails_loudly():
+    """With no CUDA device the executable exits non-zero with the reason, and runs nothing."""
+    import ctypes
+    try:
+        n = ctypes.c_int(0)
+        ok = ctypes.CDLL("libcuda.so.1").cuInit(0) == 0 and ctypes.CDLL("libcuda.so.1").cuDeviceGetCount(ctypes.byref(n)) == 0 and n.value > 0
+    except OSError:
+        ok = False
+    if ok:
+        pytest.skip("a CUDA device is present")
+    out = subprocess.run([EXE, os.path.join(DECKS, "fodo_deck.in")], cwd=ROOT, capture_output=True,
+                         text=True, timeout=120)
+    assert out.returncode == 2
+    assert "accel+gpu:" in out.stderr
