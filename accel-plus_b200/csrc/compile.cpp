@@ -1,4 +1,4 @@
-// compile.cpp — lower accel_elem_desc descriptors to 384-byte device records.
+// compile.cpp — lower accel_elem_desc descriptors to 512-byte device records (DevElem).
 //
 // Every expression below that depends only on element parameters is one the reference evaluates
 // inside its per-particle loops; it is evaluated here once, with the same operands in the same

@@ -317,7 +317,7 @@ void Deck::lattice(std::istream& in) {
             // correct_tune / correct_chrom: type=T, famname=(F1 F2) [x, y] [REPEAT] [EXACT]
             // (process.cpp:545-766); EXACT runs Newton iterations on exact one-turn matrices
             const bool tune = (k == 5);
-            cout << (tune ? "$$$Correct tunes***********************" : "$$$Correct chromaticities***********************") << endl;
+            cout << (tune ? "$$$Correct Tunes***********************" : "$$$Correct chromaticities***********************") << endl;
             string type, f1, f2;
             double t1 = 0, t2 = 0;
             bool repeat = false, exact = false;
