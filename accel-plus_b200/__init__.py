@@ -112,6 +112,7 @@ def lib() -> C.CDLL:
         "accel_adjoint_forward": (I, [P, P, P]),
         "accel_adjoint_backward": (I, [P, P, P, P]),
         "accel_beam_stat": (I, [P, P, I, I, C.POINTER(D), C.POINTER(D), C.POINTER(D), C.POINTER(I)]),
+        "accel_beam_stat_noalloc": (I, [P, I, C.c_int64, P, P]),
         "accel_fp64_peak": (I, [P, C.POINTER(D)]),
         "accel_launch_count": (I, [P, C.POINTER(C.c_int64)]),
         "accel_profile_enable": (I, [P, I]),
@@ -255,6 +256,20 @@ class Context:
         _check(lib().accel_beam_stat(self.h, ptr, layout, n, mean, sig, cross, C.byref(nl)),
                "accel_beam_stat")
         return np.array(mean), np.array(sig), np.array(cross), nl.value
+
+
+def beam_stat_noalloc(r, out, layout=LAYOUT_AOS, n=None, stream=None):
+    """accel_beam_stat_noalloc: beam moments of a device tensor into the device tensor `out`
+    (19 float64: mean[6], sigma[6], cross[6], live count), without any device allocation.
+    Returns once the kernels are queued on `stream` (None = the legacy default stream)."""
+    if not hasattr(r, "data_ptr") or not hasattr(out, "data_ptr"):
+        raise ValueError("r and out must be device tensors")
+    if out.numel() < 19:
+        raise ValueError("out must hold 19 doubles")
+    ptr, n = _ptr_and_n(r, n, layout)
+    s = C.c_void_p(stream) if stream is not None else None
+    _check(lib().accel_beam_stat_noalloc(ptr, layout, n, C.c_void_p(out.data_ptr()), s),
+           "accel_beam_stat_noalloc")
 
 
 def _ptr_and_n(r, n=None, layout=LAYOUT_AOS):

@@ -230,6 +230,24 @@ int  accel_adjoint_backward(accel_adjoint* adj, const double* dl_drfinal, double
 int  accel_beam_stat(accel_ctx* ctx, const double* r, int layout, int N, double* mean,
                      double* sigma, double* cross, int* nlive);
 
+/* The same beam moments with no device allocation.  No counterpart in the reference: it exists
+ * for callers that cannot let a library allocate (code running while a stream is captured,
+ * device memory reserved up front by a pool or another framework, per-turn sampling loops that a
+ * cudaMalloc/cudaFree synchronisation would stall).
+ *   r    device array of N particles in `layout`, read in place; out  device array of 19 doubles
+ *        receiving mean[6], sigma[6], cross[6] and the live count (as a double), in that order.
+ *   N    1 .. ACCEL_NOALLOC_STAT_MAX_N; larger N returns ACCEL_E_TOO_LARGE and launches nothing.
+ *   stream  where the five small kernels run (NULL = the legacy default stream); the call
+ *        returns without synchronising, and `out` is ready when that stream reaches it.
+ * Partial sums live in one fixed device array per device (12 * 4096 + 32 doubles), which every
+ * call overwrites before reading: nothing in it needs to start at zero.  Because that array is
+ * shared, calls on the same device must not overlap: issue them on one stream, or order them
+ * with events.  The first call on each device does a one-time set-up (the scratch's address via
+ * cudaGetSymbolAddress, and the kernels loaded) with that device current; make that first call
+ * before beginning any stream capture.                                                         */
+#define ACCEL_NOALLOC_STAT_MAX_N 4194304
+int  accel_beam_stat_noalloc(const double* r, int layout, int64_t N, double* out, void* stream);
+
 /* Device FP64 FMA throughput micro-benchmark (TFLOP/s, FMA = 2 flops). */
 int  accel_fp64_peak(accel_ctx* ctx, double* tflops);
 
