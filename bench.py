@@ -47,6 +47,7 @@ def parse():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-kernel comparison")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint (gradient) leg")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--small", action="store_true",
                     help="profiling case: 16 copies, 20 turns, one step (for ncu)")
@@ -208,27 +209,118 @@ def config_dict(args, off, aos):
             "seeds": "copy k of rank r: error seed r*copies+k; grid sizes default_rng(12345+r)"}
 
 
+def adjoint_leg(A, LT, ctx, steps: int = 3) -> dict:
+    """Gradient of L = sum over particles of (x^2 + y^2) after 512 turns of the 4D DBA (no cavity,
+    radiation off), 4,096 Gaussian particles (seed 1), with respect to the 6 x 4,096 initial
+    coordinates and the 36 sextupole knobs (mirror pairs of the 72 sextupoles), checkpointed every
+    64 turns.  The adjoint pair and the tracking it is compared with are synchronous host calls on
+    the context's stream, so wall-clock time around them is device time plus microseconds.
+    Finite-difference cost, in tracks of the same 4,096 particles for 512 turns: naive central
+    differences per scalar input 2 x (6 x 4096 + 36); batched over the independent particles
+    (one coordinate of every particle at once) 2 x (6 + 36)."""
+    ring = LT.config4_ring()
+    line = A.Line(ctx, ring)
+    pairs = LT.sextupole_pairs(ring)
+    elems = sorted({i for p in pairs for i in p})
+    params = [(i, A.F_POLYNOMB, 2) for i in elems]
+    n, nturn, every = 4096, 512, 64
+    r0 = LT.config4_particles(n, seed=1)
+    adj = A.Adjoint(line, n, nturn, every, params)
+
+    def gradient():
+        rf = adj.forward(r0)
+        g = np.zeros_like(rf)
+        live = ~np.isnan(rf[:, 0])
+        g[live, 0], g[live, 2] = 2 * rf[live, 0], 2 * rf[live, 2]
+        dr0, dp = adj.backward(g)
+        return rf, dr0, dp
+
+    gradient()
+    t = time.perf_counter()
+    for _ in range(steps):
+        rf, dr0, dp = gradient()
+    t_adj = (time.perf_counter() - t) / steps
+    r = r0.copy()
+    line.track(r, nturn)
+    t = time.perf_counter()
+    for _ in range(steps):
+        r = r0.copy()
+        line.track(r, nturn)
+    t_track = (time.perf_counter() - t) / steps
+    knob = {e: j for j, e in enumerate(elems)}
+    dknob = np.array([dp[knob[a]] + dp[knob[b]] for a, b in pairs])
+    n_in = 6 * n + len(pairs)
+    naive, batched = 2 * n_in, 2 * (6 + len(pairs))
+    adj.close()
+    line.close()
+    return {"workload": "4D DBA, 4096 particles, 512 turns, checkpoints every 64, 36 sextupole knobs",
+            "gradients_per_s": 1.0 / t_adj, "gradient_components_per_s": n_in / t_adj,
+            "ms_per_gradient": 1e3 * t_adj, "ms_per_track": 1e3 * t_track,
+            "fd_tracks_naive": naive, "fd_tracks_batched": batched,
+            "fd_cost_ratio_naive": naive * t_track / t_adj,
+            "fd_cost_ratio_batched": batched * t_track / t_adj,
+            "survivors": int((~np.isnan(rf[:, 0])).sum()),
+            "knob_gradient_norm": float(np.linalg.norm(dknob)),
+            "timing": "wall clock around synchronous C-ABI calls, mean of %d" % steps}
+
+
+class Ranks:
+    """One process per GPU, as torchrun starts them (RANK / LOCAL_RANK / WORLD_SIZE, rendezvous on
+    MASTER_ADDR).  Every rank takes the same collective steps in the same order; a single process
+    (WORLD_SIZE unset or 1) needs no process group.  `backend` is "nccl" for the GPU run and
+    "gloo" for CPU tests of this plumbing."""
+
+    def __init__(self, backend: str = "nccl", timeout_s: int = 600):
+        import torch
+        import torch.distributed as dist
+        self.torch, self.dist = torch, dist
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.dev = torch.device("cuda", self.local) if backend == "nccl" else torch.device("cpu")
+        if self.world > 1:
+            from datetime import timedelta
+            kw = {"device_id": self.dev} if backend == "nccl" else {}
+            if backend == "nccl":
+                torch.cuda.set_device(self.local)
+            dist.init_process_group(backend, timeout=timedelta(seconds=timeout_s), **kw)
+
+    def barrier(self):
+        if self.world > 1:
+            self.dist.barrier()
+
+    def _reduce(self, x: float, op) -> float:
+        if self.world == 1:
+            return x
+        t = self.torch.tensor([x], device=self.dev, dtype=self.torch.float64)
+        self.dist.all_reduce(t, op=op)
+        return float(t.item())
+
+    def max(self, x: float) -> float:
+        return self._reduce(x, self.dist.ReduceOp.MAX)
+
+    def sum(self, x: float) -> float:
+        return self._reduce(x, self.dist.ReduceOp.SUM)
+
+    def close(self):
+        if self.world > 1:
+            self.dist.destroy_process_group()
+
+
 def engine_arm(args):
     import torch
-    import torch.distributed as dist
 
     A = importlib.import_module("accel-plus_b200")
     LT = importlib.import_module("accel-plus_b200.lattices")
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        from datetime import timedelta
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600),
-                                device_id=torch.device("cuda", local))
+    ranks = Ranks("nccl")
+    world, rank, local = ranks.world, ranks.rank, ranks.local
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     if args.small:
         args.copies, args.turns, args.steps, args.warmup = 16, 20, 1, 1
-        args.no_plain = args.no_cpu = args.no_e2e = True
+        args.no_plain = args.no_cpu = args.no_e2e = args.no_adjoint = True
     if args.engine_only:
-        args.no_plain = args.no_cpu = args.no_e2e = True
+        args.no_plain = args.no_cpu = args.no_e2e = args.no_adjoint = True
 
     rings, off, aos, sizes = workload(args.copies, rank)
     ntot = int(off[-1])
@@ -240,23 +332,7 @@ def engine_arm(args):
     flush = torch.empty(256 * 1024 * 1024 // 4, device=dev, dtype=torch.float32)
     stream = torch.cuda.current_stream().cuda_stream
 
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
-    def sum_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        return float(t.item())
+    barrier, max_over_ranks, sum_over_ranks = ranks.barrier, ranks.max, ranks.sum
 
     def step(mode=A.MODE_FUSED, k=0):
         flush.fill_(float(k))
@@ -364,6 +440,10 @@ def engine_arm(args):
                "d2h_bytes_per_step": int(h_out.numel() * 8 + h_loss.numel() * 4),
                "ms_per_step": ems, "path": "accel_track_batched (C-ABI) with pinned host in/out"}
 
+    adjoint = None
+    if not args.no_adjoint:
+        adjoint = adjoint_leg(A, LT, ctx)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_reference_rate(rings, off, aos)
@@ -375,6 +455,7 @@ def engine_arm(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": config_dict(args, off, aos), "roofline": roofline, "cpu_baseline": cpu,
             "e2e": e2e, "gpu_launches": int(launches), "clocks": clk, "plain": plain,
+            "adjoint": adjoint,
             "tile": {"block": tile[0], "seg_turns": tile[1], "variant": tile[2] % 100,
                      "sched": ["atomic chunks per warp", "contiguous range per block"][tile[2] // 100]}
                     if tile else None,
@@ -385,8 +466,7 @@ def engine_arm(args):
     for l in lines:
         l.close()
     ctx.close()
-    if world > 1:
-        dist.destroy_process_group()
+    ranks.close()
 
 
 def main():

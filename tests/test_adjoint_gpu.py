@@ -150,3 +150,37 @@ def test_handles_released_in_any_order(A, ctx, LT):
     assert L.accel_adjoint_forward(adj, C.c_void_p(r.ctypes.data), C.c_void_p(out.ctypes.data)) == 0
     assert np.all(np.isfinite(out)) and np.any(out != r)
     assert L.accel_adjoint_destroy(adj) == 0
+
+
+def test_autograd_function_over_the_adjoint_pair(A, ctx, LT):
+    """A torch.autograd.Function whose forward and backward are the C-ABI pair: loss.backward()
+    on a torch expression of the tracked coordinates returns the adjoint's gradients with respect
+    to the initial coordinates and the sextupole strengths."""
+    torch = pytest.importorskip("torch")
+    ring = LT.config4_ring()
+    sx = [i for i, d in enumerate(ring) if d.type == A.STRMPOLE and d.poly_b[2] != 0][:4]
+    line = A.Line(ctx, ring)
+    n, nturn = 64, 32
+    adj = A.Adjoint(line, n, nturn, 8, [(i, A.F_POLYNOMB, 2) for i in sx])
+
+    class Track(torch.autograd.Function):
+        @staticmethod
+        def forward(fctx, r0, k2):
+            # k2 carries the strengths the line already holds; it is the leaf for their gradient
+            return torch.from_numpy(adj.forward(r0.detach().numpy()))
+
+        @staticmethod
+        def backward(fctx, g):
+            dr0, dp = adj.backward(g.detach().contiguous().numpy())
+            return torch.from_numpy(dr0), torch.from_numpy(dp)
+
+    r0 = torch.tensor(small_particles(n, seed=3), dtype=torch.float64, requires_grad=True)
+    k2 = torch.tensor([ring[i].poly_b[2] for i in sx], dtype=torch.float64, requires_grad=True)
+    rf = Track.apply(r0, k2)
+    loss = (rf[:, 0] ** 2 + rf[:, 2] ** 2).sum()
+    loss.backward()
+    rf2 = adj.forward(r0.detach().numpy())
+    dr0, dp = adj.backward(grad_final(rf2))
+    assert np.array_equal(rf.detach().numpy(), rf2)
+    assert np.allclose(r0.grad.numpy(), dr0, rtol=1e-14, atol=0)
+    assert np.allclose(k2.grad.numpy(), dp, rtol=1e-14, atol=0)

@@ -84,8 +84,9 @@ def test_deck_compare_accepts_reference_against_itself():
             ref = f.read().splitlines()
         compare(ref, ref)
         bent = list(ref)
-        i = next(k for k, l in enumerate(bent) if l.startswith("Tunes"))
-        bent[i] = bent[i].replace("0.", "0.9", 1)
+        i = next(k for k, l in enumerate(bent) if any(float(x) != 0 for x in NUM.findall(l)))
+        x = next(m for m in NUM.finditer(bent[i]) if float(m.group()) != 0)
+        bent[i] = bent[i][:x.start()] + repr(1.001 * float(x.group())) + bent[i][x.end():]
         with pytest.raises(AssertionError):
             compare(bent, ref)
 
