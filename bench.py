@@ -406,10 +406,14 @@ def engine_arm(args):
         p1.record()
         torch.cuda.synchronize()
         pms = max_over_ranks(p0.elapsed_time(p1))
-        same = bool(np.array_equal(loss.cpu().numpy(), loss_np))
+        lp = loss.cpu().numpy()
+        diff = lp != loss_np
         plain = {"value": total_pt / (pms / 1e3), "ms_per_step": pms,
                  "fused_over_plain": (total_pt / (ms_step / 1e3)) / (total_pt / (pms / 1e3)),
-                 "loss_turns_identical_to_fused": same}
+                 "loss_turn_mismatches": int(diff.sum()),
+                 "mismatch_note": "particles whose loss turn differs between the two kernels; the "
+                                  "parity tests confine such differences to the chaotic aperture edge",
+                 "survival_mismatches": int(((lp < 0) != (loss_np < 0)).sum())}
 
     # ---- end to end through the C-ABI with host buffers ----
     e2e = None

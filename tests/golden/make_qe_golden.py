@@ -12,8 +12,8 @@ growth       qe_moments.npz: the moments (mean[6], sigma[6], cross[6], live coun
              PROCS x PER particles after TURNS turns from the origin (about two minutes).
 equilibrium  qe_equilibrium.npz: a Gaussian bunch (sigma_z 3 mm, sigma_delta 1e-3, 10 nm / 10 pm
              emittances matched to the ring-entrance Twiss) tracked for EQ_TURNS turns, which is
-             about three transverse damping times; rms sizes of all particles every EQ_EVERY
-             turns (about an hour on 8 cores).
+             about three transverse damping times; the moments (mean, sigma, cross, live count)
+             of all particles every EQ_EVERY turns (about an hour on 8 cores).
 """
 from __future__ import annotations
 
@@ -94,12 +94,14 @@ def equilibrium(A, LT, path):
     with mp.get_context("spawn").Pool(PROCS) as pool:
         parts = pool.map(worker_eq, jobs)
     snaps = np.concatenate(parts, axis=1)  # [snapshot, particle, 6]
-    sig = np.array([moments(s)[1] for s in snaps])
-    nl = np.array([moments(s)[3] for s in snaps])
+    mom = [moments(s) for s in snaps]
     turns = EQ_EVERY * (1 + np.arange(len(snaps)))
-    np.savez_compressed(os.path.join(HERE, "qe_equilibrium.npz"), sigma=sig, nlive=nl, turns=turns,
-                        m66=m66, seed=np.array([EQ_SEED]), n=np.array([PROCS * EQ_PER]))
-    print("turns", turns, "\nsigma\n", sig, "\nlive", nl)
+    np.savez_compressed(os.path.join(HERE, "qe_equilibrium.npz"),
+                        mean=np.array([m[0] for m in mom]), sigma=np.array([m[1] for m in mom]),
+                        cross=np.array([m[2] for m in mom]), nlive=np.array([m[3] for m in mom]),
+                        turns=turns, m66=m66, seed=np.array([EQ_SEED]), n=np.array([PROCS * EQ_PER]))
+    sig = np.array([m[1] for m in mom])
+    print("turns", turns, "\nsigma\n", sig, "\nlive", [m[3] for m in mom])
 
 
 def main():
