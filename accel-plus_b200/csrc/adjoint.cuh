@@ -69,6 +69,73 @@ __device__ __forceinline__ void forward(const DevElem& e, double* r) {
     lit::pass<double>(e, r, q);
 }
 
+// The same forward map on any number type (Dual<6> for the block Jacobians of the tape).
+template <class T>
+__device__ __forceinline__ void forward_t(const DevElem& e, T* r) {
+    if (lit::is_lost(r[0])) return;
+    if (e.op == OP_STRMPOLE || e.op == OP_STRKICK) {
+        double A[ACCEL_MAX_MPOLE], B[ACCEL_MAX_MPOLE];
+#pragma unroll
+        for (int i = 0; i < ACCEL_MAX_MPOLE; i++) { A[i] = e.v[V_A + i]; B[i] = e.v[V_B + i]; }
+        const int M = e.order_eff;
+        if (e.op == OP_STRKICK) { lit::strthinkick(r, A, B, 1.0, M); return; }
+        const double L1 = e.v[V_L1], L2 = e.v[V_L2], K1 = e.v[V_K1], K2 = e.v[V_K2];
+        // delta does not change inside the element: the slices' NormL are the same every time
+        const T norm = 1 / (1 + r[5]);
+        const T N1 = L1 * norm, N2 = L2 * norm;
+        for (int m = 0; m < e.nslice; m++) {
+            lit::fastdrift(r, N1);
+            lit::strthinkick(r, A, B, K1, M);
+            lit::fastdrift(r, N2);
+            lit::strthinkick(r, A, B, K2, M);
+            lit::fastdrift(r, N2);
+            lit::strthinkick(r, A, B, K1, M);
+            lit::fastdrift(r, N1);
+        }
+        return;
+    }
+    lit::QeSource q{0, 0, 0, 0, 0};
+    lit::pass<T>(e, r, q);
+}
+
+// Parameter element on dual numbers with parameter directions: r carries d/d(block input) in
+// d[0..5]; directions 6 + j seed the element's parameters j = 0 .. n-1 (kind/index as in
+// ElemParams).  Afterwards r[i].d[k] (k < 6) is the Jacobian of block and element together and
+// r[i].d[6 + j] = d out_i / d p_j.
+constexpr int kPD = 6 + kMaxParamsPerElem;
+__device__ __forceinline__ void forward_params(const DevElem& e, Dual<kPD>* r, int n, const int* kind,
+                                               const int* index) {
+    if (lit::is_lost(r[0])) return;
+    if (e.op == OP_QUAD) {
+        Dual<kPD> K(e.v[V_QK]);
+        for (int j = 0; j < n; j++)
+            if (kind[j] == PK_QUADK) K.d[6 + j] = 1.0;
+        lit::quad6(r, e.v[V_LEN], K);
+        return;
+    }
+    Dual<kPD> A[ACCEL_MAX_MPOLE], B[ACCEL_MAX_MPOLE];
+#pragma unroll
+    for (int i = 0; i < ACCEL_MAX_MPOLE; i++) { A[i] = Dual<kPD>(e.v[V_A + i]); B[i] = Dual<kPD>(e.v[V_B + i]); }
+    for (int j = 0; j < n; j++) {
+        if (kind[j] == PK_B) B[index[j]].d[6 + j] = 1.0;
+        else if (kind[j] == PK_A) A[index[j]].d[6 + j] = 1.0;
+    }
+    const int M = e.order_eff;
+    if (e.op == OP_STRKICK) { lit::strthinkick(r, A, B, 1.0, M); return; }
+    const double L1 = e.v[V_L1], L2 = e.v[V_L2], K1 = e.v[V_K1], K2 = e.v[V_K2];
+    for (int m = 0; m < e.nslice; m++) {
+        Dual<kPD> norm = 1 / (1 + r[5]);
+        Dual<kPD> N1 = L1 * norm, N2 = L2 * norm;
+        lit::fastdrift(r, N1);
+        lit::strthinkick(r, A, B, K1, M);
+        lit::fastdrift(r, N2);
+        lit::strthinkick(r, A, B, K2, M);
+        lit::fastdrift(r, N2);
+        lit::strthinkick(r, A, B, K1, M);
+        lit::fastdrift(r, N1);
+    }
+}
+
 // ---- VJPs ---------------------------------------------------------------------------------------
 // r: the drift's input (only px, py, delta are read); N = L/(1+delta) as the forward used it.
 __device__ __forceinline__ void vjp_drift(double px, double py, double d, double N, double* lam) {

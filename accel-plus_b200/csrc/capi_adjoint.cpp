@@ -2,9 +2,15 @@
 //
 // accel_adjoint_forward tracks N particles for nturn turns (literal maps, effective Horner order),
 // keeping the state at every ckpt_every-th turn.  accel_adjoint_backward then walks the segments
-// last to first: recompute the segment's turn-start states from its checkpoint, and reverse its
-// turns last to first (kern_adjoint.cu).  Memory on the device: (nseg + K + ne + 3) x 6 x N
-// doubles for checkpoints, the turn tape, the element tape, state, adjoint and scratch.
+// last to first: recompute the segment's turn-start states from its checkpoint, then reverse its
+// turns in chunks, last to first.  For each chunk, one wide kernel tapes every turn's unit
+// Jacobians (the 6x6 maps from one parameter element's output to the next one's) and the
+// parameter sensitivities, with dual numbers, and one kernel per particle sweeps them backwards
+// (kern_adjoint.cu).  The chunk is
+// as many turns of a segment as fit a 4 GB tape; when not even one turn fits, each turn is
+// reversed element by element instead (one launch per turn, an element-input tape of ne x 6 x N).
+// Memory on the device: (nseg + K + 3) x 6 x N doubles for checkpoints, turn-start states, state,
+// adjoint and scratch, plus the tape.
 //
 // Parameters are (element, field, index) triples: StrMPole PolynomB/PolynomA[index] (field K on a
 // StrMPole is PolynomB[1]), Quad K.  The line must be free of radiation, quantum excitation and
@@ -34,6 +40,7 @@ using namespace accel;
 
 namespace {
 constexpr int kMaxAdjParams = 2048;
+constexpr double kTapeBudgetBytes = 4.0e9;  // block-Jacobian tape of one chunk of turns
 
 bool dev_ptr(const void* p) {
     cudaPointerAttributes a;
@@ -50,10 +57,14 @@ struct accel_adjoint {
     int n = 0, nturn = 0, every = 1, nseg = 0, ne = 0, nparam = 0;
     std::vector<int> order;  // caller's parameter j -> sorted position
     std::vector<int32_t> pfirst, pcount, pkind, pindex;
-    DevBuf st, lam, aos, tape, ckpt, turn_tape, part, meta, final_x, grad;
+    std::vector<int32_t> pelem;  // elements carrying parameters, in line order
+    int npe = 0;
+    int chunk = 0;               // turns per block-Jacobian tape; 0: per-turn element reversal
+    DevBuf st, lam, aos, tape, ckpt, turn_tape, part, meta, final_x, grad, jt, rt, pel;
     bool have_forward = false;
     ~accel_adjoint() {
-        for (DevBuf* b : {&st, &lam, &aos, &tape, &ckpt, &turn_tape, &part, &meta, &final_x, &grad}) b->release();
+        for (DevBuf* b : {&st, &lam, &aos, &tape, &ckpt, &turn_tape, &part, &meta, &final_x, &grad, &jt, &rt, &pel})
+            b->release();
     }
 };
 
@@ -154,8 +165,25 @@ int accel_adjoint_create(accel_line* L, int N, int nturn, int every, const int32
     CK(cudaMemcpy(L->d_tbl.p, L->host_tbl.data(), L->host_tbl.size() * sizeof(DevElem), cudaMemcpyHostToDevice));
     const size_t s6 = sizeof(double) * 6 * (size_t)N;
     int nblk = adj_blocks(N);
+    for (int e = 0; e < ne; e++)
+        if (J->pcount[(size_t)e] > 0) J->pelem.push_back(e);
+    J->npe = (int)J->pelem.size();
+    const double per_turn = 8.0 * (double)N * (36.0 * (J->npe + 1) + 6.0 * nparam);
+    J->chunk = (int)std::min<double>(std::min(every, nturn), std::floor(kTapeBudgetBytes / per_turn));
+    if (J->chunk >= 1) {
+        const size_t c = (size_t)J->chunk, nn = (size_t)N;
+        if ((s = J->jt.ensure(sizeof(double) * c * (size_t)(J->npe + 1) * 36 * nn)) ||
+            (s = J->rt.ensure(sizeof(double) * std::max<size_t>(1, c * (size_t)nparam * 6 * nn))) ||
+            (s = J->pel.ensure(sizeof(int32_t) * (size_t)std::max(1, J->npe))))
+            return s;
+        if (J->npe > 0)
+            CK(cudaMemcpy(J->pel.p, J->pelem.data(), sizeof(int32_t) * J->pelem.size(), cudaMemcpyHostToDevice));
+    } else {
+        J->chunk = 0;
+        if ((s = J->tape.ensure(s6 * (size_t)ne))) return s;
+    }
     if ((s = J->st.ensure(s6)) || (s = J->lam.ensure(s6)) || (s = J->aos.ensure(s6)) ||
-        (s = J->tape.ensure(s6 * (size_t)ne)) || (s = J->ckpt.ensure(s6 * (size_t)J->nseg)) ||
+        (s = J->ckpt.ensure(s6 * (size_t)J->nseg)) ||
         (s = J->turn_tape.ensure(s6 * (size_t)std::min(every, nturn))) ||
         (s = J->part.ensure(sizeof(double) * (size_t)std::max(1, nblk * nparam))) ||
         (s = J->meta.ensure(sizeof(int32_t) * (size_t)(2 * ne + 2 * std::max(1, nparam)))) ||
@@ -238,10 +266,21 @@ int accel_adjoint_backward(accel_adjoint* J, const double* g, double* dr0, doubl
         const double* ck = (const double*)J->ckpt.p + (size_t)seg * 6 * J->n;
         launch_adj_recompute(a, ck, (double*)J->turn_tape.p, nt, s);
         launches++;
-        for (int j = nt - 1; j >= 0; j--) {
-            launch_adj_turn_reverse(a, (const double*)J->turn_tape.p + (size_t)j * 6 * J->n,
-                                    (const double*)J->final_x.p, s);
-            launches++;
+        if (J->chunk > 0) {
+            for (int hi = nt; hi > 0; hi -= J->chunk) {
+                const int lo = std::max(0, hi - J->chunk);
+                launch_adj_jtape(a, (const double*)J->turn_tape.p, lo, hi - lo, (const double*)J->final_x.p,
+                                 J->npe, (double*)J->jt.p, (double*)J->rt.p, s);
+                launch_adj_jsweep(a, hi - lo, (const double*)J->final_x.p, J->npe, (const int32_t*)J->pel.p,
+                                  (const double*)J->jt.p, (const double*)J->rt.p, s);
+                launches += 2;
+            }
+        } else {
+            for (int j = nt - 1; j >= 0; j--) {
+                launch_adj_turn_reverse(a, (const double*)J->turn_tape.p + (size_t)j * 6 * J->n,
+                                        (const double*)J->final_x.p, s);
+                launches++;
+            }
         }
     }
     launch_soa_to_aos((const double*)J->lam.p, (double*)J->aos.p, J->n, s);

@@ -1,7 +1,11 @@
 // kern_adjoint.cu — forward-with-checkpoints and reverse-turn kernels of the adjoint pair.
 //
-// One thread per particle throughout (particles are independent; only parameter gradients are
-// summed over them).  State, adjoint and tapes are SoA in HBM:
+// The forward runs and the recomputation of turn-start states use the register-resident element
+// maps of the fused tracker (elem_fast.cuh), with the literal map for everything they do not
+// specialise; the tapes are taken with dual numbers on the literal maps.
+//
+// One thread per particle in the forward and sweep kernels (particles are independent; only
+// parameter gradients are summed over them).  State, adjoint and tapes are SoA in HBM:
 //   st[6][n]             state being advanced
 //   lam[6][n]            adjoint dL/d(state)
 //   ckpt[nseg][6][n]     state at the first turn of every checkpoint segment
@@ -14,9 +18,75 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include "adjoint.cuh"
+#include "elem_fast.cuh"
 #include "kernels.h"
 
 namespace accel {
+
+namespace {
+// Elements the fast maps do not specialise take the literal map, out of line, state by value.
+__device__ __noinline__ fast::St literal_elem(fast::St s, const DevElem* __restrict__ e) {
+    double r[6] = {s.x, s.px, s.y, s.py, s.z, s.d};
+    adj::forward(*e, r);
+    return fast::St{r[0], r[1], r[2], r[3], r[4], r[5]};
+}
+
+// One element on the fast maps of the fused tracker (an adjoint's line has no radiation).
+__device__ __forceinline__ void fast_elem(fast::St& s, const DevElem* __restrict__ e) {
+    switch (e->op) {
+    case OP_NOP: return;
+    case OP_DRIFT: fast::drift_elem(s, e->h[H_LEN]); return;
+    case OP_CAVITY: fast::cavity(s, e); return;
+    case OP_APERTURE: fast::aperture(s, e); return;
+    case OP_STRMPOLE: {
+        const int sk = (e->flags & STR_SKEW) ? ((e->flags & STR_SKEW0) ? 1 : 2) : 0;
+        switch (e->order_eff * 4 + sk) {
+        case 0: fast::strmpole<0, 0>(s, e); return;
+        case 1: fast::strmpole<0, 1>(s, e); return;
+        case 2: fast::strmpole<0, 2>(s, e); return;
+        case 4: fast::strmpole<1, 0>(s, e); return;
+        case 5: fast::strmpole<1, 1>(s, e); return;
+        case 6: fast::strmpole<1, 2>(s, e); return;
+        case 8: fast::strmpole<2, 0>(s, e); return;
+        case 9: fast::strmpole<2, 1>(s, e); return;
+        case 10: fast::strmpole<2, 2>(s, e); return;
+        case 12: fast::strmpole<3, 0>(s, e); return;
+        case 13: fast::strmpole<3, 1>(s, e); return;
+        case 14: fast::strmpole<3, 2>(s, e); return;
+        default: break;
+        }
+        break;
+    }
+    case OP_BENDMPOLE: {
+        if (e->flags != 0) break;
+        const bool pure = e->h[H_BK1] == 0.0 && e->h[H_BK2] == 0.0;
+        switch (e->order_eff * 2 + (pure ? 1 : 0)) {
+        case 0: fast::bendmpole<0, false>(s, e, 0, 0, 0); return;
+        case 1: fast::bendmpole<0, true>(s, e, 0, 0, 0); return;
+        case 2: fast::bendmpole<1, false>(s, e, 0, 0, 0); return;
+        case 3: fast::bendmpole<1, true>(s, e, 0, 0, 0); return;
+        case 4: fast::bendmpole<2, false>(s, e, 0, 0, 0); return;
+        case 5: fast::bendmpole<2, true>(s, e, 0, 0, 0); return;
+        case 6: fast::bendmpole<3, false>(s, e, 0, 0, 0); return;
+        case 7: fast::bendmpole<3, true>(s, e, 0, 0, 0); return;
+        default: break;
+        }
+        break;
+    }
+    default: break;
+    }
+    s = literal_elem(s, e);
+}
+
+__device__ __forceinline__ void fast_turn(const AdjParams& a, double* r) {
+    fast::St s{r[0], r[1], r[2], r[3], r[4], r[5]};
+    for (int e = 0; e < a.ne; e++) {
+        fast_elem(s, a.tbl + e);
+        if (s.x != s.x) break;
+    }
+    r[0] = s.x; r[1] = s.px; r[2] = s.y; r[3] = s.py; r[4] = s.z; r[5] = s.d;
+}
+}  // namespace
 
 namespace {
 constexpr unsigned FULL = 0xffffffffu;
@@ -42,7 +112,7 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_fwd(const AdjParams a, doub
     load6(a.st, a.n, p, r);
     for (int t = 0; t < nturn; t++) {
         if (t % every == 0) store6(ckpt + (int64_t)(t / every) * 6 * a.n, a.n, p, r);
-        for (int e = 0; e < a.ne; e++) adj::forward(a.tbl[e], r);
+        if (!(r[0] != r[0])) fast_turn(a, r);
     }
     store6(a.st, a.n, p, r);
 }
@@ -56,8 +126,7 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_recompute(const AdjParams a
     load6(ck, a.n, p, r);
     for (int j = 0; j < nt; j++) {
         store6(turn_tape + (int64_t)j * 6 * a.n, a.n, p, r);
-        if (j + 1 < nt)
-            for (int e = 0; e < a.ne; e++) adj::forward(a.tbl[e], r);
+        if (j + 1 < nt && !(r[0] != r[0])) fast_turn(a, r);
     }
 }
 
@@ -112,6 +181,132 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_turn_reverse(const AdjParam
     }
 }
 
+// ---- block-Jacobian tape -------------------------------------------------------------------------
+// The elements of a turn are cut after each parameter element (one carrying parameters whose
+// gradient is returned): unit c = the plain elements before parameter element c, then element c
+// itself (c = 0 .. npe-1), and a last unit of the plain elements after the last one.  For a chunk
+// of nt turns of the current segment (turn-start states in turn_tape, turns j0 .. j0+nt-1), one
+// thread per (turn, particle) re-tracks its turn with dual numbers restarted at every unit, and
+// stores, with t = turn - j0,
+//   jt[((t * (npe + 1) + c) * 36 + 6 * i + k) * n + p] = d out_i / d in_k of unit c,
+//   st[((t * nparam + q) * 6 + i) * n + p]            = d out_i / d p_q at the output of the
+//                                                        unit whose element carries parameter q.
+// Every turn of the chunk is independent, so this runs nt x n threads wide; the sequential part
+// of the reverse sweep (k_adj_jsweep) is left with 6x6 products and dot products.  A particle lost
+// by the end of the forward run carries no adjoint and is skipped.
+__global__ void __launch_bounds__(128) k_adj_jtape(const AdjParams a, const double* turn_tape, int j0, int nt,
+                                                   const double* final_x, int npe, double* jt, double* sens) {
+    const int64_t n = a.n;
+    const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= n * nt) return;
+    const int t = (int)(gid / n);
+    const int64_t p = gid - (int64_t)t * n;
+    if (final_x[p] != final_x[p]) return;
+    const double* s0 = turn_tape + (int64_t)(j0 + t) * 6 * n;
+    Dual<6> r[6];
+#pragma unroll
+    for (int i = 0; i < 6; i++) {
+        r[i] = Dual<6>(s0[i * n + p]);
+        r[i].d[i] = 1.0;
+    }
+    int c = 0;
+    for (int e = 0; e < a.ne; e++) {
+        const int np = a.pcount[e];
+        if (np == 0) {
+            adj::forward_t(a.tbl[e], r);
+            continue;
+        }
+        const int f = a.pfirst[e];
+        int kind[adj::kMaxParamsPerElem], index[adj::kMaxParamsPerElem];
+        for (int j = 0; j < np; j++) { kind[j] = a.pkind[f + j]; index[j] = a.pindex[f + j]; }
+        Dual<adj::kPD> q[6];
+#pragma unroll
+        for (int i = 0; i < 6; i++) {
+            q[i] = Dual<adj::kPD>(r[i].v);
+#pragma unroll
+            for (int k = 0; k < 6; k++) q[i].d[k] = r[i].d[k];
+        }
+        adj::forward_params(a.tbl[e], q, np, kind, index);
+        double* J = jt + ((int64_t)t * (npe + 1) + c) * 36 * n + p;
+#pragma unroll
+        for (int i = 0; i < 6; i++) {
+#pragma unroll
+            for (int k = 0; k < 6; k++) J[(6 * i + k) * n] = q[i].d[k];
+        }
+        for (int j = 0; j < np; j++) {
+            double* S = sens + ((int64_t)t * a.nparam + f + j) * 6 * n + p;
+#pragma unroll
+            for (int i = 0; i < 6; i++) S[i * n] = q[i].d[6 + j];
+        }
+#pragma unroll
+        for (int i = 0; i < 6; i++) {
+            r[i] = Dual<6>(q[i].v);
+            r[i].d[i] = 1.0;
+        }
+        c++;
+    }
+    double* J = jt + ((int64_t)t * (npe + 1) + npe) * 36 * n + p;
+#pragma unroll
+    for (int i = 0; i < 6; i++)
+#pragma unroll
+        for (int k = 0; k < 6; k++) J[(6 * i + k) * n] = r[i].d[k];
+}
+
+// Reverse sweep over the chunk's turns, last to first, one particle per thread: at each unit's
+// output the parameter gradients take sens^T lam, then lam <- J^T lam.  pelem lists the parameter
+// elements in line order.
+__global__ void __launch_bounds__(kAdjThreads) k_adj_jsweep(const AdjParams a, int nt, const double* final_x,
+                                                            int npe, const int32_t* pelem, const double* jt,
+                                                            const double* sens) {
+    extern __shared__ double rows[];  // [warps][nparam]
+    const int64_t n = a.n;
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    for (int j = threadIdx.x; j < nwarps * a.nparam; j += blockDim.x) rows[j] = 0.0;
+    __syncthreads();
+    const bool alive = p < n && !(final_x[p] != final_x[p]);
+    double lam[6] = {0, 0, 0, 0, 0, 0};
+    if (alive) load6(a.lam, n, p, lam);
+    for (int t = nt - 1; t >= 0; t--) {
+        for (int c = npe; c >= 0; c--) {
+            if (c < npe) {
+                const int e = pelem[c];
+                const int np = a.pcount[e], f = a.pfirst[e];
+                for (int j = 0; j < np; j++) {  // np is the same for every lane (one lattice)
+                    double v = 0.0;
+                    if (alive) {
+                        const double* S = sens + ((int64_t)t * a.nparam + f + j) * 6 * n + p;
+#pragma unroll
+                        for (int i = 0; i < 6; i++) v = fma(S[i * n], lam[i], v);
+                    }
+                    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+                    if (lane == 0) rows[warp * a.nparam + f + j] += v;
+                }
+            }
+            if (alive) {
+                const double* J = jt + ((int64_t)t * (npe + 1) + c) * 36 * n + p;
+                double out[6];
+#pragma unroll
+                for (int k = 0; k < 6; k++) {
+                    double acc = 0.0;
+#pragma unroll
+                    for (int i = 0; i < 6; i++) acc = fma(J[(6 * i + k) * n], lam[i], acc);
+                    out[k] = acc;
+                }
+#pragma unroll
+                for (int k = 0; k < 6; k++) lam[k] = out[k];
+            }
+        }
+    }
+    if (alive) store6(a.lam, n, p, lam);
+    __syncthreads();
+    for (int j = threadIdx.x; j < a.nparam; j += blockDim.x) {
+        double s = 0;
+        for (int w = 0; w < nwarps; w++) s += rows[w * a.nparam + j];
+        a.pgrad_part[(int64_t)blockIdx.x * a.nparam + j] += s;
+    }
+}
+
 __global__ void k_adj_reduce(const double* part, int nblk, int nparam, double* out) {
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nparam; j += gridDim.x * blockDim.x) {
         double s = 0;
@@ -129,6 +324,16 @@ void launch_adj_recompute(const AdjParams& a, const double* ck, double* turn_tap
 void launch_adj_turn_reverse(const AdjParams& a, const double* r_start, const double* final_x, cudaStream_t s) {
     const size_t sh = sizeof(double) * (kAdjThreads / 32) * (size_t)a.nparam;
     k_adj_turn_reverse<<<adj_blocks(a.n), kAdjThreads, sh, s>>>(a, r_start, final_x);
+}
+void launch_adj_jtape(const AdjParams& a, const double* turn_tape, int j0, int nt, const double* final_x,
+                      int npe, double* jt, double* sens, cudaStream_t s) {
+    const int64_t threads = a.n * (int64_t)nt;
+    k_adj_jtape<<<(unsigned)((threads + 127) / 128), 128, 0, s>>>(a, turn_tape, j0, nt, final_x, npe, jt, sens);
+}
+void launch_adj_jsweep(const AdjParams& a, int nt, const double* final_x, int npe, const int32_t* pelem,
+                       const double* jt, const double* sens, cudaStream_t s) {
+    const size_t sh = sizeof(double) * (kAdjThreads / 32) * (size_t)a.nparam;
+    k_adj_jsweep<<<adj_blocks(a.n), kAdjThreads, sh, s>>>(a, nt, final_x, npe, pelem, jt, sens);
 }
 void launch_adj_reduce(const double* part, int nblk, int nparam, double* out, cudaStream_t s) {
     if (nparam > 0) k_adj_reduce<<<(nparam + 127) / 128, 128, 0, s>>>(part, nblk, nparam, out);

@@ -85,5 +85,11 @@ void launch_adj_forward(const AdjParams& a, double* ckpt, int nturn, int every, 
 void launch_adj_recompute(const AdjParams& a, const double* ck, double* turn_tape, int nt, cudaStream_t s);
 void launch_adj_turn_reverse(const AdjParams& a, const double* r_start, const double* final_x, cudaStream_t s);
 void launch_adj_reduce(const double* part, int nblk, int nparam, double* out, cudaStream_t s);
+// block-Jacobian tape of nt turns (unit Jacobians and parameter sensitivities) and the reverse
+// sweep over it (kern_adjoint.cu)
+void launch_adj_jtape(const AdjParams& a, const double* turn_tape, int j0, int nt, const double* final_x,
+                      int npe, double* jt, double* sens, cudaStream_t s);
+void launch_adj_jsweep(const AdjParams& a, int nt, const double* final_x, int npe, const int32_t* pelem,
+                       const double* jt, const double* sens, cudaStream_t s);
 
 }  // namespace accel
