@@ -211,11 +211,12 @@ def config_dict(args, off, aos):
             "seeds": "copy k of rank r: error seed r*copies+k; grid sizes default_rng(12345+r)"}
 
 
-def adjoint_leg(A, LT, ctx, steps: int = 3) -> dict:
+def adjoint_leg(A, LT, ctx, steps: int = 3, ranks=None) -> dict:
     """Gradient of L = sum over particles of (x^2 + y^2) after 512 turns of the 4D DBA (no cavity,
     radiation off), 4,096 Gaussian particles (seed 1), with respect to the 6 x 4,096 initial
     coordinates and the 36 sextupole knobs (mirror pairs of the 72 sextupoles), checkpointed every
-    64 turns.  The adjoint pair and the tracking it is compared with are synchronous host calls on
+    64 turns.  Under torchrun each rank takes its own 4,096 particles (seed 1 + rank) and the knob
+    gradients of all ranks are summed with one all-reduce; times are the max over ranks.  The adjoint pair and the tracking it is compared with are synchronous host calls on
     the context's stream, so wall-clock time around them is device time plus microseconds.
     Finite-difference cost, in tracks of the same 4,096 particles for 512 turns, each priced at
     the faster of the tracker and the adjoint's forward pass: naive central differences per scalar
@@ -227,7 +228,8 @@ def adjoint_leg(A, LT, ctx, steps: int = 3) -> dict:
     elems = sorted({i for p in pairs for i in p})
     params = [(i, A.F_POLYNOMB, 2) for i in elems]
     n, nturn, every = 4096, 512, 64
-    r0 = LT.config4_particles(n, seed=1)
+    rank = ranks.rank if ranks else 0
+    r0 = LT.config4_particles(n, seed=1 + rank)
     adj = A.Adjoint(line, n, nturn, every, params)
 
     def gradient():
@@ -258,9 +260,13 @@ def adjoint_leg(A, LT, ctx, steps: int = 3) -> dict:
     t_track = (time.perf_counter() - t) / steps
     # a finite-difference track costs the fastest forward available for this job: the tracker
     # (untuned for so few particles) or the adjoint's own forward pass over the same turns
+    if ranks:
+        t_adj, t_fwd, t_track = ranks.max(t_adj), ranks.max(t_fwd), ranks.max(t_track)
     t_fd = min(t_track, t_fwd)
     knob = {e: j for j, e in enumerate(elems)}
     dknob = np.array([dp[knob[a]] + dp[knob[b]] for a, b in pairs])
+    if ranks:
+        dknob = ranks.sum_array(dknob)
     n_in = 6 * n + len(pairs)
     naive, batched = 2 * n_in, 2 * (6 + len(pairs))
     adj.close()
@@ -312,6 +318,14 @@ class Ranks:
 
     def max(self, x: float) -> float:
         return self._reduce(x, self.dist.ReduceOp.MAX)
+
+    def sum_array(self, a: np.ndarray) -> np.ndarray:
+        """Element-wise sum over ranks of a float64 array (one all-reduce)."""
+        if self.world == 1:
+            return np.asarray(a, dtype=np.float64)
+        t = self.torch.tensor(np.asarray(a, dtype=np.float64), device=self.dev)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.SUM)
+        return t.cpu().numpy()
 
     def sum(self, x: float) -> float:
         return self._reduce(x, self.dist.ReduceOp.SUM)
@@ -460,7 +474,7 @@ def engine_arm(args):
 
     adjoint = None
     if not args.no_adjoint:
-        adjoint = adjoint_leg(A, LT, ctx)
+        adjoint = adjoint_leg(A, LT, ctx, ranks=ranks)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:

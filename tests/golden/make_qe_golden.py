@@ -1,6 +1,6 @@
 """Quantum-excitation statistics from the reference library itself (oracle/_ref), as fixtures.
 
-    make -C oracle all && python tests/golden/make_qe_golden.py [growth|equilibrium]
+    make -C oracle all && python tests/golden/make_qe_golden.py [growth | equilibrium [BATCH]]
 
 The 18-cell DBA with radiation + quantum excitation (RADQE) and the cavity on; every particle
 starts at the origin, so after T turns the spread is entirely the excitation's (the mean carries
@@ -13,7 +13,9 @@ growth       qe_moments.npz: the moments (mean[6], sigma[6], cross[6], live coun
 equilibrium  qe_equilibrium.npz: a Gaussian bunch (sigma_z 3 mm, sigma_delta 1e-3, 10 nm / 10 pm
              emittances matched to the ring-entrance Twiss) tracked for EQ_TURNS turns, which is
              about three transverse damping times; the moments (mean, sigma, cross, live count)
-             of all particles every EQ_EVERY turns (about an hour on 8 cores).
+             of all particles every EQ_EVERY turns (about an hour on 8 cores).  BATCH b > 0 draws
+             other particles and other srand seeds and writes qe_equilibrium_b<b>.npz, so that
+             independent batches can be pooled.
 """
 from __future__ import annotations
 
@@ -84,22 +86,23 @@ def moments(r):
     return m, sig, cross, int(live.sum())
 
 
-def equilibrium(A, LT, path):
+def equilibrium(A, LT, path, batch=0):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     ring = LT.config2_ring()
     m66 = entrance_m66(A, O, ring)
-    r0 = LT.config5_particles(PROCS * EQ_PER, m66, seed=EQ_SEED)
-    jobs = [(2000 + k, path, r0[k * EQ_PER:(k + 1) * EQ_PER].copy()) for k in range(PROCS)]
+    r0 = LT.config5_particles(PROCS * EQ_PER, m66, seed=EQ_SEED + batch)
+    jobs = [(2000 + 100 * batch + k, path, r0[k * EQ_PER:(k + 1) * EQ_PER].copy()) for k in range(PROCS)]
     with mp.get_context("spawn").Pool(PROCS) as pool:
         parts = pool.map(worker_eq, jobs)
     snaps = np.concatenate(parts, axis=1)  # [snapshot, particle, 6]
     mom = [moments(s) for s in snaps]
     turns = EQ_EVERY * (1 + np.arange(len(snaps)))
-    np.savez_compressed(os.path.join(HERE, "qe_equilibrium.npz"),
+    name = "qe_equilibrium.npz" if batch == 0 else f"qe_equilibrium_b{batch}.npz"
+    np.savez_compressed(os.path.join(HERE, name),
                         mean=np.array([m[0] for m in mom]), sigma=np.array([m[1] for m in mom]),
                         cross=np.array([m[2] for m in mom]), nlive=np.array([m[3] for m in mom]),
-                        turns=turns, m66=m66, seed=np.array([EQ_SEED]), n=np.array([PROCS * EQ_PER]))
+                        turns=turns, m66=m66, seed=np.array([EQ_SEED + batch]), n=np.array([PROCS * EQ_PER]))
     sig = np.array([m[1] for m in mom])
     print("turns", turns, "\nsigma\n", sig, "\nlive", [m[3] for m in mom])
 
@@ -112,7 +115,7 @@ def main():
     os.close(fd)
     A.write_lattice(path, LT.config2_ring())
     if len(sys.argv) > 1 and sys.argv[1] == "equilibrium":
-        equilibrium(A, LT, path)
+        equilibrium(A, LT, path, int(sys.argv[2]) if len(sys.argv) > 2 else 0)
         os.unlink(path)
         return
     with mp.get_context("spawn").Pool(PROCS) as pool:

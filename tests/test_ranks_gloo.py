@@ -1,7 +1,8 @@
 """bench.py's multi-rank plumbing on CPU: two `gloo` ranks, as torchrun would start them.
 
 Covers what the GPU run relies on without a second GPU: the max / sum reductions that turn
-per-rank timings and particle counts into the job's numbers, the barrier, the per-rank workload
+per-rank timings and particle counts into the job's numbers, the all-reduce of the adjoint's knob
+gradients, the barrier, the per-rank workload
 shards (different error seeds and grid sizes on each rank, identical on a re-run), and the
 reference arm, which only rank 0 runs.
 """
@@ -26,6 +27,7 @@ r = bench.Ranks("gloo", timeout_s=60)
 out = {"rank": r.rank, "world": r.world}
 out["max"] = r.max(float(r.rank + 1))
 out["sum"] = r.sum(10.0 * (r.rank + 1))
+out["sum_array"] = r.sum_array(np.arange(4.0) * (r.rank + 1)).tolist()
 r.barrier()
 rings, off, aos, sizes = bench.workload(4, r.rank)
 rings2, off2, aos2, sizes2 = bench.workload(4, r.rank)
@@ -69,6 +71,7 @@ def test_two_gloo_ranks():
     r0, r1 = sorted(res, key=lambda d: d["rank"])
     for r in (r0, r1):
         assert r["world"] == 2 and r["max"] == 2.0 and r["sum"] == 30.0
+        assert r["sum_array"] == [0.0, 3.0, 6.0, 9.0]
         assert r["repeat_identical"]
         assert r["total"] == r0["particles"] + r1["particles"]
     assert r0["sizes"] != r1["sizes"]          # each rank draws its own grids ...
