@@ -85,6 +85,8 @@ def lib() -> C.CDLL:
         "accel_device_count": (I, [C.POINTER(I)]),
         "accel_ctx_create": (I, [I, C.POINTER(P)]),
         "accel_ctx_destroy": (I, [P]),
+        "accel_nccl_unique_id": (I, [C.c_char_p]),
+        "accel_ctx_set_comm": (I, [P, C.c_char_p, I, I]),
         "accel_lattice_read": (I, [C.c_char_p, C.POINTER(pd), C.POINTER(I)]),
         "accel_lattice_parse": (I, [C.c_char_p, C.POINTER(pd), C.POINTER(I)]),
         "accel_lattice_write": (I, [C.c_char_p, pd, I, I]),
@@ -201,6 +203,24 @@ def device_count() -> int:
     return n.value
 
 
+def _process_nccl():
+    """Load torch (when present) before the library loads NCCL: libtorch links its own
+    libnccl.so.2, and a process can hold only one library of that name.  The library's dlopen then
+    returns torch's copy instead of loading another one that torch could not use."""
+    try:
+        import torch  # noqa: F401
+    except ImportError:
+        pass
+
+
+def nccl_unique_id() -> bytes:
+    """A new NCCL communicator id (accel_nccl_unique_id), to be shared with the other ranks."""
+    _process_nccl()
+    buf = C.create_string_buffer(128)
+    _check(lib().accel_nccl_unique_id(buf), "accel_nccl_unique_id")
+    return buf.raw
+
+
 class Context:
     """One CUDA device: streams, scratch buffers, tuned tiles (accel_ctx)."""
 
@@ -220,6 +240,14 @@ class Context:
             self.close()
         except Exception:
             pass
+
+    def set_comm(self, uid: bytes, nranks: int, rank: int):
+        """Join a bunch spread over nranks GPUs (accel_ctx_set_comm); uid from nccl_unique_id()
+        on rank 0, the same bytes on every rank.  Blocks until every rank has joined."""
+        if len(uid) != 128:
+            raise ValueError("uid must be 128 bytes")
+        _process_nccl()
+        _check(lib().accel_ctx_set_comm(self.h, uid, nranks, rank), "accel_ctx_set_comm")
 
     def set_tile(self, block=0, seg_turns=0, variant=-1):
         _check(lib().accel_set_tile(self.h, block, seg_turns, variant), "accel_set_tile")

@@ -22,6 +22,8 @@
 #include <string>
 #include <tuple>
 #include <vector>
+#include <dlfcn.h>
+#include <nccl.h>
 #include "engine.h"
 #include "kernels.h"
 #include "runtime.h"
@@ -130,6 +132,42 @@ static int check_supported(const accel_line* L, int e0, int e1) {
 // ------------------------------------------------------------------------------------------
 // the core: track SoA device state for `nturn` turns through [e0, e1)
 // ------------------------------------------------------------------------------------------
+// ---- NCCL, loaded at run time ----------------------------------------------------------------
+// The library links no NCCL; a context that is given a communicator (accel_ctx_set_comm) loads
+// libnccl.so.2 and resolves the five functions it uses.
+struct NcclApi {
+    bool ok = false;
+    std::string err;
+    ncclResult_t (*GetUniqueId)(ncclUniqueId*) = nullptr;
+    ncclResult_t (*CommInitRank)(ncclComm_t*, int, ncclUniqueId, int) = nullptr;
+    ncclResult_t (*CommDestroy)(ncclComm_t) = nullptr;
+    ncclResult_t (*AllReduce)(const void*, void*, size_t, ncclDataType_t, ncclRedOp_t, ncclComm_t,
+                              cudaStream_t) = nullptr;
+    const char* (*GetErrorString)(ncclResult_t) = nullptr;
+};
+
+static NcclApi& nccl() {
+    static NcclApi api;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* h = dlopen("libnccl.so.2", RTLD_NOW | RTLD_LOCAL);
+        if (!h) h = dlopen("libnccl.so", RTLD_NOW | RTLD_LOCAL);
+        if (!h) { api.err = std::string("cannot load libnccl.so.2: ") + dlerror(); return; }
+        api.GetUniqueId = (decltype(api.GetUniqueId))dlsym(h, "ncclGetUniqueId");
+        api.CommInitRank = (decltype(api.CommInitRank))dlsym(h, "ncclCommInitRank");
+        api.CommDestroy = (decltype(api.CommDestroy))dlsym(h, "ncclCommDestroy");
+        api.AllReduce = (decltype(api.AllReduce))dlsym(h, "ncclAllReduce");
+        api.GetErrorString = (decltype(api.GetErrorString))dlsym(h, "ncclGetErrorString");
+        api.ok = api.GetUniqueId && api.CommInitRank && api.CommDestroy && api.AllReduce && api.GetErrorString;
+        if (!api.ok) api.err = "libnccl.so.2 lacks a required function";
+    });
+    return api;
+}
+
+static int nccl_fail(const char* what, ncclResult_t r) {
+    return fail(ACCEL_E_CUDA, std::string(what) + ": " + nccl().GetErrorString(r));
+}
+
 struct CoreReq {
     accel_line* const* lines;
     int ninst;
@@ -218,10 +256,32 @@ static int emit_part(accel_ctx* C, const CoreReq& q, int part, int turns, cudaSt
         return ACCEL_OK;
     }
     if (turns <= 0) return ACCEL_OK;
+    int coll_status = ACCEL_OK;
     auto coll = [&](int k) {
         if (L0->desc[k].type == ACCEL_LONGWAKE) {
-            launch_longwake(P, q.tables + k, L0->host_tbl[k], (double*)C->scratch.p, (int32_t*)C->iscratch.p, s);
-            launches += L0->host_tbl[k].flags ? 5 : 2;
+            double* scr = (double*)C->scratch.p;
+            int32_t* counts = (int32_t*)C->iscratch.p;
+            if (!C->comm) {
+                launch_longwake(P, q.tables + k, L0->host_tbl[k], scr, counts, s);
+                launches += L0->host_tbl[k].flags ? 5 : 2;
+                return;
+            }
+            // the bunch is spread over the communicator's ranks: exchange its z range and live
+            // count, then its bin counts (every rank takes the same steps: same lattice)
+            const LwParams w = longwake_params(L0->host_tbl[k]);
+            ncclComm_t cm = (ncclComm_t)C->comm;
+            launch_longwake_stage(1, P, w, scr, counts, s);
+            launches += 2;
+            if (!w.on) return;
+            ncclResult_t r = nccl().AllReduce(scr + 0, scr + 0, 1, ncclFloat64, ncclMin, cm, s);
+            if (r == ncclSuccess) r = nccl().AllReduce(scr + 1, scr + 1, 1, ncclFloat64, ncclMax, cm, s);
+            if (r == ncclSuccess) r = nccl().AllReduce(scr + 4, scr + 4, 1, ncclFloat64, ncclSum, cm, s);
+            launch_lw_regeom(scr, w.nbins, w.charge, s);
+            launch_longwake_stage(2, P, w, scr, counts, s);
+            if (r == ncclSuccess) r = nccl().AllReduce(counts, counts, (size_t)w.nbins, ncclInt32, ncclSum, cm, s);
+            launch_longwake_stage(3, P, w, scr, counts, s);
+            launches += 4;
+            if (r != ncclSuccess && coll_status == ACCEL_OK) coll_status = nccl_fail("ncclAllReduce (wake)", r);
         } else {
             launch_transwake(P, q.tables + k, L0->host_tbl[k], nullptr, s);
             launches += 3;
@@ -273,7 +333,7 @@ static int emit_part(accel_ctx* C, const CoreReq& q, int part, int turns, cudaSt
         launch_plain_turn_end(P, cnt + 3, s);
         launches += 2;
     }
-    return ACCEL_OK;
+    return coll_status;
 }
 
 static int capture_part(accel_ctx* C, const CoreReq& q, int part, int turns, cudaGraphExec_t* out,
@@ -339,7 +399,8 @@ static int run_core(accel_ctx* C, const CoreReq& q, cudaStream_t user) {
                  (int64_t)q.variant, (int64_t)plan.seg, (int64_t)q.sched, (int64_t)(intptr_t)q.st, (int64_t)(intptr_t)q.loss,
                  (int64_t)(intptr_t)q.tables, (int64_t)(intptr_t)q.tbl_off, (int64_t)(intptr_t)q.pinst,
                  (int64_t)q.probe, (int64_t)(intptr_t)C->live0.p, (int64_t)(intptr_t)C->cnt.p,
-                 (int64_t)(intptr_t)C->scratch.p, (int64_t)(intptr_t)C->iscratch.p};
+                 (int64_t)(intptr_t)C->scratch.p, (int64_t)(intptr_t)C->iscratch.p,
+                 (int64_t)(intptr_t)C->comm};
         for (int i = 0; i < q.ninst && i < 4; i++) {
             key.v.push_back((int64_t)(intptr_t)q.lines[i]);
             key.v.push_back(q.lines[i]->version);
@@ -443,6 +504,7 @@ void ctx_unref(accel_ctx* C) {
     if (C->refs.fetch_sub(1) != 1) return;
     cudaSetDevice(C->device);
     cudaStreamSynchronize(C->stream);
+    if (C->comm) nccl().CommDestroy((ncclComm_t)C->comm);
     delete C;
 }
 
@@ -467,6 +529,40 @@ extern "C" {
 int accel_ctx_destroy(accel_ctx* C) {
     if (!C) return ACCEL_OK;
     accel::ctx_unref(C);
+    return ACCEL_OK;
+}
+
+int accel_nccl_unique_id(unsigned char* id) {
+    if (!id) return fail(ACCEL_E_INVALID, "id is NULL");
+    NcclApi& api = nccl();
+    if (!api.ok) return fail(ACCEL_E_UNSUPPORTED, api.err);
+    ncclUniqueId u;
+    ncclResult_t r = api.GetUniqueId(&u);
+    if (r != ncclSuccess) return nccl_fail("ncclGetUniqueId", r);
+    std::memcpy(id, u.internal, NCCL_UNIQUE_ID_BYTES);
+    return ACCEL_OK;
+}
+
+int accel_ctx_set_comm(accel_ctx* C, const unsigned char* id, int nranks, int rank) {
+    if (!C || !id || nranks < 1 || rank < 0 || rank >= nranks) return fail(ACCEL_E_INVALID, "bad argument");
+    NcclApi& api = nccl();
+    if (!api.ok) return fail(ACCEL_E_UNSUPPORTED, api.err);
+    std::lock_guard<std::mutex> lk(C->mu);
+    CK(cudaSetDevice(C->device));
+    CK(cudaStreamSynchronize(C->stream));
+    if (C->comm) {
+        api.CommDestroy((ncclComm_t)C->comm);
+        C->comm = nullptr;
+        C->nranks = 1;
+    }
+    C->graphs.clear();
+    ncclUniqueId u;
+    std::memcpy(u.internal, id, NCCL_UNIQUE_ID_BYTES);
+    ncclComm_t cm = nullptr;
+    ncclResult_t r = api.CommInitRank(&cm, nranks, u, rank);
+    if (r != ncclSuccess) return nccl_fail("ncclCommInitRank", r);
+    C->comm = cm;
+    C->nranks = nranks;
     return ACCEL_OK;
 }
 

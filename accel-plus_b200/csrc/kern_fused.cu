@@ -406,26 +406,52 @@ __global__ void __launch_bounds__(kLwThreads) k_lw_kick(TrackParams P, const dou
     }
 }
 
+// The wake in three stages, so that a multi-GPU run can exchange the bunch's z range and count
+// after stage 1 and its bin counts after stage 2 (capi.cpp).  Stage 1: first half drift, z range
+// and live count, local bin geometry, zeroed counts (with the wake off, also the second half
+// drift: the element is then done).  Stage 2: histogram.  Stage 3: wake potential and kick, then
+// the second half drift.
+LwParams longwake_params(const DevElem& e) {
+    LwParams w;
+    w.half = 0.5 * e.v[V_LEN];
+    w.energy = e.v[V_W + 0];
+    w.charge = e.v[V_W + 1];
+    w.Rs = e.v[V_W + 2];
+    w.fr = e.v[V_W + 3];
+    w.Q = e.v[V_W + 4];
+    w.nbins = (int)e.v[V_W + 5];
+    if (w.nbins < 1) w.nbins = 1;
+    if (w.nbins > 4096) w.nbins = 4096;
+    w.on = e.flags != 0;
+    return w;
+}
+
+void launch_longwake_stage(int stage, const TrackParams& p, const LwParams& w, double* scr, int32_t* counts,
+                           cudaStream_t s) {
+    if (stage == 1) {
+        k_lw_drift_minmax<<<kLwBlocks, kLwThreads, 0, s>>>(p, w.half, scr);
+        if (!w.on) {
+            // wake off: the second half drift still applies
+            k_lw_kick<<<kLwBlocks, kLwThreads, 0, s>>>(p, scr, 0, 0.0, w.half);
+            return;
+        }
+        k_lw_setup<<<1, 256, 0, s>>>(scr, counts, w.nbins, w.charge);
+    } else if (stage == 2) {
+        k_lw_hist<<<kLwBlocks, kLwThreads, w.nbins * sizeof(int), s>>>(p, scr, counts, w.nbins);
+    } else {
+        k_lw_voltage<<<1, 256, w.nbins * sizeof(double), s>>>(scr, counts, w.nbins, w.Rs, w.fr, w.Q);
+        k_lw_kick<<<kLwBlocks, kLwThreads, 0, s>>>(p, scr, w.nbins, 1.0 / (w.energy * 1e6), w.half);
+    }
+}
+
 void launch_longwake(const TrackParams& p, const DevElem* e_dev, const DevElem& e, double* scr,
                      int32_t* counts, cudaStream_t s) {
     (void)e_dev;
-    const double len = e.v[V_LEN];
-    const double energy = e.v[V_W + 0], charge = e.v[V_W + 1], Rs = e.v[V_W + 2], fr = e.v[V_W + 3],
-                 Q = e.v[V_W + 4];
-    int nbins = (int)e.v[V_W + 5];
-    if (nbins < 1) nbins = 1;
-    if (nbins > 4096) nbins = 4096;
-    const double half = 0.5 * len;
-    k_lw_drift_minmax<<<kLwBlocks, kLwThreads, 0, s>>>(p, half, scr);
-    if (!e.flags) {
-        // wake off: the second half drift still applies
-        k_lw_kick<<<kLwBlocks, kLwThreads, 0, s>>>(p, scr, 0, 0.0, half);
-        return;
-    }
-    k_lw_setup<<<1, 256, 0, s>>>(scr, counts, nbins, charge);
-    k_lw_hist<<<kLwBlocks, kLwThreads, nbins * sizeof(int), s>>>(p, scr, counts, nbins);
-    k_lw_voltage<<<1, 256, nbins * sizeof(double), s>>>(scr, counts, nbins, Rs, fr, Q);
-    k_lw_kick<<<kLwBlocks, kLwThreads, 0, s>>>(p, scr, nbins, 1.0 / (energy * 1e6), half);
+    const LwParams w = longwake_params(e);
+    launch_longwake_stage(1, p, w, scr, counts, s);
+    if (!w.on) return;
+    launch_longwake_stage(2, p, w, scr, counts, s);
+    launch_longwake_stage(3, p, w, scr, counts, s);
 }
 
 // ---- transverse resonator wake, O(N^2) pairwise as ATransWake::pass (accel.cpp:1603-1657) ----

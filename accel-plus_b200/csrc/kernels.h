@@ -52,6 +52,13 @@ void launch_longwake(const TrackParams& p, const DevElem* e_dev, const DevElem& 
 void launch_transwake(const TrackParams& p, const DevElem* e_dev, const DevElem& e_host,
                       double* xsnap, cudaStream_t s);
 size_t longwake_scratch_doubles(int nbins);
+// the longitudinal wake in stages, for runs whose bunch is spread over several GPUs
+struct LwParams { double half, energy, charge, Rs, fr, Q; int nbins; bool on; };
+LwParams longwake_params(const DevElem& e_host);
+void launch_longwake_stage(int stage, const TrackParams& p, const LwParams& w, double* scratch,
+                           int32_t* counts, cudaStream_t s);
+// scratch[0..5] from the exchanged z range and count (kern_coll.cu)
+void launch_lw_regeom(double* scratch, int nbins, double charge_nc, cudaStream_t s);
 // moments of live particles: out[0..5] mean, [6..11] sigma, [12..17] cross, [18] nlive
 void launch_beam_stat(const double* st, int64_t n, double* partial, int nblk, double* out,
                       cudaStream_t s);

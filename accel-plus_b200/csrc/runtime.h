@@ -65,6 +65,8 @@ struct accel_ctx {
     int64_t launches = 0;
     bool profile = false;                  // direct launches with events (accel_profile_enable)
     std::vector<cudaEvent_t> prof_events;  // [begin, end] per tracking launch, then whole call
+    void* comm = nullptr;                  // NCCL communicator of a bunch spread over GPUs
+    int nranks = 1;
     ~accel_ctx();
 };
 

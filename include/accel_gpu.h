@@ -148,6 +148,19 @@ int  accel_device_count(int* n);
 int  accel_ctx_create(int device, accel_ctx** out);
 int  accel_ctx_destroy(accel_ctx* ctx);
 
+/* A bunch spread over several GPUs, one process and one context each (no counterpart in the
+ * reference, which runs on one host).  Rank 0 makes an id with accel_nccl_unique_id and sends it
+ * to the other ranks (e.g. over torch.distributed); every rank then calls accel_ctx_set_comm with
+ * the same id.  From then on each longitudinal wake element of the context's tracking exchanges
+ * the bunch's z range, live count and bin counts over NCCL, so every rank kicks its particles
+ * with the whole bunch's wake.  libnccl.so.2 is loaded at run time; without it both calls return
+ * ACCEL_E_UNSUPPORTED.  A process holds one libnccl.so.2: where another component (PyTorch) links
+ * its own, load that component first and the library uses its copy.  accel_ctx_set_comm blocks
+ * until all nranks ranks have called it.  Every rank must then issue the same tracking calls in
+ * the same order.                                                                              */
+int  accel_nccl_unique_id(unsigned char id[128]);
+int  accel_ctx_set_comm(accel_ctx* ctx, const unsigned char id[128], int nranks, int rank);
+
 /* ---- lattice files (host only; no GPU needed) ----------------------------------------------
  * accel_lattice_read follows AccelElement::deserialize (accel.cpp:67-133) and the per-type
  * create() readers; it allocates *elems with malloc (free with accel_lattice_free).          */

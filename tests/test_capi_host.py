@@ -113,3 +113,9 @@ def test_model_flops_match_survey_formula(A, LT):
     ring = LT.config1_ring()
     per_cell = 2 * 10 * (52 + 3 * 12) + 2 * 10 * (52 + 3 * 20) + 2 * (10 * (184 + 3 * 44) + 8) + 4 * 14
     assert LT.flops_per_turn(ring) == 32 * per_cell
+
+
+def test_nccl_unique_id_without_a_gpu(A):
+    """The communicator id is made on the host (NCCL is loaded at run time); ids differ."""
+    a, b = A.nccl_unique_id(), A.nccl_unique_id()
+    assert len(a) == len(b) == 128 and a != b and any(a)

@@ -64,3 +64,57 @@ def test_quantum_excitation_is_reproducible_and_seeded(A, ctx, LT):
         runs.append(r)
     assert np.array_equal(runs[0], runs[1])
     assert not np.array_equal(runs[0], runs[2])
+
+
+def pooled(files, snap):
+    """Mean and the second moments <xx>, <x'x'>, <xx'>, <x d>, <x' d>, <zz>, <dd> of several
+    independent reference batches pooled at snapshot `snap`."""
+    ns = [float(f["nlive"][snap]) for f in files]
+    N = sum(ns)
+    mu = sum(n * f["mean"][snap] for n, f in zip(ns, files)) / N
+
+    def cov(a, b, f):
+        if a == b:
+            return f["sigma"][snap][a] ** 2
+        pairs = [(0, 1), (2, 3), (0, 5), (1, 5), (2, 4), (3, 4)]
+        return f["cross"][snap][pairs.index((a, b))]
+
+    def pool(a, b):
+        return sum(n * (cov(a, b, f) + (f["mean"][snap][a] - mu[a]) * (f["mean"][snap][b] - mu[b]))
+                   for n, f in zip(ns, files)) / N
+    return {k: pool(*k) for k in [(0, 0), (1, 1), (0, 1), (0, 5), (1, 5), (4, 4), (5, 5)]}, N
+
+
+def emittance_x(c):
+    """Horizontal emittance with the dispersive (delta-correlated) part of x and x' removed."""
+    dd = c[(5, 5)]
+    xx = c[(0, 0)] - c[(0, 5)] ** 2 / dd
+    pp = c[(1, 1)] - c[(1, 5)] ** 2 / dd
+    xp = c[(0, 1)] - c[(0, 5)] * c[(1, 5)] / dd
+    return np.sqrt(xx * pp - xp * xp)
+
+
+def test_quantum_excitation_equilibrium(A, ctx, LT):
+    """Equilibrium emittance and bunch length after 10,000 turns (about three transverse damping
+    times) of RADQE tracking from the matched Gaussian bunch (sigma_z 3 mm, sigma_delta 1e-3,
+    10 nm / 10 pm), against the reference's moments pooled over its independent batches
+    (tests/golden/qe_equilibrium*.npz): horizontal emittance, bunch length and energy spread within
+    2 %.  The engine tracks 131,072 particles drawn from the same distribution."""
+    import glob
+    files = [np.load(p) for p in sorted(glob.glob(os.path.join(GOLDEN, "qe_equilibrium*.npz")))]
+    turns = files[0]["turns"]
+    ref, n_ref = pooled(files, len(turns) - 1)
+    n = 131072
+    r = LT.config5_particles(n, files[0]["m66"], seed=777)
+    line = A.Line(ctx, LT.config2_ring())
+    line.set_flags(rad=A.RAD_RADQE, cavity=1)
+    line.set_seed(97531)
+    line.track(r, int(turns[-1]))
+    live = ~np.isnan(r[:, 0])
+    assert live.all()
+    d = r - r.mean(axis=0)
+    mine = {(a, b): float((d[:, a] * d[:, b]).mean()) for (a, b) in ref}
+    for name, g, w in (("emittance_x", emittance_x(mine), emittance_x(ref)),
+                       ("sigma_z", np.sqrt(mine[(4, 4)]), np.sqrt(ref[(4, 4)])),
+                       ("sigma_delta", np.sqrt(mine[(5, 5)]), np.sqrt(ref[(5, 5)]))):
+        assert abs(g - w) <= 0.02 * w, (name, g, w, n_ref)

@@ -1,0 +1,51 @@
+"""The longitudinal wake of a bunch spread over GPUs, on the one GPU a test gets.
+
+With a communicator, every wake element runs in stages with NCCL exchanges in between: the
+bunch's z range and live count (min / max / sum), then its bin counts (sum), after which the bin
+geometry is recomputed from the exchanged values.  A one-rank communicator exchanges with itself,
+so the staged path must reproduce the single-GPU wake bit for bit: the same kernels, the same
+formulas, and NCCL inside the captured tracking graphs.  Runs over several ranks need several GPUs;
+they take the same code path with real peers.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def ring_with_wake(A, LT):
+    ring = LT.config2_ring()
+    return ring[:-1] + [LT.longwake_elem()] + ring[-1:]  # wake before the aperture
+
+
+def test_one_rank_exchange_reproduces_local_wake(A, LT):
+    rng = np.random.default_rng(12)
+    n = 20000
+    r0 = np.zeros((n, 6))
+    r0[:, 0] = rng.normal(0, 2e-4, n)
+    r0[:, 2] = rng.normal(0, 2e-5, n)
+    r0[:, 4] = rng.normal(0, 3e-3, n)
+    r0[:, 5] = rng.normal(0, 1e-3, n)
+    out = []
+    for with_comm in (False, True):
+        ctx = A.Context(0)
+        if with_comm:
+            ctx.set_comm(A.nccl_unique_id(), 1, 0)
+        line = A.Line(ctx, ring_with_wake(A, LT))
+        r = r0.copy()
+        lt = np.empty(n, dtype=np.int32)
+        line.track(r, 30, loss=lt)
+        out.append((r, lt))
+        line.close()
+        ctx.close()
+    (a, la), (b, lb) = out
+    assert np.array_equal(la, lb)
+    assert np.array_equal(a, b, equal_nan=True)
+    # the wake did act: the same ring without it ends elsewhere
+    ctx = A.Context(0)
+    line = A.Line(ctx, LT.config2_ring())
+    c = r0.copy()
+    line.track(c, 30)
+    assert not np.array_equal(a, c, equal_nan=True)
