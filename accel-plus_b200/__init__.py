@@ -115,6 +115,7 @@ def lib() -> C.CDLL:
         "accel_adjoint_backward": (I, [P, P, P, P]),
         "accel_beam_stat": (I, [P, P, I, I, C.POINTER(D), C.POINTER(D), C.POINTER(D), C.POINTER(I)]),
         "accel_beam_stat_noalloc": (I, [P, I, C.c_int64, P, P]),
+        "accel_naff": (I, [P, I, D, D, C.POINTER(D)]),
         "accel_fp64_peak": (I, [P, C.POINTER(D)]),
         "accel_launch_count": (I, [P, C.POINTER(C.c_int64)]),
         "accel_profile_enable": (I, [P, I]),
@@ -211,6 +212,14 @@ def _process_nccl():
         import torch  # noqa: F401
     except ImportError:
         pass
+
+
+def naff(record, xlow: float = 0.0, xhi: float = 0.5) -> float:
+    """Tune of a turn-by-turn record (accel_naff; host only)."""
+    x = np.ascontiguousarray(record, dtype=np.float64)
+    nu = C.c_double()
+    _check(lib().accel_naff(C.c_void_p(x.ctypes.data), len(x), xlow, xhi, C.byref(nu)), "accel_naff")
+    return nu.value
 
 
 def nccl_unique_id() -> bytes:

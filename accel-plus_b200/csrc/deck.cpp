@@ -12,11 +12,11 @@
 //   Optics   print_tune  print_chrom  print_matrix  print_optics
 //   Track    Distribution (none | Zero NPar= | Coordinate r=(..;..) | Gaussian .. | Linear ..
 //            | Load F[, format=plain|accel-export]; shift=(..); Print)  Monitor  Do_Track  Transport
-//   DAMA     track_DA  track_MA
+//   DAMA     track_DA  track_MA  track_dNudJ
 // Differences: Gaussian distributions come from a seeded generator (--seed; the reference seeds
 // rand() with the time, process.cpp:42); Transport prints the transported coordinates (the
-// reference prints the untransported array, process.cpp:2201); apply_setpt and track_dNudJ are
-// reported as not supported.
+// reference prints the untransported array, process.cpp:2201); apply_setpt is reported as not
+// supported.
 #include <algorithm>
 #include <cctype>
 #include <cmath>
@@ -725,8 +725,21 @@ void Deck::dama(std::istream& in) {
             for (unsigned i = 0; i < nmoni; i++) cout << dp[i] << " \t" << dm[i] << " \t" << endl;
             cout << "#" << now() << endl;
             cout << "******************************" << endl;
+        } else if (k == 3) {
+            // track_dNudJ: amplitude-dependent tune shift (process.cpp:2590-2628)
+            double xm = std::atof(get(a, "XMAX").c_str()), ym = std::atof(get(a, "YMAX").c_str());
+            unsigned nturn = (unsigned)std::atoi(get(a, "NTURN").c_str());
+            cout << "#" << xm << " " << ym << " " << nturn << endl;
+            double d[4];
+            L->set_monitor(0, 0);
+            L->set_rad_onoff(0);
+            L->set_cavity_onoff(false);
+            L->trackdnudexy(d, nturn, xm, ym, &cout);
+            cout << "$$$dtuning coefficients" << endl;
+            cout << d[0] << " \t" << d[1] << " \t" << d[2] << " \t" << d[3] << " \t" << endl;
+            cout << "*************************" << endl;
         } else {
-            cout << (k == 0 ? "apply_setpt" : "track_dNudJ") << ": not supported by this engine" << endl;
+            cout << "apply_setpt: not supported by this engine" << endl;
         }
     }
 }

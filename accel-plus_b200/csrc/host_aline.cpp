@@ -62,6 +62,92 @@ double tune_of(const double* m, int k) { return std::acos((m[6 * k + k] + m[6 * 
 
 const char* elem_type_name(int type) { return accel::type_name(type); }
 
+// ---- NAFF ----------------------------------------------------------------------------------------
+namespace {
+// -|windowed projection| at frequency nu (the quantity the search minimises)
+double projection(double nu, int N, const double* X) {
+    double re = 0, im = 0;
+    for (int i = 0; i < N; i++) {
+        const double ph = 2 * kPi * nu * i;
+        const double w = std::pow(std::sin(kPi * i / N), 4);
+        re += std::cos(ph) * X[i] * w;
+        im -= std::sin(ph) * X[i] * w;
+    }
+    return -std::sqrt(re * re + im * im);
+}
+
+// power of the packed real spectrum at even index i: (F_0^2 + F_{N/2}^2) at 0, |F_{i/2}|^2 else
+double packed_power(int N, const double* X, int i) {
+    auto dft = [&](int k, double& re, double& im) {
+        re = im = 0;
+        for (int j = 0; j < N; j++) {
+            const double ph = 2 * kPi * (double)k * j / N;
+            re += X[j] * std::cos(ph);
+            im += X[j] * std::sin(ph);
+        }
+    };
+    double r0, i0, r1, i1;
+    if (i == 0) {
+        dft(0, r0, i0);
+        dft(N / 2, r1, i1);
+        return r0 * r0 + r1 * r1;
+    }
+    dft(i / 2, r0, i0);
+    return r0 * r0 + i0 * i0;
+}
+
+// golden-section search for a minimum of f on [a, c] with interior guess b
+template <class F>
+double golden_min(F f, double a, double b, double c, double tol) {
+    const double R = 0.61803398874989484820, C = 1 - R;
+    double x0 = a, x3 = c, x1, x2;
+    if (std::fabs(c - b) > std::fabs(b - a)) { x1 = b; x2 = b + C * (c - b); }
+    else { x2 = b; x1 = b - C * (b - a); }
+    double f1 = f(x1), f2 = f(x2);
+    while (std::fabs(x3 - x0) > tol * (std::fabs(x1) + std::fabs(x2))) {
+        if (f2 < f1) {
+            x0 = x1; x1 = x2; x2 = R * x2 + C * x3;
+            f1 = f2; f2 = f(x2);
+        } else {
+            x3 = x2; x2 = x1; x1 = R * x1 + C * x0;
+            f2 = f1; f1 = f(x1);
+        }
+    }
+    return f1 < f2 ? x1 : x2;
+}
+
+void fit_slope(int n, const double* x, const double* y, double& slope) {
+    double sx = 0, sy = 0;
+    for (int i = 0; i < n; i++) { sx += x[i]; sy += y[i]; }
+    const double mx = sx / n, my = sy / n;
+    double sxx = 0, sxy = 0;
+    for (int i = 0; i < n; i++) { sxx += (x[i] - mx) * (x[i] - mx); sxy += (x[i] - mx) * (y[i] - my); }
+    slope = sxy / sxx;
+}
+
+unsigned pow2_at_least(unsigned n) {
+    unsigned nt = 1;
+    while (nt < n) nt <<= 1;
+    return nt;
+}
+}  // namespace
+
+double naff(int N, const double* X, double xlow, double xhi) {
+    xlow = std::max(xlow, 0.9 / N);
+    xhi = std::min(0.5, xhi);
+    const int ilow = ((int)(xlow * N * 2) >> 1) << 1;
+    const int ihi = ((int)(xhi * N * 2) >> 1) << 1;
+    int im = ilow;
+    double fm = packed_power(N, X, ilow);
+    for (int i = ilow + 2; i < ihi; i += 2) {
+        const double f = packed_power(N, X, i);
+        if (f > fm) { im = i; fm = f; }
+    }
+    xlow = std::max(xlow, (im - 2) * 1.0 / N / 2.0);
+    xhi = std::min(xhi, (im + 2) * 1.0 / N / 2.0);
+    return golden_min([&](double nu) { return projection(nu, N, X); }, xlow, 0.5 * (xlow + xhi), xhi, 3.0e-8);
+}
+
 void Twiss::serialize(std::ostream& os) const {
     os << s << "\t" << betx << "\t" << bety << "\t" << alfx << "\t" << alfy << "\t" << psix << "\t" << psiy << "\t" << std::endl;
 }
@@ -409,6 +495,98 @@ double ALine::trackMA(double dppmax, double dppmin, int nturn, unsigned nstep, d
     return avg;
 }
 
+// ---- turn-by-turn tunes -------------------------------------------------------------------------
+// r: AoS particles; x and y of every particle before each of nt turns into xs[p * nt + t],
+// ys[p * nt + t] (a lost particle records NaN from then on)
+static int record_tbt(ALine& L, std::vector<double>& r, int np, unsigned nt, std::vector<double>& xs,
+                      std::vector<double>& ys) {
+    xs.assign((size_t)np * nt, 0.0);
+    ys.assign((size_t)np * nt, 0.0);
+    for (unsigned t = 0; t < nt; t++) {
+        for (int p = 0; p < np; p++) {
+            xs[(size_t)p * nt + t] = r[(size_t)6 * p];
+            ys[(size_t)p * nt + t] = r[(size_t)6 * p + 2];
+        }
+        if (t + 1 < nt) {
+            int s = L.pass(r.data(), np, 0, L.getnumber());
+            if (s) return s;
+        }
+    }
+    return ACCEL_OK;
+}
+
+void ALine::tracktune(double& tunex, double& tuney, unsigned nturn, double x0, double y0, double xlow,
+                      double xhi, double ylow, double yhi) {
+    const unsigned nt = pow2_at_least(nturn);
+    std::vector<double> r(6, 0.0), xs, ys;
+    r[0] = x0;
+    r[2] = y0;
+    if ((status_ = record_tbt(*this, r, 1, nt, xs, ys))) { tunex = tuney = NAN; return; }
+    tunex = naff((int)nt, xs.data(), xlow, xhi);
+    tuney = naff((int)nt, ys.data(), ylow, yhi);
+}
+
+double ALine::trackDiffusion(int nturn, unsigned np, const double* x0, const double* y0, double* nux,
+                             double* nuy, double* dif, double xlow, double xhi, double ylow, double yhi) {
+    const unsigned nt = pow2_at_least((unsigned)std::max(1, nturn));
+    const double mdiffu = -4 * std::log(nt * 1.0);
+    std::vector<double> r((size_t)6 * np, 0.0), xs, ys;
+    for (unsigned p = 0; p < np; p++) { r[(size_t)6 * p] = x0[p]; r[(size_t)6 * p + 2] = y0[p]; }
+    if ((status_ = record_tbt(*this, r, (int)np, nt, xs, ys))) return NAN;
+    double tdif = 0;
+    const int h = (int)(nt >> 1);
+    for (unsigned p = 0; p < np; p++) {
+        const double* xl = xs.data() + (size_t)p * nt;
+        const double* yl = ys.data() + (size_t)p * nt;
+        if (std::isnan(xl[nt - 1])) {
+            nux[p] = nuy[p] = dif[p] = NAN;
+            tdif += -3.0;
+            continue;
+        }
+        const double nux0 = naff(h, xl, xlow, xhi), nuy0 = naff(h, yl, ylow, yhi);
+        const double nux1 = naff(h, xl + h, xlow, xhi), nuy1 = naff(h, yl + h, ylow, yhi);
+        nux[p] = nux0;
+        nuy[p] = nuy0;
+        const double d = std::hypot(nux1 - nux0, nuy1 - nuy0);
+        dif[p] = std::max(mdiffu, std::log(d * 2.0 / nt));
+        tdif += dif[p];
+    }
+    return tdif;
+}
+
+void ALine::trackdnudexy(double* dnudexy, unsigned nturn, double xm, double ym, std::ostream* log) {
+    Twiss tw;
+    calctwiss(tw);
+    const double tunex = tw.psix / 2 / kPi, tuney = tw.psiy / 2 / kPi;
+    const int np = 6;
+    const double tiny = 1.0e-5;
+    const unsigned nt = pow2_at_least(nturn);
+    // 6 horizontal amplitudes, then 6 vertical ones, tracked together
+    std::vector<double> r((size_t)6 * 2 * np, 0.0), de(2 * np), xs, ys;
+    for (int k = 0; k < np; k++) {
+        double* a = &r[(size_t)6 * k];
+        a[0] = tiny + k * 1.0 / (np - 1) * xm;
+        a[2] = tiny + a[0] * .02;
+        de[k] = a[0] * a[0] / tw.betx;
+        double* b = &r[(size_t)6 * (np + k)];
+        b[2] = tiny + k * 1.0 / (np - 1) * ym;
+        b[0] = tiny + b[2] * .02;
+        de[np + k] = b[2] * b[2] / tw.bety;
+    }
+    for (int q = 0; q < 4; q++) dnudexy[q] = NAN;
+    if ((status_ = record_tbt(*this, r, 2 * np, nt, xs, ys))) return;
+    std::vector<double> xt(2 * np), yt(2 * np);
+    for (int k = 0; k < 2 * np; k++) {
+        xt[k] = naff((int)nt, xs.data() + (size_t)k * nt, std::max(0.0, tunex - 0.1), std::min(0.5, tunex + 0.1));
+        yt[k] = naff((int)nt, ys.data() + (size_t)k * nt, std::max(0.0, tuney - 0.1), std::min(0.5, tuney + 0.1));
+        if (log) *log << de[k] << "\t" << xt[k] << "\t" << yt[k] << std::endl;
+    }
+    fit_slope(np, de.data(), xt.data(), dnudexy[0]);
+    fit_slope(np, de.data(), yt.data(), dnudexy[1]);
+    fit_slope(np, de.data() + np, xt.data() + np, dnudexy[2]);
+    fit_slope(np, de.data() + np, yt.data() + np, dnudexy[3]);
+}
+
 // ---- optics --------------------------------------------------------------------------------------
 int ALine::getm66(double* m, unsigned st, unsigned ed, double dpp, double delta, bool exact) {
     if ((status_ = sync())) return status_;
@@ -655,3 +833,9 @@ int ALine::correct_chrom_exact(double& chromx, double& chromy, unsigned nfam1, u
 }
 
 }  // namespace accelgpu
+
+extern "C" int accel_naff(const double* data, int n, double xlow, double xhi, double* nu) {
+    if (!data || !nu || n < 4) return accel::fail(ACCEL_E_INVALID, "accel_naff: need data, nu and n >= 4");
+    *nu = accelgpu::naff(n, data, xlow, xhi);
+    return ACCEL_OK;
+}

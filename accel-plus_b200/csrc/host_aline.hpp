@@ -90,6 +90,18 @@ public:
     // second-order chromaticity: half the least-squares slope of the chromaticity over the 11
     // momentum offsets 1e-3 * (i - 6), i = 0..10 (aline.cpp:1127-1158)
     void calcchrom2(double& chromx, double& chromy, double& chromx2, double& chromy2);
+
+    // turn-by-turn tunes (aline.cpp:1159-1185, 716-779, 1421-1500).  Particles are tracked
+    // together on the device, one turn per call, their x and y recorded before every turn; the
+    // record length is nturn rounded up to a power of two, as the reference does.
+    void tracktune(double& tunex, double& tuney, unsigned nturn, double x0, double y0,
+                   double xlow = 0, double xhi = 0.5, double ylow = 0, double yhi = 0.5);
+    double trackDiffusion(int nturn, unsigned np, const double* x0, const double* y0, double* nux,
+                          double* nuy, double* dif, double xlow = 0, double xhi = 0.5,
+                          double ylow = 0, double yhi = 0.5);
+    // amplitude-dependent tune shift: dnux/dex, dnuy/dex, dnux/dey, dnuy/dey (slopes of the tunes
+    // at 6 amplitudes against 2J = x^2/beta); per-amplitude lines "2J  nux  nuy" go to `log`
+    void trackdnudexy(double* dnudexy, unsigned nturn, double xm, double ym, std::ostream* log = nullptr);
     // one difference-response step, as the reference (aline.cpp:1243-1418)
     void correcttune(double& tunex, double& tuney, unsigned nfam1, unsigned nfam2,
                      const unsigned* lfam1, const unsigned* lfam2);
@@ -119,6 +131,11 @@ private:
 };
 
 double tune_of(const double* m, int plane);  // acos((m_kk + m_k+1,k+1)/2) / 2 pi
+// Fundamental frequency of a real turn-by-turn record (the reference's naff, utility.cpp:21-97):
+// the largest spectral line with frequency in [xlow, xhi] (bins of 1/N), then the maximum of the
+// sin^4-windowed projection |sum_i X_i w_i exp(-2 pi i nu i)| within one bin of it, by golden-
+// section search to 3e-8 relative.
+double naff(int N, const double* X, double xlow = 0, double xhi = 0.5);
 const char* elem_type_name(int type);        // the reference's class name: "Drift", "StrMPole", ...
 
 }  // namespace accelgpu

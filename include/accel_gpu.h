@@ -261,6 +261,11 @@ int  accel_beam_stat(accel_ctx* ctx, const double* r, int layout, int N, double*
 #define ACCEL_NOALLOC_STAT_MAX_N 4194304
 int  accel_beam_stat_noalloc(const double* r, int layout, int64_t N, double* out, void* stream);
 
+/* Fundamental frequency (tune) of a real turn-by-turn record, host only: the largest spectral
+ * line in [xlow, xhi], refined by golden-section search on the sin^4-windowed projection
+ * (the reference's naff, utility.cpp:21-97). */
+int  accel_naff(const double* data, int n, double xlow, double xhi, double* nu);
+
 /* Device FP64 FMA throughput micro-benchmark (TFLOP/s, FMA = 2 flops). */
 int  accel_fp64_peak(accel_ctx* ctx, double* tflops);
 

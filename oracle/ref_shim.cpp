@@ -147,6 +147,8 @@ void ref_srand(unsigned seed) { srand(seed); }
 
 double ref_grandn(void) { return grandn(0.0, 1.0); }
 
+double ref_naff(int n, double* data, double xlow, double xhi) { return naff(n, data, xlow, xhi); }
+
 double ref_trackDA(void* h, double xmax, double xmin, double ymax, int nturn, int nray,
                    int nstep, double* rx, double* ry) {
     return L(h)->trackDA(xmax, xmin, ymax, nturn, (unsigned)nray, nstep, rx, ry, false);

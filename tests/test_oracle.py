@@ -3,6 +3,8 @@ library's own outputs bit for bit — the committed golden vectors everywhere, a
 reference library (oracle/_ref) where it was built."""
 from __future__ import annotations
 
+import os
+
 import numpy as np
 import pytest
 
@@ -139,3 +141,12 @@ def test_longwake_oracle_self_consistent(A, O):
     w = amp * np.exp(-a * tau) * (np.cos(wb * tau) - a / wb * np.sin(wb * tau))
     assert np.isclose(V[3], w * 1e-9, rtol=1e-12)
     assert np.all(V[6:] == 0)
+
+
+def test_naff_matches_reference(A):
+    """The host NAFF against the reference's naff on synthetic lines (with a second harmonic and
+    noise) and on FODO turn-by-turn records: the same frequency to well inside the golden-section
+    tolerance (3e-8 relative)."""
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "naff.npz"))
+    for x, lo, hi, nu in zip(g["records"], g["xlow"], g["xhi"], g["nu"]):
+        assert abs(A.naff(x, lo, hi) - nu) <= 1e-8 * abs(nu), (A.naff(x, lo, hi), nu)
