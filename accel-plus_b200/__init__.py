@@ -100,6 +100,7 @@ def lib() -> C.CDLL:
         "accel_line_get_field": (I, [P, I, I, I, C.POINTER(D)]),
         "accel_line_set_flags": (I, [P, I, I, I]),
         "accel_line_set_energy": (I, [P, D]),
+        "accel_line_set_crab_onoff": (I, [P, I, C.POINTER(I)]),
         "accel_line_setrfphase": (I, [P, C.POINTER(D)]),
         "accel_line_set_seed": (I, [P, C.c_uint64]),
         "accel_track": (I, [P, P, I, I, I, I, I, P, I, P]),
@@ -385,6 +386,12 @@ class Line:
 
     def set_flags(self, rad=-1, cavity=-1, wake=-1):
         _check(lib().accel_line_set_flags(self.h, rad, cavity, wake), "accel_line_set_flags")
+
+    def set_crab(self, on: bool) -> int:
+        """ALine::set_crab_onoff: every CrabCav on or off; returns their number."""
+        n = C.c_int()
+        _check(lib().accel_line_set_crab_onoff(self.h, int(bool(on)), C.byref(n)), "accel_line_set_crab_onoff")
+        return n.value
 
     def set_energy(self, en: float):
         _check(lib().accel_line_set_energy(self.h, en), "accel_line_set_energy")

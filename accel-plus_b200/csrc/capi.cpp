@@ -664,12 +664,23 @@ int accel_line_set_flags(accel_line* L, int rad_flag, int cavity_on, int wake_on
     return ACCEL_OK;
 }
 
+int accel_line_set_crab_onoff(accel_line* L, int on, int* count) {
+    if (!L) return fail(ACCEL_E_INVALID, "NULL line");
+    int n = 0;
+    for (auto& d : L->desc)  // ALine::set_crab_onoff, aline.cpp:441-450
+        if (d.type == ACCEL_CRABCAV) { d.flags = on ? 1 : 0; n++; }
+    if (count) *count = n;
+    L->dirty = true;
+    return ACCEL_OK;
+}
+
 int accel_line_set_energy(accel_line* L, double en) {
     if (!L) return fail(ACCEL_E_INVALID, "NULL line");
     for (auto& d : L->desc) {  // ALine::setenergy, aline.cpp:220-257
         if (d.type == ACCEL_CAVITY) d.f[3] = en;
         else if (d.type == ACCEL_CRABCAV) d.f[4] = en;
         else if (d.type == ACCEL_RFMULT) d.f[2] = en;
+        else if (d.type == ACCEL_IDEALWIG) d.f[3] = en;
         else if (d.type == ACCEL_BENDMPOLE) d.f[3] = en;
         else if (d.type == ACCEL_TRANSWAKE) d.f[0] = en;
         else if (d.type == ACCEL_LONGWAKE) d.f[0] = en;

@@ -105,6 +105,9 @@ int accel_adjoint_create(accel_line* L, int N, int nturn, int every, const int32
         if (is_collective(d.type)) return fail(ACCEL_E_UNSUPPORTED, "the adjoint does not differentiate wake elements");
         if (d.type == ACCEL_BENDMPOLE && d.flags != 0) return fail(ACCEL_E_UNSUPPORTED, "the adjoint needs radiation off");
         if (d.type == ACCEL_SYNCRAD && d.flags != 0) return fail(ACCEL_E_UNSUPPORTED, "the adjoint needs SyncRad off");
+        if ((d.type == ACCEL_CRABCAV && d.flags != 0 && (d.f[5] > 0 || d.f[6] > 0)) ||
+            (d.type == ACCEL_RFMULT && d.f[3] > 0))
+            return fail(ACCEL_E_UNSUPPORTED, "the adjoint needs RF phase and voltage noise off");
     }
     std::unique_ptr<accel_adjoint> J(new accel_adjoint());
     J->line = L;

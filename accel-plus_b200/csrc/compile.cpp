@@ -35,7 +35,7 @@ bool is_supported(int type) {
     case ACCEL_DRIFT: case ACCEL_QUAD: case ACCEL_CORRECTOR: case ACCEL_APERTURE:
     case ACCEL_MONITOR: case ACCEL_BEND: case ACCEL_BENDMPOLE: case ACCEL_STRMPOLE:
     case ACCEL_CAVITY: case ACCEL_TRANSWAKE: case ACCEL_MATRIX: case ACCEL_SYNCRAD:
-    case ACCEL_LONGWAKE:
+    case ACCEL_LONGWAKE: case ACCEL_CRABCAV: case ACCEL_RFMULT: case ACCEL_IDEALWIG:
         return true;
     default:
         return false;
@@ -200,6 +200,34 @@ int compile_line(const accel_elem_desc* d, int n, std::vector<DevElem>& out, std
             r.flags = e.flags & 3;
             break;
         }
+        case ACCEL_CRABCAV:  // f: devoltx devolty freq phis energy sigphi sigdVV (accel.cpp:993-995)
+            r.op = OP_CRABCAV;
+            r.v[V_CNVX] = e.f[0] / e.f[4];
+            r.v[V_CNVY] = e.f[1] / e.f[4];
+            r.v[V_CK] = TWOPI_ * e.f[2] / C0_;
+            r.v[V_CPHIS] = e.f[3];
+            r.v[V_CSIGPHI] = e.f[5];
+            r.v[V_CSIGDVV] = e.f[6];
+            r.flags = e.flags ? 1 : 0;
+            break;
+        case ACCEL_RFMULT:  // f: freq phis energy sigphi sigdVV (accel.cpp:1148)
+            r.op = OP_RFMULT;
+            r.v[V_RK] = TWOPI_ * e.f[0] / C0_;
+            r.v[V_RPHIS] = e.f[1];
+            r.v[V_RSIGPHI] = e.f[3];
+            r.v[V_RM] = e.max_npole;
+            for (int i = 0; i < ACCEL_MAX_MPOLE; i++) { r.v[V_A + i] = e.poly_a[i]; r.v[V_B + i] = e.poly_b[i]; }
+            break;
+        case ACCEL_IDEALWIG: {  // f: lambda h wigtype energy (accel.cpp:1465, 1496)
+            r.op = OP_IDEALWIG;
+            r.v[V_WK] = 2.0 * PI_ / e.f[0];
+            r.v[V_WH] = e.f[1];
+            r.v[V_WTYPE] = e.f[2];
+            const double en = e.f[3];
+            r.v[V_WCRAD] = CGAMMA_ * en * en * en / (TWOPI_ * 1e9);
+            r.flags = e.flags ? 1 : 0;
+            break;
+        }
         case ACCEL_TRANSWAKE:
         case ACCEL_LONGWAKE:
             r.op = (e.type == ACCEL_TRANSWAKE) ? OP_TRANSWAKE : OP_LONGWAKE;
@@ -245,6 +273,9 @@ double model_flops(const accel_elem_desc* d, int n) {
         case ACCEL_MATRIX: f += 66 + (e.len != 0 ? 28 : 0); break;
         case ACCEL_SYNCRAD: f += 6 + (e.len != 0 ? 28 : 0); break;
         case ACCEL_LONGWAKE: f += 8 + (e.len != 0 ? 28 : 0); break;
+        case ACCEL_CRABCAV: f += 16 + (e.len != 0 ? 28 : 0); break;
+        case ACCEL_RFMULT: f += 14 + 12 * e.max_npole + (e.len != 0 ? 28 : 0); break;
+        case ACCEL_IDEALWIG: f += (e.len != 0 ? e.nslice * (28 + 12 + (e.flags ? 24 : 0)) : 0); break;
         default: break;
         }
     }

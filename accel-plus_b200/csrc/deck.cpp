@@ -232,6 +232,8 @@ void Deck::lattice(std::istream& in) {
             if (ncav > 0) cout << ncav << " cavity(ies) turned off" << endl;
             int nw = L->set_wake_onoff(false);
             if (nw > 0) cout << nw << " wake element(s) turned off" << endl;
+            int ncrab = L->set_crab_onoff(false);
+            if (ncrab > 0) cout << ncrab << " crab cavity(ies) turned off" << endl;
             break;
         }
         case 1: {

@@ -109,6 +109,16 @@ template <int N> __device__ __forceinline__ Dual<N> fabs(const Dual<N>& a) {
 }
 
 // the plain double overloads stay visible next to the Dual ones inside this namespace
+// atan2(y, x): d = (x dy - y dx) / (x^2 + y^2)
+template <int N> __device__ __forceinline__ Dual<N> atan2(const Dual<N>& y, const Dual<N>& x) {
+    Dual<N> r;
+    r.v = ::atan2(y.v, x.v);
+    const double q = 1.0 / (x.v * x.v + y.v * y.v);
+#pragma unroll
+    for (int i = 0; i < N; i++) r.d[i] = (x.v * y.d[i] - y.v * x.d[i]) * q;
+    return r;
+}
+using ::atan2;
 using ::sqrt;
 using ::sin;
 using ::cos;

@@ -8,6 +8,7 @@
 // Parameter-only subexpressions (slice lengths, irho*tan(e), CRAD, ...) arrive precomputed in the
 // element record (compile.cpp), evaluated on the host with the same operand order.
 #pragma once
+#include <type_traits>
 #include <cmath>
 #include "engine.h"
 #include "dual.cuh"
@@ -315,6 +316,98 @@ __device__ void pass(const DevElem& e, T* r, QeSource& q) {
         if (len != 0) {
             fastdrift(r, len / (1 + r[5]));
             aperture_test(r, a, b, c, d);
+        }
+        return;
+    }
+    case OP_CRABCAV: {  // accel.cpp:991-1032
+        const double k = e.v[V_CK];
+        if (len != 0) fastdrift(r, 0.5 * len / (1 + r[5]));
+        if (e.flags) {
+            T omega_t = -k * r[4] + e.v[V_CPHIS];
+            if (e.v[V_CSIGPHI] > 0) omega_t = omega_t + e.v[V_CSIGPHI] * q.next();
+            double nvxa = e.v[V_CNVX], nvya = e.v[V_CNVY];
+            if (e.v[V_CSIGDVV] > 0) {
+                nvxa = nvxa * (1.0 + e.v[V_CSIGDVV] * q.next());
+                nvya = nvya * (1.0 + e.v[V_CSIGDVV] * q.next());
+            }
+            r[1] += nvxa * sin(omega_t);
+            r[3] += nvya * sin(omega_t);
+            r[5] += -(nvya * r[2] + nvxa * r[0]) * k * cos(omega_t) / (1 + r[5]);
+        }
+        if (len != 0) fastdrift(r, 0.5 * len / (1 + r[5]));
+        return;
+    }
+    case OP_RFMULT: {  // accel.cpp:1146-1197, cylindrical sums of the RF multipole
+        const double k = e.v[V_RK];
+        if (len != 0) fastdrift(r, 0.5 * len / (1 + r[5]));
+        T omega_t = -k * r[4] + e.v[V_RPHIS];
+        if (e.v[V_RSIGPHI] > 0) omega_t = omega_t + e.v[V_RSIGPHI] * q.next();
+        const int M = (int)e.v[V_RM];
+        if constexpr (std::is_same<T, double>::value) {
+            T rho = sqrt(r[0] * r[0] + r[2] * r[2]);
+            T phis = atan2(r[2], r[0]);
+            T AsL = T(0.0), ArhoL = T(0.0), AphiL = T(0.0), nrho = T(1.0);
+            for (int n = 0; n < M; n++) {
+                T nphi = (double)(n + 1) * phis;
+                T td = e.v[V_B + n] * cos(nphi) + e.v[V_A + n] * sin(nphi);
+                ArhoL += nrho * td;
+                AphiL += nrho * (-e.v[V_B + n] * sin(nphi) + e.v[V_A + n] * cos(nphi));
+                nrho = nrho * rho;
+                AsL += 1.0 / (n + 1) * nrho * td;
+            }
+            r[1] += (ArhoL * cos(phis) - AphiL * sin(phis)) * cos(omega_t);
+            r[3] += (ArhoL * sin(phis) + AphiL * cos(phis)) * cos(omega_t);
+            r[5] += k * AsL * sin(omega_t) / (1. + r[5]);
+        } else {
+            // the same kicks in Cartesian form, smooth at x = y = 0 for derivative types:
+            // with c_n = B_n - i A_n and z = x + i y, P = sum c_n z^n, Q = sum c_n z^(n+1) / (n+1);
+            // dpx = Re P cos(wt), dpy = -Im P cos(wt), d(delta) = k Re Q sin(wt) / (1 + delta)
+            T zr = T(1.0), zi = T(0.0), Pr = T(0.0), Pi = T(0.0), Qr = T(0.0);
+            for (int n = 0; n < M; n++) {
+                const double cr = e.v[V_B + n], ci = -e.v[V_A + n];
+                Pr += cr * zr - ci * zi;
+                Pi += cr * zi + ci * zr;
+                T nr = zr * r[0] - zi * r[2];
+                zi = zr * r[2] + zi * r[0];
+                zr = nr;
+                Qr += (cr * zr - ci * zi) / (double)(n + 1);
+            }
+            r[1] += Pr * cos(omega_t);
+            r[3] -= Pi * cos(omega_t);
+            r[5] += k * Qr * sin(omega_t) / (1. + r[5]);
+        }
+        if (len != 0) fastdrift(r, 0.5 * len / (1 + r[5]));
+        return;
+    }
+    case OP_IDEALWIG: {  // accel.cpp:1463-1533
+        if (len == 0) return;
+        const double k = e.v[V_WK], h = e.v[V_WH], crad = e.v[V_WCRAD];
+        const int ns = e.nslice, wt = (int)e.v[V_WTYPE];
+        const bool rad = e.flags != 0;
+        auto rad_kick = [&]() {
+            T dp = r[5];
+            T yp = r[3] / (1 + dp);
+            T xp = r[1] / (1 + dp);
+            r[5] = r[5] - crad * ((1 + r[5]) * (1 + r[5])) * h * h * len / ns / 2.0;
+            r[1] = xp * (1 + r[5]);
+            r[3] = yp * (1 + r[5]);
+        };
+        for (int j = 0; j < ns; j++) {
+            fastdrift(r, 0.5 * len / (1 + r[5]) / ns);
+            T y = r[2];
+            T x = r[0];
+            if (rad) rad_kick();
+            if (wt == 0) {
+                T y3 = y * y * y;
+                double k2 = k * k;
+                r[3] -= h * h * (0.5 * y + 1.0 / 3.0 * y3 * k2 + 1.0 / 15.0 * y3 * y * y * k2 * k2) * len / ns;
+            } else if (wt == 1) {
+                T x3 = x * x * x;
+                double k2 = k * k;
+                r[1] -= h * h * (0.5 * x + 1.0 / 3.0 * x3 * k2 + 1.0 / 15.0 * x3 * x * x * k2 * k2) * len / ns;
+            }
+            if (rad) rad_kick();
+            fastdrift(r, 0.5 * len / (1 + r[5]) / ns);
         }
         return;
     }

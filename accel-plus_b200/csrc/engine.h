@@ -32,6 +32,9 @@ enum DevOp : int32_t {
     OP_SYNCRAD = 11,
     OP_TRANSWAKE = 12, // collective: never inside a fused range
     OP_LONGWAKE = 13,  // collective: never inside a fused range
+    OP_CRABCAV = 14,
+    OP_RFMULT = 15,
+    OP_IDEALWIG = 16,
 };
 
 struct alignas(128) DevElem {
@@ -86,6 +89,12 @@ enum : int {
     V_SIGD = 9,
     // LongWake / TransWake keep their descriptor fields in v[1..12]
     V_W = 1,
+    // CrabCav: devolt/energy, 2 pi f / c, phase, phase noise, voltage noise
+    V_CNVX = 1, V_CNVY = 2, V_CK = 3, V_CPHIS = 4, V_CSIGPHI = 5, V_CSIGDVV = 6,
+    // RFMult: 2 pi f / c, phase, phase noise, number of poles (A, B at V_A, V_B)
+    V_RK = 1, V_RPHIS = 2, V_RSIGPHI = 3, V_RM = 4,
+    // IdealWig: 2 pi / lambda, h, type, CGAMMA E^3 / (2 pi 1e9)
+    V_WK = 1, V_WH = 2, V_WTYPE = 3, V_WCRAD = 4,
 };
 
 enum : int32_t { STR_SKEW = 1 << 8, STR_SKEW0 = 1 << 9 };  // any A non-zero; only A[0]

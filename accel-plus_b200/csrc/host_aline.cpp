@@ -278,6 +278,14 @@ int ALine::set_cavity_onoff(bool flag) {
     return cnt;
 }
 
+int ALine::set_crab_onoff(bool flag) {  // aline.cpp:441-450
+    int n = 0;
+    for (auto& d : desc_)
+        if (d.type == ACCEL_CRABCAV) { d.flags = flag ? 1 : 0; n++; }
+    dirty_ = true;
+    return n;
+}
+
 int ALine::set_wake_onoff(bool flag) {
     int cnt = 0;
     for (auto& d : desc_)

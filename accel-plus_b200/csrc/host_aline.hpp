@@ -55,6 +55,7 @@ public:
     int set_rad_onoff(unsigned flag);
     int set_cavity_onoff(bool flag);
     int set_wake_onoff(bool flag);
+    int set_crab_onoff(bool flag);
     int set_monitor(unsigned flag, unsigned index = 0);
     int set_monitor_pass(int num = 0);
     unsigned monitor_flag() const { return mon_flag_; }

@@ -136,6 +136,7 @@ void default_desc(int type, accel_elem_desc* d) {
     case ACCEL_CAVITY: d->f[1] = 476.314e6; d->f[3] = 3000; d->flags = 1; break;
     case ACCEL_CRABCAV: d->f[2] = 476.314e6 * 6; d->f[4] = 3000; break;
     case ACCEL_RFMULT: d->f[0] = 476.314e6 * 6; d->f[2] = 3000; break;
+    case ACCEL_IDEALWIG: d->f[0] = 0.10; d->f[3] = 3000; break;  // f3: energy (not in the file)
     case ACCEL_TRANSWAKE:
         d->f[0] = 3000; d->f[3] = 1.0e10; d->f[4] = 1; d->f[6] = 1.0e10; d->f[7] = 1; break;
     case ACCEL_MATRIX:

@@ -56,10 +56,10 @@ extern "C" {
 #define ACCEL_BENDMPOLE  7
 #define ACCEL_STRMPOLE   8
 #define ACCEL_CAVITY     9
-#define ACCEL_WIGTABLE  10   /* parsed, tracking returns ACCEL_E_UNSUPPORTED */
-#define ACCEL_IDEALWIG  11   /* parsed, tracking returns ACCEL_E_UNSUPPORTED */
-#define ACCEL_CRABCAV   12   /* parsed, tracking returns ACCEL_E_UNSUPPORTED */
-#define ACCEL_RFMULT    13   /* parsed, tracking returns ACCEL_E_UNSUPPORTED */
+#define ACCEL_WIGTABLE  10   /* parsed (table skipped), tracking returns ACCEL_E_UNSUPPORTED */
+#define ACCEL_IDEALWIG  11
+#define ACCEL_CRABCAV   12
+#define ACCEL_RFMULT    13
 #define ACCEL_TRANSWAKE 14
 #define ACCEL_MATRIX    15
 #define ACCEL_SYNCRAD   16
@@ -91,9 +91,14 @@ extern "C" {
  *   MATRIX     mat[36] row-major
  *   SYNCRAD    f0 Energy, f1 U0, f2 Jx, f3 Jy, f4 EmitX, f5 EmitY, f6 SigDelta, f7 BetaX, f8 BetaY
  *   LONGWAKE   f0 Energy [MeV], f1 Charge [nC], f2 Rs [Ohm], f3 fr [Hz], f4 Q, f5 nbins
+ *   CRABCAV    f0 DeVoltX, f1 DeVoltY [MV], f2 Frequency [Hz], f3 Phis, f4 Energy [MeV],
+ *              f5 SigPhi, f6 SigdVV (noise from the device's counter-based normals)
+ *   RFMULT     f0 Frequency, f1 Phis, f2 Energy, f3 SigPhi, f4 SigdVV; poly_a, poly_b; max_npole
+ *   IDEALWIG   f0 lambda, f1 h, f2 type (0 horizontal, 1 vertical), f3 Energy [MeV]; nslice
  * irho is kept as its own field because the reference only refreshes it when BendingAngle is set
  * (accel.h:170, accel.cpp:497,581), not when Length changes.
- * flags: BENDMPOLE / SYNCRAD radiation flag (ACCEL_RAD_*), CAVITY / TRANSWAKE / LONGWAKE on-off.
+ * flags: BENDMPOLE / SYNCRAD / IDEALWIG radiation flag (ACCEL_RAD_*), CAVITY / TRANSWAKE /
+ * LONGWAKE / CRABCAV on-off.
  */
 typedef struct accel_elem_desc {
     int32_t type;
@@ -179,6 +184,8 @@ int  accel_line_set_field(accel_line* line, int idx, int field, int index, const
 int  accel_line_get_field(const accel_line* line, int idx, int field, int index, double* value);
 int  accel_line_set_flags(accel_line* line, int rad_flag, int cavity_on, int wake_on);
 int  accel_line_set_energy(accel_line* line, double energy_mev);
+/* ALine::set_crab_onoff (aline.cpp:441-450): every CrabCav on or off; *count gets their number */
+int  accel_line_set_crab_onoff(accel_line* line, int on, int* count);
 int  accel_line_setrfphase(accel_line* line, double* phis_out);      /* ALine::setrfphase() */
 int  accel_line_set_seed(accel_line* line, uint64_t seed);           /* Philox key for QE     */
 

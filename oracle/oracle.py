@@ -128,6 +128,7 @@ def ref():
         sig = {
             "ref_line_load": (P, [S]), "ref_line_free": (None, [P]), "ref_line_nelem": (I, [P]),
             "ref_set_threads": (None, [I]), "ref_max_threads": (I, []),
+            "ref_set_crab": (None, [P, I]),
             "ref_pass": (None, [P, P, I, I]), "ref_pass_range": (None, [P, P, I, I, I]),
             "ref_track_loss": (None, [P, P, I, I, P]),
             "ref_m66": (None, [P, I, I, D, D, P]),
@@ -217,6 +218,9 @@ class RefLine:
 
     def setrfphase(self) -> float:
         return ref().ref_setrfphase(self.h)
+
+    def set_crab(self, on):
+        ref().ref_set_crab(self.h, int(bool(on)))
 
     def set_flags(self, rad=None, cavity=None, wake=None):
         if rad is not None:

@@ -101,6 +101,7 @@ double ref_setrfphase(void* h) { return L(h)->setrfphase(); }
 void ref_set_rad(void* h, int flag) { L(h)->set_rad_onoff((unsigned)flag); }
 void ref_set_cavity(void* h, int on) { L(h)->set_cavity_onoff(on != 0); }
 void ref_set_wake(void* h, int on) { L(h)->set_wake_onoff(on != 0); }
+void ref_set_crab(void* h, int on) { L(h)->set_crab_onoff(on != 0); }
 void ref_set_energy(void* h, double en) { L(h)->setenergy(en); }
 
 // PolynomB/PolynomA[index] of a StrMPole (accel.cpp:773-785) or PolynomB of a BendMPole.

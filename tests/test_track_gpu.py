@@ -210,7 +210,7 @@ def test_longwake_against_oracle(A, ctx, O, LT):
 
 
 def test_errors_are_statuses(A, ctx):
-    wig = A.elem(A.IDEALWIG, "W", 1.0)
+    wig = A.elem(A.WIGTABLE, "W", 1.0)  # the one type still refused
     line = A.Line(ctx, [wig])
     r = np.zeros((4, 6))
     with pytest.raises(A.AccelError) as ei:
@@ -248,3 +248,26 @@ def test_autotune_and_launch_count(A, ctx, LT):
     torch.cuda.synchronize()
     assert torch.equal(la, lb)
     assert rel_err(a.cpu().numpy().T, b.cpu().numpy().T) < 1e-13
+
+
+@pytest.mark.parametrize("mode", ["plain", "fused"])
+def test_crab_rfmult_wiggler_against_reference(A, ctx, mode):
+    """CrabCav, RFMult and IdealWig (both planes, and with radiation) against the reference's
+    passes (tests/golden/elements_extra.npz, make_elem_extra_golden.py).  These maps call sin,
+    cos, atan2 and sqrt, so the plain kernel agrees to 1e-14 rather than bit for bit."""
+    import os
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+    import make_elem_extra_golden as X
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "elements_extra.npz"))
+    m = A.MODE_PLAIN if mode == "plain" else A.MODE_FUSED
+    for name, elems in X.cases(A).items():
+        line = A.Line(ctx, elems)
+        r = g["elem_in"].copy()
+        line.track(r, 1, mode=m)
+        ref = g[f"elem_{name}"]
+        tol = 1e-14 if mode == "plain" else 1e-12
+        assert rel_err(r, ref) < tol, (name, rel_err(r, ref))
+        if name != "idealwig_rad":  # the exact tangent map against the reference's difference map
+            ex, fd = line.m66(method=0), line.m66(method=1, delta=1e-8)
+            assert np.all(np.isfinite(ex)) and np.max(np.abs(ex - fd)) < 1e-6 * np.max(np.abs(fd)), name
