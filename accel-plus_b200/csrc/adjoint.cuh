@@ -99,9 +99,12 @@ __device__ __forceinline__ void forward_t(const DevElem& e, T* r) {
 }
 
 // Parameter element on dual numbers with parameter directions: r carries d/d(block input) in
-// d[0..5]; directions 6 + j seed the element's parameters j = 0 .. n-1 (kind/index as in
+// d[0..5]; directions 6 + j stand for the element's parameters j = 0 .. n-1 (kind/index as in
 // ElemParams).  Afterwards r[i].d[k] (k < 6) is the Jacobian of block and element together and
-// r[i].d[6 + j] = d out_i / d p_j.
+// r[i].d[6 + j] = d out_i / d p_j.  The coefficients stay plain doubles: each kick is taken on
+// the dual state, then each parameter's explicit derivative is added to its direction; with
+// P = sum (B_n + i A_n) z^n and the kick px -= K Re P, py += K Im P,
+//   d px / d B_n = -K Re z^n,  d py / d B_n = K Im z^n,  d px / d A_n = K Im z^n,  d py / d A_n = K Re z^n.
 constexpr int kPD = 6 + kMaxParamsPerElem;
 __device__ __forceinline__ void forward_params(const DevElem& e, Dual<kPD>* r, int n, const int* kind,
                                                const int* index) {
@@ -113,25 +116,35 @@ __device__ __forceinline__ void forward_params(const DevElem& e, Dual<kPD>* r, i
         lit::quad6(r, e.v[V_LEN], K);
         return;
     }
-    Dual<kPD> A[ACCEL_MAX_MPOLE], B[ACCEL_MAX_MPOLE];
+    double A[ACCEL_MAX_MPOLE], B[ACCEL_MAX_MPOLE];
 #pragma unroll
-    for (int i = 0; i < ACCEL_MAX_MPOLE; i++) { A[i] = Dual<kPD>(e.v[V_A + i]); B[i] = Dual<kPD>(e.v[V_B + i]); }
-    for (int j = 0; j < n; j++) {
-        if (kind[j] == PK_B) B[index[j]].d[6 + j] = 1.0;
-        else if (kind[j] == PK_A) A[index[j]].d[6 + j] = 1.0;
-    }
+    for (int i = 0; i < ACCEL_MAX_MPOLE; i++) { A[i] = e.v[V_A + i]; B[i] = e.v[V_B + i]; }
     const int M = e.order_eff;
-    if (e.op == OP_STRKICK) { lit::strthinkick(r, A, B, 1.0, M); return; }
+    auto kick = [&](double K) {
+        const double x = r[0].v, y = r[2].v;
+        lit::strthinkick(r, A, B, K, M);
+        for (int j = 0; j < n; j++) {
+            double zr = 1.0, zi = 0.0;
+            for (int q = 0; q < index[j]; q++) {
+                const double t = zr * x - zi * y;
+                zi = zr * y + zi * x;
+                zr = t;
+            }
+            if (kind[j] == PK_B) { r[1].d[6 + j] -= K * zr; r[3].d[6 + j] += K * zi; }
+            else if (kind[j] == PK_A) { r[1].d[6 + j] += K * zi; r[3].d[6 + j] += K * zr; }
+        }
+    };
+    if (e.op == OP_STRKICK) { kick(1.0); return; }
     const double L1 = e.v[V_L1], L2 = e.v[V_L2], K1 = e.v[V_K1], K2 = e.v[V_K2];
+    const Dual<kPD> norm = 1 / (1 + r[5]);  // delta is constant inside the element
+    const Dual<kPD> N1 = L1 * norm, N2 = L2 * norm;
     for (int m = 0; m < e.nslice; m++) {
-        Dual<kPD> norm = 1 / (1 + r[5]);
-        Dual<kPD> N1 = L1 * norm, N2 = L2 * norm;
         lit::fastdrift(r, N1);
-        lit::strthinkick(r, A, B, K1, M);
+        kick(K1);
         lit::fastdrift(r, N2);
-        lit::strthinkick(r, A, B, K2, M);
+        kick(K2);
         lit::fastdrift(r, N2);
-        lit::strthinkick(r, A, B, K1, M);
+        kick(K1);
         lit::fastdrift(r, N1);
     }
 }
