@@ -237,12 +237,27 @@ void Deck::lattice(std::istream& in) {
             break;
         }
         case 1: {
+            // reset_first (process.cpp:280-340): type + famname -> that element; famname alone ->
+            // every member of the family in turn, each with its own type and index 1
             string type = get(a, "TYPE"), fam = get(a, "FAMNAME");
             unsigned index = (unsigned)std::atoi(get(a, "INDEX", "1").c_str());
-            auto sel = select(*L, type, fam, index == 0 ? 1 : index);
-            if (sel.empty()) { cout << "resetfirstelement: element not found" << endl; break; }
-            L->resetfirstelement(sel[0]);
-            cout << "First element is now " << accelgpu::elem_type_name(L->element(0).type) << "." << L->element(0).famname << endl;
+            auto reset = [&](const string& t, unsigned i) {
+                cout << "First element moved to: type=" << t << ", famname=" << fam << ", index= " << i << endl;
+                unsigned e;
+                if (i == 0) std::cerr << "resetfirstelement: element index cannot be zero" << endl;
+                if (L->findelements(&e, t, fam, i == 0 ? 1 : i) == 0)
+                    cout << "resetfirstelement: element not found (type =" << t << ", famname =" << fam
+                         << ", index =" << i << ")" << endl;
+                else
+                    L->resetfirstelement(e);
+            };
+            if (!type.empty() && !fam.empty()) {
+                reset(type, index);
+            } else if (type.empty() && !fam.empty()) {
+                unsigned ne = L->getnumber();
+                for (unsigned i = 0; i < ne; i++)
+                    if (L->element(i).famname == fam) reset(accelgpu::elem_type_name(L->element(i).type), 1);
+            }
             break;
         }
         case 2: {
@@ -385,15 +400,30 @@ void Deck::lattice(std::istream& in) {
             break;
         }
         case 9: {
-            string rad = get(a, "RADIATION"), cav = get(a, "CAVITY"), wake = get(a, "WAKE");
-            if (iequal(rad, "ON") || iequal(rad, "RAD")) L->set_rad_onoff(ACCEL_RAD_RAD);
-            else if (iequal(rad, "RADQE")) L->set_rad_onoff(ACCEL_RAD_RADQE);
-            else if (iequal(rad, "LUMP")) L->set_rad_onoff(ACCEL_RAD_LUMP);
-            else if (iequal(rad, "OFF")) L->set_rad_onoff(ACCEL_RAD_OFF);
-            if (iequal(cav, "ON")) L->set_cavity_onoff(true);
-            else if (iequal(cav, "OFF")) L->set_cavity_onoff(false);
-            if (iequal(wake, "ON")) L->set_wake_onoff(true);
-            else if (iequal(wake, "OFF")) L->set_wake_onoff(false);
+            // set_flags (process.cpp:880-965): keys in the order given, each with its message;
+            // radiation=lump is this engine's addition and prints nothing
+            for (auto& kvp : a) {
+                const string& k = kvp.first;
+                const string& v = kvp.second;
+                int nl = 0;
+                if (k == "RADIATION") {
+                    if (iequal(v, "OFF")) { L->set_rad_onoff(ACCEL_RAD_OFF); cout << "radiation turned off" << endl; }
+                    else if (iequal(v, "RAD") || iequal(v, "ON")) {
+                        L->set_rad_onoff(ACCEL_RAD_RAD);
+                        cout << "radiation turned on without quantum excitation" << endl;
+                    } else if (iequal(v, "RADQE")) {
+                        L->set_rad_onoff(ACCEL_RAD_RADQE);
+                        cout << "radiation turned on with quantum excitation" << endl;
+                    } else if (iequal(v, "LUMP")) L->set_rad_onoff(ACCEL_RAD_LUMP);
+                } else if (k == "CAVITY" || k == "CRABCAV" || k == "WAKE") {
+                    bool on = iequal(v, "ON");
+                    if (!on && !iequal(v, "OFF")) continue;
+                    const char* what = k == "CAVITY" ? " cavity(ies) turned " : k == "CRABCAV" ? " crab cavity(ies) turned "
+                                                                                                : " wake element(s) turned ";
+                    nl = k == "CAVITY" ? L->set_cavity_onoff(on) : k == "CRABCAV" ? L->set_crab_onoff(on) : L->set_wake_onoff(on);
+                    if (nl > 0) cout << nl << what << (on ? "on" : "off") << endl;
+                }
+            }
             break;
         }
         case 10:
@@ -629,6 +659,13 @@ void Deck::track(std::istream& in) {
             if (iequal(rf, "OFF")) L->set_cavity_onoff(false);
             else if (iequal(rf, "ON")) L->set_cavity_onoff(true);
             if (np > 0 && nturn > 0) {
+                // the reference reads "PrintFlag" from element 0 whatever its type
+                // (process.cpp:2000-2002); the multipole classes report the missing field
+                // (accel.cpp:619, 770) and the flag is then unset there; here nothing is printed
+                int t0 = L->element(0).type;
+                if (t0 == ACCEL_STRMPOLE || t0 == ACCEL_BENDMPOLE)
+                    cout << (t0 == ACCEL_STRMPOLE ? "AStrMPole" : "ABendMPole")
+                         << "::getfield() --> no matched field PrintFlag" << endl;
                 unsigned flag = L->monitor_flag();
                 if (flag == accelgpu::MON_COORD) {
                     double ratio = L->element(0).type == ACCEL_MONITOR ? L->element(0).f[1] : 1.0;
@@ -660,10 +697,24 @@ void Deck::track(std::istream& in) {
                 cout << "*************************************" << endl;
             }
         } else if (k == 3) {
-            string type = get(a, "TYPE"), fam = get(a, "FAMNAME");
-            unsigned index = (unsigned)std::atoi(get(a, "INDEX", "0").c_str());
-            auto sel = select(*L, type, fam, index);
-            cout << type << " " << fam << " " << index << endl;
+            // Transport (process.cpp:2108-2205): index=N or an index list index=[i, j, ...].  At
+            // each watch point the reference prints the block's distribution as the last Do_Track
+            // left it; its transported copy is advanced but not printed.  This deck does the same.
+            string type = get(a, "TYPE"), fam = get(a, "FAMNAME"), idx = get(a, "INDEX", "0"), indices;
+            unsigned index = 0;
+            if (!idx.empty() && idx[0] == '[') {
+                indices = idx.substr(1, idx.size() - 2);
+                std::replace(indices.begin(), indices.end(), ',', ' ');
+                size_t b = indices.find_first_not_of(" \t"), e = indices.find_last_not_of(" \t");
+                indices = (b == string::npos) ? string() : indices.substr(b, e - b + 1);
+                indices += " ";
+            } else {
+                index = (unsigned)std::atoi(idx.c_str());
+            }
+            auto sel = select(*L, type, fam, index, indices);
+            cout << type << " " << fam << " ";
+            if (indices.empty()) cout << index << endl;
+            else cout << indices << endl;
             if (sel.empty()) { cout << "No watch point found" << endl; continue; }
             std::vector<double> nr = r;
             cout << "$$$Track-Transport: ************************" << endl;
@@ -673,7 +724,7 @@ void Deck::track(std::istream& in) {
                 cout << "type=" << type << ", famname=" << fam << ", ring index=" << e << ", spos=" << L->getlength(e) << endl;
                 for (int i = 0; i < np; i++) {
                     cout << e << "\t";
-                    for (int j = 0; j < 6; j++) cout << nr[(size_t)6 * i + j] << "\t";
+                    for (int j = 0; j < 6; j++) cout << r[(size_t)6 * i + j] << "\t";
                     cout << endl;
                 }
                 cout << "#------end of ring index=" << e << endl;
