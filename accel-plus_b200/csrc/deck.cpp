@@ -14,9 +14,9 @@
 //            | Load F[, format=plain|accel-export]; shift=(..); Print)  Monitor  Do_Track  Transport
 //   DAMA     track_DA  track_MA  track_dNudJ
 // Differences: Gaussian distributions come from a seeded generator (--seed; the reference seeds
-// rand() with the time, process.cpp:42); Transport prints the transported coordinates (the
-// reference prints the untransported array, process.cpp:2201); apply_setpt is reported as not
-// supported.
+// rand() with the time, process.cpp:42); a family member picked with index >= 2 is that member
+// (the reference's findelements leaves list[0] unset then, aline.cpp:531-533); apply_setpt is
+// reported as not supported.
 #include <algorithm>
 #include <cctype>
 #include <cmath>
@@ -138,7 +138,9 @@ std::vector<unsigned> select(ALine& L, const string& type, const string& fam, un
         }
     } else if (!indices.empty()) {
         unsigned nf = L.findelements(list.data(), type, fam, index);
-        std::stringstream ss(indices);
+        string idx = indices;
+        std::replace(idx.begin(), idx.end(), ',', ' ');
+        std::stringstream ss(idx);
         int t;
         n = 0;
         while (ss >> t)
@@ -320,13 +322,16 @@ void Deck::lattice(std::istream& in) {
         }
         case 4: {
             string type = get(a, "TYPE"), fam = get(a, "FAMNAME");
-            auto sel = select(*L, type, fam, 0);
+            // export_element (process.cpp:505-545): RING or LINE writes the whole line with no
+            // closing row; a type, or a type and family, writes those elements and a closing row
+            bool whole = iequal(type, "RING") || iequal(type, "LINE");
+            auto sel = whole ? select(*L, "ALL", "", 0) : select(*L, type, fam, 0);
             cout << "$$$Export-Elements***********************" << endl;
             std::vector<accel_elem_desc> v;
             for (unsigned i : sel) v.push_back(L->element(i));
             ALine tmp(ctx, v);
             tmp.serialize(cout, 6);
-            cout << "******************************" << endl;
+            if (!whole) cout << "******************************************" << endl;
             break;
         }
         case 5:
@@ -368,9 +373,15 @@ void Deck::lattice(std::istream& in) {
             cout << "*********************************" << endl;
             break;
         }
-        case 7:
-            cout << "#set_max_num_threads: tracking runs on the GPU; the setting is ignored" << endl;
+        case 7: {
+            // set_max_num_threads (process.cpp:768-779): the reference's OpenMP thread count.  The
+            // tracking here runs on the GPU, so the number is only echoed, with the reference's line.
+            string v = line.substr(line.find_first_of("=:") == string::npos ? line.size() : line.find_first_of("=:") + 1);
+            int num = 0;
+            std::stringstream(v) >> num;
+            cout << "Maximum thread number set to " << std::max(num, 1) << endl;
             break;
+        }
         case 8: {
             // modify_element: type, famname, index, field, value= | delta= (process.cpp:776-873).
             // As in the reference, `index` both picks the index-th family member (0 = all) and
@@ -561,40 +572,52 @@ int Deck::distribution(const string& line_in) {
         return n;
     }
     if (iequal(opt, "LINEAR")) {
-        // Linear X=a:step:b — one coordinate swept, the others zero
-        const char* names[6] = {"X", "XP", "Y", "YP", "Z", "DP"};
-        for (int c = 0; c < 6; c++) {
-            if (!has(a, names[c])) continue;
-            string spec = get(a, names[c]);
-            std::replace(spec.begin(), spec.end(), ':', ' ');
-            double lo, st, hi;
-            std::stringstream(spec) >> lo >> st >> hi;
-            for (double v = lo; (st > 0) ? (v <= hi + 1e-15) : (v >= hi - 1e-15); v += st) {
-                double p[6] = {0, 0, 0, 0, 0, 0};
-                p[c] = v;
-                r.insert(r.end(), p, p + 6);
-                if (st == 0) break;
-            }
-            break;
-        }
-        return (int)(r.size() / 6);
+        // Linear C=start:step:end (process.cpp:1761-1802): the first key names the swept
+        // coordinate (X XP Y YP Z DELTA; anything else sweeps X), the others stay zero; the count
+        // comes from stepping a running value, the values are start + step * i
+        const char* names[6] = {"X", "XP", "Y", "YP", "Z", "DELTA"};
+        string key, spec;
+        for (auto& kvp : a)
+            if (!kvp.second.empty()) { key = kvp.first; spec = kvp.second; break; }
+        int c = 0;
+        for (int j = 0; j < 6; j++)
+            if (key == names[j]) c = j;
+        if (key == "DP") c = 5;
+        std::replace(spec.begin(), spec.end(), ':', ' ');
+        double lo = 0, st = 0, hi = 0;
+        std::stringstream(spec) >> lo >> st >> hi;
+        if (st == 0) { cout << "interval cannot be zero" << endl; return 0; }
+        int n = 0;
+        for (double v = lo; (v <= hi && st > 0) || (v >= hi && st < 0); v += st) n++;
+        r.assign((size_t)6 * n, 0.0);
+        for (int i = 0; i < n; i++) r[(size_t)6 * i + c] = lo + st * i;
+        return n;
     }
     if (iequal(opt, "LOAD")) {
+        // Load FILE[, format=plain|accel-export] (process.cpp:1471-1555): the file name is echoed;
+        // an accel-export file is read from its "Full export" block, whose Np line and data lines
+        // are echoed as they are read; lines of 11 characters or fewer and "%" lines are skipped
         string fname;
         ss >> fname;
         if (!fname.empty() && fname.back() == ',') fname.pop_back();
+        cout << fname << endl;
         bool exported = upper(sel).find("ACCEL-EXPORT") != string::npos;
         std::ifstream f(fname);
         string sl;
         if (exported)
             while (mgetline(f, sl))
-                if (sl.compare(0, 3, "$$$") == 0 && sl.find("Full export") != string::npos) { mgetline(f, sl); break; }
+                if (sl.compare(0, 3, "$$$") == 0 && sl.find("Full export") != string::npos) {
+                    mgetline(f, sl);
+                    cout << sl << endl;
+                    break;
+                }
         while (mgetline(f, sl)) {
             if (sl.compare(0, 5, "*****") == 0) break;
             trim(sl);
-            if (sl.size() <= 11) continue;
+            if (sl.size() <= 11 || sl[0] == '%') continue;
+            if (exported) cout << sl << endl;
             std::stringstream ls(sl);
-            double t, v[6];
+            double t, v[6] = {0, 0, 0, 0, 0, 0};
             if (exported) ls >> t;
             for (int j = 0; j < 6; j++) ls >> v[j];
             r.insert(r.end(), v, v + 6);

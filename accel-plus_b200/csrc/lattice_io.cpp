@@ -277,12 +277,18 @@ int parse_lattice(const std::string& text, std::vector<accel_elem_desc>& out, st
 }
 
 // The reference's serialize() layout (accel.cpp:143-1742), with a caller-chosen precision so
-// that a written lattice reads back bit-identically at precision 17.
+// that a written lattice reads back bit-identically at precision 17.  As in the reference, the
+// frequency and phase of Cavity, CrabCav and RFMult are written with at least 16 digits
+// (accel.cpp:855, 932, 1047).
 std::string format_lattice(const accel_elem_desc* e, int n, int precision) {
     std::string s;
     char buf[256];
     auto num = [&](double x) {
         std::snprintf(buf, sizeof(buf), "%.*g", precision, x);
+        s += buf;
+    };
+    auto num16 = [&](double x) {
+        std::snprintf(buf, sizeof(buf), "%.*g", precision > 16 ? precision : 16, x);
         s += buf;
     };
     auto tab = [&]() { s += "\t"; };
@@ -312,10 +318,14 @@ std::string format_lattice(const accel_elem_desc* e, int n, int precision) {
             s += "\n\t\t\t";
             for (int i = 0; i < d.max_npole; i++) { num(d.poly_a[i]); tab(); }
             break;
-        case ACCEL_CAVITY: for (int i = 0; i < 4; i++) { tab(); num(d.f[i]); } break;
-        case ACCEL_CRABCAV: for (int i = 0; i < 7; i++) { tab(); num(d.f[i]); } break;
+        case ACCEL_CAVITY:
+            for (int i = 0; i < 4; i++) { tab(); (i == 1 || i == 2) ? num16(d.f[i]) : num(d.f[i]); }
+            break;
+        case ACCEL_CRABCAV:
+            for (int i = 0; i < 7; i++) { tab(); (i == 2 || i == 3) ? num16(d.f[i]) : num(d.f[i]); }
+            break;
         case ACCEL_RFMULT:
-            for (int i = 0; i < 5; i++) { tab(); num(d.f[i]); }
+            for (int i = 0; i < 5; i++) { tab(); i < 2 ? num16(d.f[i]) : num(d.f[i]); }
             tab(); s += std::to_string(d.max_npole);
             s += "\n\t\t\t";
             for (int i = 0; i < d.max_npole; i++) { num(d.poly_b[i]); tab(); }

@@ -70,7 +70,7 @@ def compare(mine, ref):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("deck", ["dba_deck", "fodo_deck", "ops_deck"])
+@pytest.mark.parametrize("deck", ["dba_deck", "fodo_deck", "ops_deck", "dist_deck"])
 def test_deck_matches_reference(deck):
     with open(os.path.join(GOLDEN, deck + ".ref.out")) as f:
         ref = [l for l in f.read().splitlines() if not l.startswith("#UTC")]
@@ -79,7 +79,7 @@ def test_deck_matches_reference(deck):
 
 def test_deck_compare_accepts_reference_against_itself():
     """The comparison's own logic, on the golden outputs alone (no GPU)."""
-    for deck in ("dba_deck", "fodo_deck", "ops_deck"):
+    for deck in ("dba_deck", "fodo_deck", "ops_deck", "dist_deck"):
         with open(os.path.join(GOLDEN, deck + ".ref.out")) as f:
             ref = f.read().splitlines()
         compare(ref, ref)
