@@ -91,6 +91,10 @@ def lib() -> C.CDLL:
         "accel_lattice_parse": (I, [C.c_char_p, C.POINTER(pd), C.POINTER(I)]),
         "accel_lattice_write": (I, [C.c_char_p, pd, I, I]),
         "accel_lattice_free": (None, [pd]),
+        "accel_wigtable_create": (I, [I, I, P, P, P, P, C.POINTER(C.c_int32)]),
+        "accel_wigtable_info": (I, [C.c_int32, C.POINTER(I), C.POINTER(I)]),
+        "accel_wigtable_get": (I, [C.c_int32, P, P, P, P]),
+        "accel_wigtable_destroy": (I, [C.c_int32]),
         "accel_elem_default": (I, [I, pd]),
         "accel_line_create": (I, [P, pd, I, C.POINTER(P)]),
         "accel_line_destroy": (I, [P]),
@@ -192,6 +196,38 @@ def elem(type_: int, famname: str = "undefined", length: float = 0.0, **kw) -> E
     if type_ in (BEND, BENDMPOLE) and length != 0:
         d.f[4] = d.f[0] / length
     return d
+
+
+def wigtable(xl, yl, xkick, ykick) -> int:
+    """Register a WigTable kick table (accel_wigtable_create) and return its id, the value of a
+    WigTable descriptor's f[0].  xkick and ykick are [len(yl)][len(xl)]: kick[i][j] at
+    (xl[j], yl[i])."""
+    xl = np.ascontiguousarray(xl, dtype=np.float64)
+    yl = np.ascontiguousarray(yl, dtype=np.float64)
+    xk = np.ascontiguousarray(xkick, dtype=np.float64)
+    yk = np.ascontiguousarray(ykick, dtype=np.float64)
+    if xk.shape != (len(yl), len(xl)) or yk.shape != xk.shape:
+        raise ValueError("kick tables must be [len(yl)][len(xl)]")
+    tid = C.c_int32()
+    _check(lib().accel_wigtable_create(len(xl), len(yl), C.c_void_p(xl.ctypes.data), C.c_void_p(yl.ctypes.data),
+                                       C.c_void_p(xk.ctypes.data), C.c_void_p(yk.ctypes.data), C.byref(tid)),
+           "accel_wigtable_create")
+    return tid.value
+
+
+def wigtable_get(tid: int):
+    """(xl, yl, xkick, ykick) of a registered table (accel_wigtable_info / accel_wigtable_get)."""
+    mx, my = C.c_int(), C.c_int()
+    _check(lib().accel_wigtable_info(tid, C.byref(mx), C.byref(my)), "accel_wigtable_info")
+    xl, yl = np.empty(mx.value), np.empty(my.value)
+    xk, yk = np.empty((my.value, mx.value)), np.empty((my.value, mx.value))
+    _check(lib().accel_wigtable_get(tid, C.c_void_p(xl.ctypes.data), C.c_void_p(yl.ctypes.data),
+                                    C.c_void_p(xk.ctypes.data), C.c_void_p(yk.ctypes.data)), "accel_wigtable_get")
+    return xl, yl, xk, yk
+
+
+def wigtable_destroy(tid: int) -> None:
+    _check(lib().accel_wigtable_destroy(tid), "accel_wigtable_destroy")
 
 
 def desc_array(elems: Sequence[ElemDesc]):

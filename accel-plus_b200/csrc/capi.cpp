@@ -103,9 +103,30 @@ int accel::line_sync(accel_line* L) {
     std::string err;
     int s = compile_line(L->desc.data(), (int)L->desc.size(), recs, err);
     if (s != ACCEL_OK) return fail(s, err);
-    L->host_tbl = recs;
     cudaSetDevice(L->ctx->device);
-    int st = L->d_tbl.ensure(std::max<size_t>(1, recs.size()) * sizeof(DevElem));
+    // WigTable kick tables: one device block per line, each record given its table's address
+    std::vector<double> aux;
+    std::vector<std::pair<size_t, size_t>> at;  // (record, offset in doubles)
+    for (size_t k = 0; k < recs.size(); k++) {
+        if (recs[k].op != OP_WIGTABLE) continue;
+        auto t = wigtable_find((int32_t)recs[k].v[V_TID]);
+        if (!t) return fail(ACCEL_E_INVALID, "WigTable kick table was destroyed");
+        at.push_back({k, aux.size()});
+        aux.insert(aux.end(), t->data.begin(), t->data.end());
+    }
+    int st = 0;
+    if (!aux.empty()) {
+        st = L->d_aux.ensure(aux.size() * sizeof(double));
+        if (st) return st;
+        CK(cudaMemcpy(L->d_aux.p, aux.data(), aux.size() * sizeof(double), cudaMemcpyHostToDevice));
+        for (auto& a : at) {
+            const double* dp = (const double*)L->d_aux.p + a.second;
+            static_assert(sizeof(dp) == sizeof(double), "a device address must fit a payload slot");
+            std::memcpy(&recs[a.first].v[V_TPTR], &dp, sizeof(dp));
+        }
+    }
+    L->host_tbl = recs;
+    st = L->d_tbl.ensure(std::max<size_t>(1, recs.size()) * sizeof(DevElem));
     if (st) return st;
     if (!recs.empty())
         CK(cudaMemcpy(L->d_tbl.p, recs.data(), recs.size() * sizeof(DevElem), cudaMemcpyHostToDevice));
@@ -517,6 +538,7 @@ void line_unref(accel_line* L) {
         cudaStreamSynchronize(C->stream);
         C->graphs.clear();
         L->d_tbl.release();
+        L->d_aux.release();
         L->d_rng.release();
         delete L;
     }

@@ -36,6 +36,7 @@ bool is_supported(int type) {
     case ACCEL_MONITOR: case ACCEL_BEND: case ACCEL_BENDMPOLE: case ACCEL_STRMPOLE:
     case ACCEL_CAVITY: case ACCEL_TRANSWAKE: case ACCEL_MATRIX: case ACCEL_SYNCRAD:
     case ACCEL_LONGWAKE: case ACCEL_CRABCAV: case ACCEL_RFMULT: case ACCEL_IDEALWIG:
+    case ACCEL_WIGTABLE:
         return true;
     default:
         return false;
@@ -228,6 +229,20 @@ int compile_line(const accel_elem_desc* d, int n, std::vector<DevElem>& out, std
             r.flags = e.flags ? 1 : 0;
             break;
         }
+        case ACCEL_WIGTABLE: {  // accel.cpp:1335-1377; the table's device address is set by the line
+            const int32_t id = (int32_t)e.f[0];
+            auto t = wigtable_find(id);
+            if (!t) {
+                err = std::string("WigTable ") + e.famname + ": no kick table with id " + std::to_string(id);
+                return ACCEL_E_INVALID;
+            }
+            r.op = OP_WIGTABLE;
+            r.v[V_TMX] = t->mx;
+            r.v[V_TMY] = t->my;
+            r.v[V_TID] = id;
+            r.v[V_THL] = 0.5 * e.len;
+            break;
+        }
         case ACCEL_TRANSWAKE:
         case ACCEL_LONGWAKE:
             r.op = (e.type == ACCEL_TRANSWAKE) ? OP_TRANSWAKE : OP_LONGWAKE;
@@ -276,6 +291,8 @@ double model_flops(const accel_elem_desc* d, int n) {
         case ACCEL_CRABCAV: f += 16 + (e.len != 0 ? 28 : 0); break;
         case ACCEL_RFMULT: f += 14 + 12 * e.max_npole + (e.len != 0 ? 28 : 0); break;
         case ACCEL_IDEALWIG: f += (e.len != 0 ? e.nslice * (28 + 12 + (e.flags ? 24 : 0)) : 0); break;
+        // two cell coordinates (6) and two bilinear sums (2 x 13) per kick; two drifts per slice
+        case ACCEL_WIGTABLE: f += (e.len != 0 ? e.nslice * (32 + 28 + 4) : 32); break;
         default: break;
         }
     }

@@ -226,6 +226,30 @@ struct QeSource {
 
 // One element on one particle.  Returns without touching a lost particle (x NaN), which is what
 // every reference pass method does first (e.g. accel.cpp:166-167).
+// WigTable interpolation (interp2, utility.cpp:174-188): the bilinear interpolation of a table
+// on a rectangular grid from Numerical Recipes 3rd ed. (Bilin_interp, interp_2d.h), restated.
+// The cell is found by bisection on a monotonic grid of n >= 2 points (the book's locate,
+// interp_1d.h), so a point outside the grid is extrapolated from the edge cell.
+__device__ __forceinline__ int grid_cell(const double* g, int n, double x) {
+    const bool ascending = g[n - 1] >= g[0];
+    int lo = 0, hi = n - 1;
+    while (hi - lo > 1) {
+        int mid = (hi + lo) >> 1;
+        if ((x >= g[mid]) == ascending) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// t, u: the point's fractions across cell (i, j); z: a table [my][mx], z[jj*mx + ii] at
+// (xl[ii], yl[jj]).  Sum and product order as written in the book.
+template <class T>
+__device__ __forceinline__ T bilinear(const double* z, int mx, int i, int j, const T& t, const T& u) {
+    const double z00 = z[j * mx + i], z10 = z[j * mx + i + 1];
+    const double z01 = z[(j + 1) * mx + i], z11 = z[(j + 1) * mx + i + 1];
+    return (1. - t) * (1. - u) * z00 + t * (1. - u) * z10 + (1. - t) * u * z01 + t * u * z11;
+}
+
 template <class T>
 __device__ void pass(const DevElem& e, T* r, QeSource& q) {
     if (is_lost(r[0])) return;
@@ -408,6 +432,42 @@ __device__ void pass(const DevElem& e, T* r, QeSource& q) {
             }
             if (rad) rad_kick();
             fastdrift(r, 0.5 * len / (1 + r[5]) / ns);
+        }
+        return;
+    }
+    case OP_WIGTABLE: {  // accel.cpp:1335-1377
+        const int mx = (int)e.v[V_TMX], my = (int)e.v[V_TMY], ns = e.nslice;
+        const double* tab;
+        memcpy(&tab, &e.v[V_TPTR], sizeof(tab));
+        const double* xl = tab;
+        const double* yl = tab + mx;
+        const double* xk = yl + my;
+        const double* yk = xk + mx * my;
+        // both kicks at the point (x, y); the reference interpolates each table separately, with
+        // the same cell and fractions
+        auto kicks = [&](T& kx, T& ky) {
+            const T x = r[0], y = r[2];
+            const int i = grid_cell(xl, mx, val(x)), j = grid_cell(yl, my, val(y));
+            const T t = (x - xl[i]) / (xl[i + 1] - xl[i]);
+            const T u = (y - yl[j]) / (yl[j + 1] - yl[j]);
+            kx = bilinear(xk, mx, i, j, t, u);
+            ky = bilinear(yk, mx, i, j, t, u);
+        };
+        if (len == 0) {
+            T kx, ky;
+            kicks(kx, ky);
+            r[1] += kx;
+            r[3] += ky;
+            return;
+        }
+        const double hl = e.v[V_THL];
+        for (int j = 0; j < ns; j++) {
+            fastdrift(r, hl / (1 + r[5]) / ns);
+            T kx, ky;
+            kicks(kx, ky);
+            r[1] += kx / ns;
+            r[3] += ky / ns;
+            fastdrift(r, hl / (1 + r[5]) / ns);
         }
         return;
     }

@@ -6,6 +6,7 @@
 #include <vector>
 #include <mutex>
 #include <atomic>
+#include <memory>
 #include "accel_gpu.h"
 
 namespace accel {
@@ -35,6 +36,7 @@ enum DevOp : int32_t {
     OP_CRABCAV = 14,
     OP_RFMULT = 15,
     OP_IDEALWIG = 16,
+    OP_WIGTABLE = 17,
 };
 
 struct alignas(128) DevElem {
@@ -95,6 +97,8 @@ enum : int {
     V_RK = 1, V_RPHIS = 2, V_RSIGPHI = 3, V_RM = 4,
     // IdealWig: 2 pi / lambda, h, type, CGAMMA E^3 / (2 pi 1e9)
     V_WK = 1, V_WH = 2, V_WTYPE = 3, V_WCRAD = 4,
+    // WigTable: grid sizes, device address of the table (bit pattern), registry id, len / 2
+    V_TMX = 1, V_TMY = 2, V_TPTR = 3, V_TID = 4, V_THL = 5,
 };
 
 enum : int32_t { STR_SKEW = 1 << 8, STR_SKEW0 = 1 << 9 };  // any A non-zero; only A[0]
@@ -111,6 +115,17 @@ std::string format_lattice(const accel_elem_desc* e, int n, int precision);
 void default_desc(int type, accel_elem_desc* d);
 const char* type_name(int type);
 int type_from_name(const std::string& s);
+
+// WigTable kick tables (wigtable.cpp).  data = xl[mx], yl[my], xkick[my][mx], ykick[my][mx].
+constexpr int kWigTabMaxX = 101, kWigTabMaxY = 21;  // MAX_WIGTAB_X / MAX_WIGTAB_Y, accel.h:401-402
+struct WigTab {
+    int mx = 0, my = 0;
+    std::vector<double> data;
+};
+inline size_t wigtable_doubles(int mx, int my) { return (size_t)mx + my + 2 * (size_t)mx * my; }
+std::shared_ptr<const WigTab> wigtable_find(int32_t id);
+int wigtable_register(int mx, int my, const double* xl, const double* yl, const double* xkick,
+                      const double* ykick, int32_t* id, std::string& err);
 
 // compile descriptors to device records (compile.cpp)
 int compile_line(const accel_elem_desc* d, int n, std::vector<DevElem>& out, std::string& err);

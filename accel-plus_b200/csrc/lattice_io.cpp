@@ -16,6 +16,8 @@
 //   CrabCav    len dvx dvy freq phis en sigphi sigdVV accel.cpp:937-946
 //   RFMult     len freq phis en sigphi sigdVV MaxNPole / PolyB / PolyA   accel.cpp:1058-1072
 //   WigTable   len nslice mx my / xl / yl / xkick rows / blank / ykick rows accel.cpp:1294-1333
+//              (the numbers after the size line are read as one sequence, so the blank line
+//              is optional; the table goes to the registry, the descriptor keeps its id)
 //   IdealWig   len nslice lambda h wigtype           accel.cpp:1449-1461
 //   TransWake  len energy Ne Wx fRx Qx Wy fRy Qy     accel.cpp:1546-1554
 //   Matrix     len / six rows of six                 accel.cpp:1673-1687
@@ -233,15 +235,25 @@ int parse_lattice(const std::string& text, std::vector<accel_elem_desc>& out, st
             c.rest_of_line();
             break;
         }
-        case ACCEL_WIGTABLE: {  // kept for reading only: its table is skipped
+        case ACCEL_WIGTABLE: {  // the table is registered; the descriptor keeps its id
             d.nslice = (int)get(1, 1);
-            int mx = (int)get(2, 0), my = (int)get(3, 0);
-            d.f[0] = mx; d.f[1] = my;
+            const int mx = (int)get(2, 0), my = (int)get(3, 0);
+            if (mx < 2 || mx > kWigTabMaxX || my < 2 || my > kWigTabMaxY) {
+                err = std::string("WigTable ") + d.famname + ": table size outside 2..101 x 2..21";
+                return ACCEL_E_IO;
+            }
+            std::vector<double> t(wigtable_doubles(mx, my));
+            for (size_t i = 0; i < t.size(); i++)
+                if (!c.number(t[i])) {
+                    err = std::string("WigTable ") + d.famname + ": table ends early";
+                    return ACCEL_E_IO;
+                }
             c.rest_of_line();
-            c.rest_of_line();
-            for (int i = 0; i < my; i++) c.rest_of_line();
-            c.rest_of_line();
-            for (int i = 0; i < my; i++) c.rest_of_line();
+            int32_t id = 0;
+            const double* p = t.data();
+            int st = wigtable_register(mx, my, p, p + mx, p + mx + my, p + mx + my + mx * my, &id, err);
+            if (st) { err = std::string("WigTable ") + d.famname + ": " + err; return ACCEL_E_IO; }
+            d.f[0] = id;
             break;
         }
         case ACCEL_IDEALWIG:
@@ -336,6 +348,28 @@ std::string format_lattice(const accel_elem_desc* e, int n, int precision) {
             tab(); s += std::to_string(d.nslice);
             for (int i = 0; i < 3; i++) { tab(); num(d.f[i]); }
             break;
+        case ACCEL_WIGTABLE: {  // accel.cpp:1247-1270: sizes, xl, yl, xkick rows, blank, ykick rows
+            auto t = wigtable_find((int32_t)d.f[0]);
+            const int mx = t ? t->mx : 0, my = t ? t->my : 0;
+            tab(); s += std::to_string(d.nslice);
+            tab(); s += std::to_string(mx);
+            tab(); s += std::to_string(my);
+            if (!t) break;
+            const double* p = t->data.data();
+            s += "\n";
+            for (int j = 0; j < mx; j++) { num(p[j]); tab(); }
+            s += "\n";
+            for (int i = 0; i < my; i++) { num(p[mx + i]); tab(); }
+            for (int k = 0; k < 2; k++) {
+                const double* z = p + mx + my + (size_t)k * mx * my;
+                if (k == 1) s += "\n";
+                for (int i = 0; i < my; i++) {
+                    s += "\n";
+                    for (int j = 0; j < mx; j++) { num(z[i * mx + j]); tab(); }
+                }
+            }
+            break;
+        }
         case ACCEL_TRANSWAKE: for (int i = 0; i < 8; i++) { tab(); num(d.f[i]); } break;
         case ACCEL_MATRIX:
             for (int i = 0; i < 6; i++) {

@@ -76,6 +76,7 @@ struct accel_line {
     std::vector<accel_elem_desc> desc;
     std::vector<accel::DevElem> host_tbl;
     accel::DevBuf d_tbl;
+    accel::DevBuf d_aux;  // WigTable kick tables of this line, addressed from their records
     accel::DevBuf d_rng;  // [0]: QE turn base, advanced by every tracking call
     bool dirty = true;
     int64_t version = 0;

@@ -56,7 +56,7 @@ extern "C" {
 #define ACCEL_BENDMPOLE  7
 #define ACCEL_STRMPOLE   8
 #define ACCEL_CAVITY     9
-#define ACCEL_WIGTABLE  10   /* parsed (table skipped), tracking returns ACCEL_E_UNSUPPORTED */
+#define ACCEL_WIGTABLE  10   /* kick table by id: accel_wigtable_create */
 #define ACCEL_IDEALWIG  11
 #define ACCEL_CRABCAV   12
 #define ACCEL_RFMULT    13
@@ -95,6 +95,7 @@ extern "C" {
  *              f5 SigPhi, f6 SigdVV (noise from the device's counter-based normals)
  *   RFMULT     f0 Frequency, f1 Phis, f2 Energy, f3 SigPhi, f4 SigdVV; poly_a, poly_b; max_npole
  *   IDEALWIG   f0 lambda, f1 h, f2 type (0 horizontal, 1 vertical), f3 Energy [MeV]; nslice
+ *   WIGTABLE   f0 table id (accel_wigtable_create; 0 = none, which tracking rejects); nslice
  * irho is kept as its own field because the reference only refreshes it when BendingAngle is set
  * (accel.h:170, accel.cpp:497,581), not when Length changes.
  * flags: BENDMPOLE / SYNCRAD / IDEALWIG radiation flag (ACCEL_RAD_*), CAVITY / TRANSWAKE /
@@ -172,6 +173,27 @@ int  accel_ctx_set_comm(accel_ctx* ctx, const unsigned char id[128], int nranks,
 int  accel_lattice_read(const char* path, accel_elem_desc** elems, int* n);
 int  accel_lattice_parse(const char* text, accel_elem_desc** elems, int* n);
 int  accel_lattice_write(const char* path, const accel_elem_desc* elems, int n, int precision);
+
+/*
+ * WigTable kick tables (AWigTable, accel.h:403-425; table read/written at accel.cpp:1247-1333).
+ * A table is held in a process-wide registry and named from its elements' descriptors by id
+ * (f0).  accel_lattice_read / accel_lattice_parse register one table per WigTable entry they read
+ * and accel_lattice_write writes it back in the reference's layout.  A line copies the table to
+ * its device when it is compiled, so a table may be destroyed once no line will be (re)compiled
+ * from descriptors that name it.
+ *   mx in 2..101 and my in 2..21 (MAX_WIGTAB_X / MAX_WIGTAB_Y, accel.h:401-402; the
+ *   reference's interpolation needs two points per axis, interp_1d.h locate);
+ *   xl[mx], yl[my]: the grid, each monotonic (ascending or descending);
+ *   xkick, ykick: [my][mx] row-major, kick[i*mx + j] at (xl[j], yl[i]) — the reference's
+ *   xkick[i][j] rows.
+ * The kicks are interpolated bilinearly (interp2, utility.cpp:174-188), extrapolated from the
+ * edge cell outside the grid.  accel_wigtable_get copies out any non-null array.
+ */
+int  accel_wigtable_create(int mx, int my, const double* xl, const double* yl, const double* xkick,
+                           const double* ykick, int32_t* id);
+int  accel_wigtable_info(int32_t id, int* mx, int* my);
+int  accel_wigtable_get(int32_t id, double* xl, double* yl, double* xkick, double* ykick);
+int  accel_wigtable_destroy(int32_t id);
 void accel_lattice_free(accel_elem_desc* elems);
 int  accel_elem_default(int type, accel_elem_desc* out);   /* the reference's default ctor */
 

@@ -81,6 +81,51 @@ def test_lattice_reader_errors(A):
     assert ei.value.status == A.E_IO
 
 
+def test_wigtable_registry_and_lattice_format(A, tmp_path):
+    """WigTable kick tables: registered, read back, written in the reference's layout (sizes, xl,
+    yl, xkick rows, a blank line, ykick rows; accel.cpp:1247-1270) and parsed again bit-exactly."""
+    xl = np.linspace(-0.02, 0.02, 5)
+    yl = np.array([0.01, 0.0, -0.01])          # descending is allowed
+    xk = np.arange(15.0).reshape(3, 5) * 1e-5 + 1.0 / 3.0
+    yk = -np.arange(15.0).reshape(3, 5) * 1e-6
+    tid = A.wigtable(xl, yl, xk, yk)
+    got = A.wigtable_get(tid)
+    for a, b in zip(got, (xl, yl, xk, yk)):
+        assert np.array_equal(a, b)
+    ring = [A.elem(A.DRIFT, "D", 1.0), A.elem(A.WIGTABLE, "WT", 1.5, nslice=4, f=[tid]),
+            A.elem(A.DRIFT, "D", 0.5)]
+    p = str(tmp_path / "w.lat")
+    A.write_lattice(p, ring)
+    lines = open(p).read().splitlines()
+    assert lines[1].split() == ["WT", ":", "WigTable", "1.5", "4", "5", "3"]
+    assert len(lines) == 1 + 1 + 2 + 3 + 1 + 3 + 1 and lines[7].strip() == ""
+    back = A.read_lattice(p)
+    assert [d.type for d in back] == [A.DRIFT, A.WIGTABLE, A.DRIFT] and back[2].len == 0.5
+    assert back[1].nslice == 4 and back[1].len == 1.5 and int(back[1].f[0]) != tid
+    for a, b in zip(A.wigtable_get(int(back[1].f[0])), (xl, yl, xk, yk)):
+        assert np.array_equal(a, b)
+    A.wigtable_destroy(tid)
+    with pytest.raises(A.AccelError) as ei:
+        A.wigtable_get(tid)
+    assert ei.value.status == A.E_INVALID
+
+
+def test_wigtable_rejects_bad_tables(A):
+    ok_x, ok_y = np.linspace(-1, 1, 4), np.linspace(-1, 1, 3)
+    z = np.zeros((3, 4))
+    for xl, yl, zz in ((np.array([0.0]), ok_y, np.zeros((3, 1))),          # one grid point
+                       (np.linspace(-1, 1, 102), ok_y, np.zeros((3, 102))),  # above MAX_WIGTAB_X
+                       (ok_x, np.linspace(-1, 1, 22), np.zeros((22, 4))),    # above MAX_WIGTAB_Y
+                       (np.array([0.0, 1.0, 1.0, 2.0]), ok_y, z),            # repeated point
+                       (np.array([0.0, 2.0, 1.0, 3.0]), ok_y, z)):           # not monotonic
+        with pytest.raises(A.AccelError) as ei:
+            A.wigtable(xl, yl, zz, zz)
+        assert ei.value.status == A.E_INVALID
+    with pytest.raises(A.AccelError) as ei:   # a table that ends early
+        A.parse_lattice("WT : WigTable 1.0 2 3 2\n 0 1 2\n 0 1\n 1 2 3\n 4 5 6\n\n 1 2 3\n")
+    assert ei.value.status == A.E_IO
+
+
 @pytest.mark.skipif(not __import__("oracle").ref_available(), reason="reference library not built here")
 def test_reader_agrees_with_reference_deserialize(A, O, LT):
     """Every element's fields as the reference's own deserialize+getfield see them."""

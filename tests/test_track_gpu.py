@@ -210,12 +210,10 @@ def test_longwake_against_oracle(A, ctx, O, LT):
 
 
 def test_errors_are_statuses(A, ctx):
-    wig = A.elem(A.WIGTABLE, "W", 1.0)  # the one type still refused
-    line = A.Line(ctx, [wig])
     r = np.zeros((4, 6))
-    with pytest.raises(A.AccelError) as ei:
-        line.track(r, 1)
-    assert ei.value.status == A.E_UNSUPPORTED
+    with pytest.raises(A.AccelError) as ei:  # a WigTable that names no kick table
+        A.Line(ctx, [A.elem(A.WIGTABLE, "W", 1.0)]).track(r, 1)
+    assert ei.value.status == A.E_INVALID
     line2 = A.Line(ctx, [A.elem(A.DRIFT, "D", 1.0)])
     with pytest.raises(A.AccelError) as ei:
         line2.track(r, 1, st=0, ed=5)
@@ -248,6 +246,32 @@ def test_autotune_and_launch_count(A, ctx, LT):
     torch.cuda.synchronize()
     assert torch.equal(la, lb)
     assert rel_err(a.cpu().numpy().T, b.cpu().numpy().T) < 1e-13
+
+
+@pytest.mark.parametrize("mode", ["plain", "fused"])
+def test_wigtable_against_reference(A, ctx, mode):
+    """WigTable (thin, sliced, and an uneven grid with y descending; particles inside and outside
+    the grid) against the reference's pass (tests/golden/wigtable.npz, make_wigtable_golden.py).
+    The map has no transcendental, so the plain kernel agrees bit for bit."""
+    import os
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+    import make_wigtable_golden as W
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "wigtable.npz"))
+    m = A.MODE_PLAIN if mode == "plain" else A.MODE_FUSED
+    for name, spec in W.tables().items():
+        line = A.Line(ctx, W.elems(A, name, spec))
+        r = g["elem_in"].copy()
+        line.track(r, 1, mode=m)
+        ref = g[f"elem_{name}"]
+        if mode == "plain":
+            assert np.array_equal(r, ref), (name, rel_err(r, ref))
+        else:
+            assert rel_err(r, ref) < 1e-12, (name, rel_err(r, ref))
+        # the exact tangent map against the reference's difference map, at a point inside a cell
+        at = np.array([0.0013, 1e-4, 0.0021, -1e-4, 0.0, 5e-4])
+        ex, fd = line.m66_at(at, method=0), line.m66_at(at, method=1, delta=1e-9)
+        assert np.all(np.isfinite(ex)) and np.max(np.abs(ex - fd)) < 1e-6 * np.max(np.abs(fd)), name
 
 
 @pytest.mark.parametrize("mode", ["plain", "fused"])
