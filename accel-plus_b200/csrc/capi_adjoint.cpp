@@ -60,6 +60,7 @@ struct accel_adjoint {
     std::vector<int32_t> pelem;  // elements carrying parameters, in line order
     int npe = 0;
     int chunk = 0;               // turns per block-Jacobian tape; 0: per-turn element reversal
+    bool general = true;         // the tape needs the dual-number fallback (jtape_needs_general)
     DevBuf st, lam, aos, tape, ckpt, turn_tape, part, meta, final_x, grad, jt, rt, pel;
     bool have_forward = false;
     ~accel_adjoint() {
@@ -171,6 +172,7 @@ int accel_adjoint_create(accel_line* L, int N, int nturn, int every, const int32
     for (int e = 0; e < ne; e++)
         if (J->pcount[(size_t)e] > 0) J->pelem.push_back(e);
     J->npe = (int)J->pelem.size();
+    J->general = jtape_needs_general(L->host_tbl.data(), ne, J->pcount.data(), J->pfirst.data(), J->pkind.data());
     const double per_turn = 8.0 * (double)N * (36.0 * (J->npe + 1) + 6.0 * nparam);
     J->chunk = (int)std::min<double>(std::min(every, nturn), std::floor(kTapeBudgetBytes / per_turn));
     if (J->chunk >= 1) {
@@ -273,7 +275,7 @@ int accel_adjoint_backward(accel_adjoint* J, const double* g, double* dr0, doubl
             for (int hi = nt; hi > 0; hi -= J->chunk) {
                 const int lo = std::max(0, hi - J->chunk);
                 launch_adj_jtape(a, (const double*)J->turn_tape.p, lo, hi - lo, (const double*)J->final_x.p,
-                                 J->npe, (double*)J->jt.p, (double*)J->rt.p, s);
+                                 J->npe, (double*)J->jt.p, (double*)J->rt.p, J->general, s);
                 launch_adj_jsweep(a, hi - lo, (const double*)J->final_x.p, J->npe, (const int32_t*)J->pel.p,
                                   (const double*)J->jt.p, (const double*)J->rt.p, s);
                 launches += 2;

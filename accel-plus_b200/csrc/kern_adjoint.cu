@@ -19,6 +19,7 @@
 #include <cstdint>
 #include "adjoint.cuh"
 #include "elem_fast.cuh"
+#include "jacobian.cuh"
 #include "kernels.h"
 
 namespace accel {
@@ -182,19 +183,95 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_turn_reverse(const AdjParam
 }
 
 // ---- block-Jacobian tape -------------------------------------------------------------------------
+// Elements the explicit-Jacobian maps do not cover take the literal map on dual numbers whose
+// directions are the current Jacobian's rows (J <- J_elem J), out of line, by value.
+__device__ __noinline__ jac::JS<6> dual_elem(jac::JS<6> j, const DevElem* __restrict__ e) {
+    Dual<6> r[6];
+#pragma unroll
+    for (int i = 0; i < 6; i++) {
+        r[i] = Dual<6>(j.s[i]);
+#pragma unroll
+        for (int k = 0; k < 6; k++) r[i].d[k] = j.m[6 * i + k];
+    }
+    adj::forward_t(*e, r);
+#pragma unroll
+    for (int i = 0; i < 6; i++) {
+        j.s[i] = r[i].v;
+#pragma unroll
+        for (int k = 0; k < 6; k++) j.m[6 * i + k] = r[i].d[k];
+    }
+    return j;
+}
+
+// GENERAL = false: the line holds only the element kinds below and every parameter element is a
+// multipole with one B or A coefficient (the host checks, jtape_needs_general), so no call is
+// made and the kernel keeps the small register budget of the explicit maps.
+template <bool GENERAL>
+__device__ __forceinline__ void jac_elem(jac::JS<6>& j, const DevElem* __restrict__ e) {
+    if (jac::lost(j.s)) return;
+    switch (e->op) {
+    case OP_NOP: return;
+    case OP_DRIFT: jac::drift_len(j, e->v[V_LEN]); return;
+    case OP_STRMPOLE:
+    case OP_STRKICK: jac::strmpole(j, *e, -1, 0); return;
+    case OP_BENDMPOLE:
+        if (e->flags) break;  // radiation (refused by the adjoint; kept general here)
+        jac::bendmpole(j, *e);
+        return;
+    case OP_CAVITY: jac::cavity(j, *e); return;
+    case OP_APERTURE:
+        if (jac::aperture_hit(j.s, *e)) return;
+        if (e->v[V_LEN] != 0) {
+            jac::drift_len(j, e->v[V_LEN]);
+            jac::aperture_hit(j.s, *e);
+        }
+        return;
+    default: break;
+    }
+    if constexpr (GENERAL) j = dual_elem(j, e);
+}
+
+// A parameter element outside the explicit path (several parameters, Quad K, ...): dual numbers
+// with parameter directions (adj::forward_params); writes the unit Jacobian and the parameter
+// sensitivities and returns the state.
+__device__ __noinline__ fast::St param_elem_dual(jac::JS<6> j, const DevElem* __restrict__ e, int np,
+                                                 const int32_t* __restrict__ kinds,
+                                                 const int32_t* __restrict__ indices, double* __restrict__ J,
+                                                 double* __restrict__ S, int64_t n, int64_t sstride) {
+    int kind[adj::kMaxParamsPerElem], index[adj::kMaxParamsPerElem];
+    for (int q = 0; q < np; q++) { kind[q] = kinds[q]; index[q] = indices[q]; }
+    Dual<adj::kPD> q[6];
+#pragma unroll
+    for (int i = 0; i < 6; i++) {
+        q[i] = Dual<adj::kPD>(j.s[i]);
+#pragma unroll
+        for (int k = 0; k < 6; k++) q[i].d[k] = j.m[6 * i + k];
+    }
+    adj::forward_params(*e, q, np, kind, index);
+#pragma unroll
+    for (int i = 0; i < 6; i++)
+#pragma unroll
+        for (int k = 0; k < 6; k++) J[(6 * i + k) * n] = q[i].d[k];
+    for (int p = 0; p < np; p++)
+#pragma unroll
+        for (int i = 0; i < 6; i++) S[p * sstride + i * n] = q[i].d[6 + p];
+    return fast::St{q[0].v, q[1].v, q[2].v, q[3].v, q[4].v, q[5].v};
+}
+
 // The elements of a turn are cut after each parameter element (one carrying parameters whose
 // gradient is returned): unit c = the plain elements before parameter element c, then element c
 // itself (c = 0 .. npe-1), and a last unit of the plain elements after the last one.  For a chunk
 // of nt turns of the current segment (turn-start states in turn_tape, turns j0 .. j0+nt-1), one
-// thread per (turn, particle) re-tracks its turn with dual numbers restarted at every unit, and
-// stores, with t = turn - j0,
+// thread per (turn, particle) re-tracks its turn carrying the Jacobian explicitly
+// (jacobian.cuh), restarted at every unit, and stores, with t = turn - j0,
 //   jt[((t * (npe + 1) + c) * 36 + 6 * i + k) * n + p] = d out_i / d in_k of unit c,
 //   st[((t * nparam + q) * 6 + i) * n + p]            = d out_i / d p_q at the output of the
 //                                                        unit whose element carries parameter q.
 // Every turn of the chunk is independent, so this runs nt x n threads wide; the sequential part
 // of the reverse sweep (k_adj_jsweep) is left with 6x6 products and dot products.  A particle lost
 // by the end of the forward run carries no adjoint and is skipped.
-__global__ void __launch_bounds__(128) k_adj_jtape(const AdjParams a, const double* turn_tape, int j0, int nt,
+template <bool GENERAL>
+__global__ void __launch_bounds__(128, GENERAL ? 1 : 3) k_adj_jtape(const AdjParams a, const double* turn_tape, int j0, int nt,
                                                    const double* final_x, int npe, double* jt, double* sens) {
     const int64_t n = a.n;
     const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -203,53 +280,52 @@ __global__ void __launch_bounds__(128) k_adj_jtape(const AdjParams a, const doub
     const int64_t p = gid - (int64_t)t * n;
     if (final_x[p] != final_x[p]) return;
     const double* s0 = turn_tape + (int64_t)(j0 + t) * 6 * n;
-    Dual<6> r[6];
+    jac::JS<6> j;
 #pragma unroll
-    for (int i = 0; i < 6; i++) {
-        r[i] = Dual<6>(s0[i * n + p]);
-        r[i].d[i] = 1.0;
-    }
+    for (int i = 0; i < 6; i++) j.s[i] = s0[i * n + p];
+    jac::set_identity(j);
     int c = 0;
     for (int e = 0; e < a.ne; e++) {
         const int np = a.pcount[e];
         if (np == 0) {
-            adj::forward_t(a.tbl[e], r);
+            jac_elem<GENERAL>(j, a.tbl + e);
             continue;
         }
         const int f = a.pfirst[e];
-        int kind[adj::kMaxParamsPerElem], index[adj::kMaxParamsPerElem];
-        for (int j = 0; j < np; j++) { kind[j] = a.pkind[f + j]; index[j] = a.pindex[f + j]; }
-        Dual<adj::kPD> q[6];
-#pragma unroll
-        for (int i = 0; i < 6; i++) {
-            q[i] = Dual<adj::kPD>(r[i].v);
-#pragma unroll
-            for (int k = 0; k < 6; k++) q[i].d[k] = r[i].d[k];
-        }
-        adj::forward_params(a.tbl[e], q, np, kind, index);
+        const DevElem* el = a.tbl + e;
         double* J = jt + ((int64_t)t * (npe + 1) + c) * 36 * n + p;
+        double* S = sens + ((int64_t)t * a.nparam + f) * 6 * n + p;
+        const int kind = a.pkind[f];
+        if (np == 1 && (el->op == OP_STRMPOLE || el->op == OP_STRKICK) && (kind == adj::PK_B || kind == adj::PK_A) &&
+            !jac::lost(j.s)) {
+            jac::JS<7> q;
 #pragma unroll
-        for (int i = 0; i < 6; i++) {
+            for (int i = 0; i < 6; i++) {
+                q.s[i] = j.s[i];
 #pragma unroll
-            for (int k = 0; k < 6; k++) J[(6 * i + k) * n] = q[i].d[k];
+                for (int k = 0; k < 6; k++) q.m[7 * i + k] = j.m[6 * i + k];
+                q.m[7 * i + 6] = 0.0;
+            }
+            jac::strmpole(q, *el, kind, a.pindex[f]);
+#pragma unroll
+            for (int i = 0; i < 6; i++) {
+#pragma unroll
+                for (int k = 0; k < 6; k++) J[(6 * i + k) * n] = q.m[7 * i + k];
+                S[i * n] = q.m[7 * i + 6];
+                j.s[i] = q.s[i];
+            }
+        } else if constexpr (GENERAL) {
+            const fast::St o = param_elem_dual(j, el, np, a.pkind + f, a.pindex + f, J, S, n, 6 * n);
+            j.s[0] = o.x; j.s[1] = o.px; j.s[2] = o.y; j.s[3] = o.py; j.s[4] = o.z; j.s[5] = o.d;
         }
-        for (int j = 0; j < np; j++) {
-            double* S = sens + ((int64_t)t * a.nparam + f + j) * 6 * n + p;
-#pragma unroll
-            for (int i = 0; i < 6; i++) S[i * n] = q[i].d[6 + j];
-        }
-#pragma unroll
-        for (int i = 0; i < 6; i++) {
-            r[i] = Dual<6>(q[i].v);
-            r[i].d[i] = 1.0;
-        }
+        jac::set_identity(j);
         c++;
     }
     double* J = jt + ((int64_t)t * (npe + 1) + npe) * 36 * n + p;
 #pragma unroll
     for (int i = 0; i < 6; i++)
 #pragma unroll
-        for (int k = 0; k < 6; k++) J[(6 * i + k) * n] = r[i].d[k];
+        for (int k = 0; k < 6; k++) J[(6 * i + k) * n] = j.m[6 * i + k];
 }
 
 // Reverse sweep over the chunk's turns, last to first, one particle per thread: at each unit's
@@ -325,10 +401,36 @@ void launch_adj_turn_reverse(const AdjParams& a, const double* r_start, const do
     const size_t sh = sizeof(double) * (kAdjThreads / 32) * (size_t)a.nparam;
     k_adj_turn_reverse<<<adj_blocks(a.n), kAdjThreads, sh, s>>>(a, r_start, final_x);
 }
+bool jtape_needs_general(const DevElem* t, int ne, const int32_t* pcount, const int32_t* pfirst,
+                         const int32_t* pkind) {
+    for (int e = 0; e < ne; e++) {
+        const int op = t[e].op;
+        if (pcount[e] == 0) {
+            switch (op) {
+            case OP_NOP: case OP_DRIFT: case OP_STRMPOLE: case OP_STRKICK: case OP_CAVITY: case OP_APERTURE:
+                break;
+            case OP_BENDMPOLE:
+                if (t[e].flags) return true;
+                break;
+            default:
+                return true;
+            }
+        } else {
+            const int k = pkind[pfirst[e]];
+            if (pcount[e] != 1 || !(op == OP_STRMPOLE || op == OP_STRKICK) || !(k == adj::PK_B || k == adj::PK_A))
+                return true;
+        }
+    }
+    return false;
+}
+
 void launch_adj_jtape(const AdjParams& a, const double* turn_tape, int j0, int nt, const double* final_x,
-                      int npe, double* jt, double* sens, cudaStream_t s) {
+                      int npe, double* jt, double* sens, bool general, cudaStream_t s) {
     const int64_t threads = a.n * (int64_t)nt;
-    k_adj_jtape<<<(unsigned)((threads + 127) / 128), 128, 0, s>>>(a, turn_tape, j0, nt, final_x, npe, jt, sens);
+    if (general)
+        k_adj_jtape<true><<<(unsigned)((threads + 127) / 128), 128, 0, s>>>(a, turn_tape, j0, nt, final_x, npe, jt, sens);
+    else
+        k_adj_jtape<false><<<(unsigned)((threads + 127) / 128), 128, 0, s>>>(a, turn_tape, j0, nt, final_x, npe, jt, sens);
 }
 void launch_adj_jsweep(const AdjParams& a, int nt, const double* final_x, int npe, const int32_t* pelem,
                        const double* jt, const double* sens, cudaStream_t s) {

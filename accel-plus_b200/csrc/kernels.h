@@ -94,8 +94,12 @@ void launch_adj_turn_reverse(const AdjParams& a, const double* r_start, const do
 void launch_adj_reduce(const double* part, int nblk, int nparam, double* out, cudaStream_t s);
 // block-Jacobian tape of nt turns (unit Jacobians and parameter sensitivities) and the reverse
 // sweep over it (kern_adjoint.cu)
+// general: the line has elements or parameters outside the explicit-Jacobian maps
+// (jtape_needs_general)
 void launch_adj_jtape(const AdjParams& a, const double* turn_tape, int j0, int nt, const double* final_x,
-                      int npe, double* jt, double* sens, cudaStream_t s);
+                      int npe, double* jt, double* sens, bool general, cudaStream_t s);
+bool jtape_needs_general(const DevElem* host_tbl, int ne, const int32_t* pcount, const int32_t* pfirst,
+                         const int32_t* pkind);
 void launch_adj_jsweep(const AdjParams& a, int nt, const double* final_x, int npe, const int32_t* pelem,
                        const double* jt, const double* sens, cudaStream_t s);
 
