@@ -61,10 +61,12 @@ struct accel_adjoint {
     int npe = 0;
     int chunk = 0;               // turns per block-Jacobian tape; 0: per-turn element reversal
     bool general = true;         // the tape needs the dual-number fallback (jtape_needs_general)
-    DevBuf st, lam, aos, tape, ckpt, turn_tape, part, meta, final_x, grad, jt, rt, pel;
+    bool all_turns = false;      // turn_tape holds every turn of the run (one recompute launch)
+    DevBuf st, lam, aos, tape, ckpt, turn_tape, part, meta, final_x, grad, jt, rt, pel, grow;
     bool have_forward = false;
     ~accel_adjoint() {
-        for (DevBuf* b : {&st, &lam, &aos, &tape, &ckpt, &turn_tape, &part, &meta, &final_x, &grad, &jt, &rt, &pel})
+        for (DevBuf* b : {&st, &lam, &aos, &tape, &ckpt, &turn_tape, &part, &meta, &final_x, &grad, &jt, &rt, &pel,
+                          &grow})
             b->release();
     }
 };
@@ -168,17 +170,22 @@ int accel_adjoint_create(accel_line* L, int N, int nturn, int every, const int32
     }
     CK(cudaMemcpy(L->d_tbl.p, L->host_tbl.data(), L->host_tbl.size() * sizeof(DevElem), cudaMemcpyHostToDevice));
     const size_t s6 = sizeof(double) * 6 * (size_t)N;
-    int nblk = adj_blocks(N);
+    const int nblk = adj_part_rows(N);
     for (int e = 0; e < ne; e++)
         if (J->pcount[(size_t)e] > 0) J->pelem.push_back(e);
     J->npe = (int)J->pelem.size();
     J->general = jtape_needs_general(L->host_tbl.data(), ne, J->pcount.data(), J->pfirst.data(), J->pkind.data());
-    const double per_turn = 8.0 * (double)N * (36.0 * (J->npe + 1) + 6.0 * nparam);
+    // every turn-start state kept when that fits the tape budget: the segments are then
+    // recomputed together in one launch instead of one narrow launch each
+    J->all_turns = J->nseg > 1 && (double)s6 * nturn <= kTapeBudgetBytes;
+    const size_t span = (size_t)adj_tile_span(N);  // tiled tapes: 32-particle tiles
+    const double per_turn = 8.0 * (double)span * (36.0 * (J->npe + 1) + 6.0 * nparam);
     J->chunk = (int)std::min<double>(std::min(every, nturn), std::floor(kTapeBudgetBytes / per_turn));
     if (J->chunk >= 1) {
-        const size_t c = (size_t)J->chunk, nn = (size_t)N;
+        const size_t c = (size_t)J->chunk, nn = span;
         if ((s = J->jt.ensure(sizeof(double) * c * (size_t)(J->npe + 1) * 36 * nn)) ||
             (s = J->rt.ensure(sizeof(double) * std::max<size_t>(1, c * (size_t)nparam * 6 * nn))) ||
+            (nparam > 384 && (s = J->grow.ensure(sizeof(double) * nn * (size_t)nparam))) ||
             (s = J->pel.ensure(sizeof(int32_t) * (size_t)std::max(1, J->npe))))
             return s;
         if (J->npe > 0)
@@ -189,7 +196,7 @@ int accel_adjoint_create(accel_line* L, int N, int nturn, int every, const int32
     }
     if ((s = J->st.ensure(s6)) || (s = J->lam.ensure(s6)) || (s = J->aos.ensure(s6)) ||
         (s = J->ckpt.ensure(s6 * (size_t)J->nseg)) ||
-        (s = J->turn_tape.ensure(s6 * (size_t)std::min(every, nturn))) ||
+        (s = J->turn_tape.ensure(s6 * (size_t)(J->all_turns ? nturn : std::min(every, nturn)))) ||
         (s = J->part.ensure(sizeof(double) * (size_t)std::max(1, nblk * nparam))) ||
         (s = J->meta.ensure(sizeof(int32_t) * (size_t)(2 * ne + 2 * std::max(1, nparam)))) ||
         (s = J->final_x.ensure(sizeof(double) * (size_t)N)) ||
@@ -261,29 +268,37 @@ int accel_adjoint_backward(accel_adjoint* J, const double* g, double* dr0, doubl
         in = (const double*)J->aos.p;
     }
     launch_aos_to_soa(in, (double*)J->lam.p, J->n, s);
-    const int nblk = adj_blocks(J->n);
+    const int nblk = adj_part_rows(J->n);
     if (J->nparam > 0) CK(cudaMemsetAsync(J->part.p, 0, sizeof(double) * (size_t)nblk * J->nparam, s));
     AdjParams a = params_of(J);
     int64_t launches = 1;
+    if (J->all_turns) {
+        launch_adj_recompute_all(a, (const double*)J->ckpt.p, (double*)J->turn_tape.p, J->nturn, J->every, s);
+        launches++;
+    }
     for (int seg = J->nseg - 1; seg >= 0; seg--) {
         const int t0 = seg * J->every;
         const int nt = std::min(J->every, J->nturn - t0);
-        const double* ck = (const double*)J->ckpt.p + (size_t)seg * 6 * J->n;
-        launch_adj_recompute(a, ck, (double*)J->turn_tape.p, nt, s);
-        launches++;
+        const double* tt = (const double*)J->turn_tape.p;  // this segment's turn-start states
+        if (J->all_turns) {
+            tt += (size_t)t0 * 6 * J->n;
+        } else {
+            const double* ck = (const double*)J->ckpt.p + (size_t)seg * 6 * J->n;
+            launch_adj_recompute(a, ck, (double*)J->turn_tape.p, nt, s);
+            launches++;
+        }
         if (J->chunk > 0) {
             for (int hi = nt; hi > 0; hi -= J->chunk) {
                 const int lo = std::max(0, hi - J->chunk);
-                launch_adj_jtape(a, (const double*)J->turn_tape.p, lo, hi - lo, (const double*)J->final_x.p,
-                                 J->npe, (double*)J->jt.p, (double*)J->rt.p, J->general, s);
+                launch_adj_jtape(a, tt, lo, hi - lo, (const double*)J->final_x.p, J->npe, (double*)J->jt.p,
+                                 (double*)J->rt.p, J->general, s);
                 launch_adj_jsweep(a, hi - lo, (const double*)J->final_x.p, J->npe, (const int32_t*)J->pel.p,
-                                  (const double*)J->jt.p, (const double*)J->rt.p, s);
+                                  (const double*)J->jt.p, (const double*)J->rt.p, (double*)J->grow.p, s);
                 launches += 2;
             }
         } else {
             for (int j = nt - 1; j >= 0; j--) {
-                launch_adj_turn_reverse(a, (const double*)J->turn_tape.p + (size_t)j * 6 * J->n,
-                                        (const double*)J->final_x.p, s);
+                launch_adj_turn_reverse(a, tt + (size_t)j * 6 * J->n, (const double*)J->final_x.p, s);
                 launches++;
             }
         }

@@ -16,6 +16,7 @@
 // own row of pacc[nblocks][nparam]; k_adj_reduce sums the rows in order.  No atomics, so the
 // result is deterministic.
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <cstdint>
 #include "adjoint.cuh"
 #include "elem_fast.cuh"
@@ -92,6 +93,7 @@ __device__ __forceinline__ void fast_turn(const AdjParams& a, double* r) {
 namespace {
 constexpr unsigned FULL = 0xffffffffu;
 constexpr int kAdjThreads = 64;
+constexpr int kTile = 32;  // particles per tile of the tape layouts (one warp of the sweep)
 }  // namespace
 
 int adj_blocks(int64_t n) { return (int)((n + kAdjThreads - 1) / kAdjThreads); }
@@ -127,6 +129,25 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_recompute(const AdjParams a
     load6(ck, a.n, p, r);
     for (int j = 0; j < nt; j++) {
         store6(turn_tape + (int64_t)j * 6 * a.n, a.n, p, r);
+        if (j + 1 < nt && !(r[0] != r[0])) fast_turn(a, r);
+    }
+}
+
+// Recompute every checkpoint segment at once, (segment, particle) per thread: turn_tape holds
+// the starting state of every turn of the run.  The segments are independent given their
+// checkpoints, so this is nseg times wider than recomputing one segment before its reversal.
+__global__ void __launch_bounds__(kAdjThreads) k_adj_recompute_all(const AdjParams a, const double* ckpt,
+                                                                   double* turn_tape, int nturn, int every) {
+    const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int nseg = (nturn + every - 1) / every;
+    if (gid >= (int64_t)nseg * a.n) return;
+    const int seg = (int)(gid / a.n);
+    const int64_t p = gid - (int64_t)seg * a.n;
+    const int t0 = seg * every, nt = min(every, nturn - t0);
+    double r[6];
+    load6(ckpt + (int64_t)seg * 6 * a.n, a.n, p, r);
+    for (int j = 0; j < nt; j++) {
+        store6(turn_tape + (int64_t)(t0 + j) * 6 * a.n, a.n, p, r);
         if (j + 1 < nt && !(r[0] != r[0])) fast_turn(a, r);
     }
 }
@@ -237,7 +258,7 @@ __device__ __forceinline__ void jac_elem(jac::JS<6>& j, const DevElem* __restric
 __device__ __noinline__ fast::St param_elem_dual(jac::JS<6> j, const DevElem* __restrict__ e, int np,
                                                  const int32_t* __restrict__ kinds,
                                                  const int32_t* __restrict__ indices, double* __restrict__ J,
-                                                 double* __restrict__ S, int64_t n, int64_t sstride) {
+                                                 double* __restrict__ S, int64_t estride, int64_t pstride) {
     int kind[adj::kMaxParamsPerElem], index[adj::kMaxParamsPerElem];
     for (int q = 0; q < np; q++) { kind[q] = kinds[q]; index[q] = indices[q]; }
     Dual<adj::kPD> q[6];
@@ -251,10 +272,10 @@ __device__ __noinline__ fast::St param_elem_dual(jac::JS<6> j, const DevElem* __
 #pragma unroll
     for (int i = 0; i < 6; i++)
 #pragma unroll
-        for (int k = 0; k < 6; k++) J[(6 * i + k) * n] = q[i].d[k];
+        for (int k = 0; k < 6; k++) J[(6 * i + k) * estride] = q[i].d[k];
     for (int p = 0; p < np; p++)
 #pragma unroll
-        for (int i = 0; i < 6; i++) S[p * sstride + i * n] = q[i].d[6 + p];
+        for (int i = 0; i < 6; i++) S[p * pstride + i * estride] = q[i].d[6 + p];
     return fast::St{q[0].v, q[1].v, q[2].v, q[3].v, q[4].v, q[5].v};
 }
 
@@ -263,10 +284,12 @@ __device__ __noinline__ fast::St param_elem_dual(jac::JS<6> j, const DevElem* __
 // itself (c = 0 .. npe-1), and a last unit of the plain elements after the last one.  For a chunk
 // of nt turns of the current segment (turn-start states in turn_tape, turns j0 .. j0+nt-1), one
 // thread per (turn, particle) re-tracks its turn carrying the Jacobian explicitly
-// (jacobian.cuh), restarted at every unit, and stores, with t = turn - j0,
-//   jt[((t * (npe + 1) + c) * 36 + 6 * i + k) * n + p] = d out_i / d in_k of unit c,
-//   st[((t * nparam + q) * 6 + i) * n + p]            = d out_i / d p_q at the output of the
-//                                                        unit whose element carries parameter q.
+// (jacobian.cuh), restarted at every unit, and stores, with t = turn - j0, particle p in tile
+// b = p / 32 at lane l = p % 32 and ntile = ceil(n / 32) (one unit of one tile is contiguous, so
+// the sweep streams it into shared memory as a block):
+//   jt[(((t * (npe + 1) + c) * ntile + b) * 36 + 6 * i + k) * 32 + l] = d out_i / d in_k of unit c,
+//   st[(((t * nparam + q) * ntile + b) * 6 + i) * 32 + l]             = d out_i / d p_q at the
+//                                                 output of the unit whose element carries q.
 // Every turn of the chunk is independent, so this runs nt x n threads wide; the sequential part
 // of the reverse sweep (k_adj_jsweep) is left with 6x6 products and dot products.  A particle lost
 // by the end of the forward run carries no adjoint and is skipped.
@@ -279,6 +302,8 @@ __global__ void __launch_bounds__(128, GENERAL ? 1 : 3) k_adj_jtape(const AdjPar
     const int t = (int)(gid / n);
     const int64_t p = gid - (int64_t)t * n;
     if (final_x[p] != final_x[p]) return;
+    const int64_t ntile = (n + kTile - 1) / kTile, b = p / kTile;
+    const int l = (int)(p % kTile);
     const double* s0 = turn_tape + (int64_t)(j0 + t) * 6 * n;
     jac::JS<6> j;
 #pragma unroll
@@ -293,8 +318,8 @@ __global__ void __launch_bounds__(128, GENERAL ? 1 : 3) k_adj_jtape(const AdjPar
         }
         const int f = a.pfirst[e];
         const DevElem* el = a.tbl + e;
-        double* J = jt + ((int64_t)t * (npe + 1) + c) * 36 * n + p;
-        double* S = sens + ((int64_t)t * a.nparam + f) * 6 * n + p;
+        double* J = jt + ((((int64_t)t * (npe + 1) + c) * ntile + b) * 36) * kTile + l;
+        double* S = sens + ((((int64_t)t * a.nparam + f) * ntile + b) * 6) * kTile + l;
         const int kind = a.pkind[f];
         if (np == 1 && (el->op == OP_STRMPOLE || el->op == OP_STRKICK) && (kind == adj::PK_B || kind == adj::PK_A) &&
             !jac::lost(j.s)) {
@@ -310,76 +335,116 @@ __global__ void __launch_bounds__(128, GENERAL ? 1 : 3) k_adj_jtape(const AdjPar
 #pragma unroll
             for (int i = 0; i < 6; i++) {
 #pragma unroll
-                for (int k = 0; k < 6; k++) J[(6 * i + k) * n] = q.m[7 * i + k];
-                S[i * n] = q.m[7 * i + 6];
+                for (int k = 0; k < 6; k++) J[(6 * i + k) * kTile] = q.m[7 * i + k];
+                S[i * kTile] = q.m[7 * i + 6];
                 j.s[i] = q.s[i];
             }
         } else if constexpr (GENERAL) {
-            const fast::St o = param_elem_dual(j, el, np, a.pkind + f, a.pindex + f, J, S, n, 6 * n);
+            const fast::St o = param_elem_dual(j, el, np, a.pkind + f, a.pindex + f, J, S, kTile, ntile * 6 * kTile);
             j.s[0] = o.x; j.s[1] = o.px; j.s[2] = o.y; j.s[3] = o.py; j.s[4] = o.z; j.s[5] = o.d;
         }
         jac::set_identity(j);
         c++;
     }
-    double* J = jt + ((int64_t)t * (npe + 1) + npe) * 36 * n + p;
+    double* J = jt + ((((int64_t)t * (npe + 1) + npe) * ntile + b) * 36) * kTile + l;
 #pragma unroll
     for (int i = 0; i < 6; i++)
 #pragma unroll
-        for (int k = 0; k < 6; k++) J[(6 * i + k) * n] = j.m[6 * i + k];
+        for (int k = 0; k < 6; k++) J[(6 * i + k) * kTile] = j.m[6 * i + k];
 }
 
-// Reverse sweep over the chunk's turns, last to first, one particle per thread: at each unit's
-// output the parameter gradients take sens^T lam, then lam <- J^T lam.  pelem lists the parameter
-// elements in line order.
-__global__ void __launch_bounds__(kAdjThreads) k_adj_jsweep(const AdjParams a, int nt, const double* final_x,
-                                                            int npe, const int32_t* pelem, const double* jt,
-                                                            const double* sens) {
-    extern __shared__ double rows[];  // [warps][nparam]
-    const int64_t n = a.n;
-    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    for (int j = threadIdx.x; j < nwarps * a.nparam; j += blockDim.x) rows[j] = 0.0;
-    __syncthreads();
+// Reverse sweep over the chunk's turns, last to first: at each unit's output the parameter
+// gradients take sens^T lam, then lam <- J^T lam.  pelem lists the parameter elements in line
+// order.  One warp per tile of 32 particles, one particle per lane.  The sweep is a dependent
+// chain per particle and the tile count is small (n / 32), so the unit tiles are streamed into
+// shared memory kSweepStages units ahead with asynchronous copies (cp.async, waited on with
+// cp.async.wait_group: no spin loop) and each step reads its operands from shared memory.
+// Gradients: each lane adds into its own slot rows[q * 32 + lane] (shared memory, or global
+// memory past kSweepSmemParams parameters), summed over the lanes in order at the end.
+constexpr int kSweepStages = 6;
+constexpr int kSweepSmemParams = 384;
+constexpr int kStageDoubles = (36 + 6 * adj::kMaxParamsPerElem) * kTile;
+
+__device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+__global__ void __launch_bounds__(kTile) k_adj_jsweep(const AdjParams a, int nt, const double* final_x, int npe,
+                                                      const int32_t* pelem, const double* jt, const double* sens,
+                                                      double* grow) {
+    extern __shared__ __align__(16) double smem[];
+    double* stage = smem;                                    // [kSweepStages][kStageDoubles]
+    const bool srows = a.nparam <= kSweepSmemParams;
+    double* rows = srows ? smem + kSweepStages * kStageDoubles  // [nparam][32]
+                         : grow + (int64_t)blockIdx.x * a.nparam * kTile;
+    const int64_t n = a.n, ntile = (n + kTile - 1) / kTile, b = blockIdx.x;
+    const int lane = threadIdx.x;
+    const int64_t p = b * kTile + lane;
+    for (int q = 0; q < a.nparam; q++) rows[q * kTile + lane] = 0.0;
     const bool alive = p < n && !(final_x[p] != final_x[p]);
     double lam[6] = {0, 0, 0, 0, 0, 0};
     if (alive) load6(a.lam, n, p, lam);
-    for (int t = nt - 1; t >= 0; t--) {
-        for (int c = npe; c >= 0; c--) {
+    const int U = nt * (npe + 1);  // units of the chunk; unit u = t * (npe + 1) + c
+    // issue unit u into stage slot st: its J tile and, for a parameter unit, its sens tiles
+    auto issue = [&](int u, int st) {
+        if (u >= 0) {
+            const int t = u / (npe + 1), c = u - t * (npe + 1);
+            double* dst = stage + st * kStageDoubles;
+            const double* src = jt + (((int64_t)u * ntile + b) * 36) * kTile;
+            for (int k = lane; k < 36 * kTile / 2; k += kTile) cp_async16(dst + 2 * k, src + 2 * k);
             if (c < npe) {
-                const int e = pelem[c];
-                const int np = a.pcount[e], f = a.pfirst[e];
-                for (int j = 0; j < np; j++) {  // np is the same for every lane (one lattice)
-                    double v = 0.0;
-                    if (alive) {
-                        const double* S = sens + ((int64_t)t * a.nparam + f + j) * 6 * n + p;
-#pragma unroll
-                        for (int i = 0; i < 6; i++) v = fma(S[i * n], lam[i], v);
-                    }
-                    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
-                    if (lane == 0) rows[warp * a.nparam + f + j] += v;
+                const int e = pelem[c], np = a.pcount[e], f = a.pfirst[e];
+                for (int j = 0; j < np; j++) {
+                    const double* ss = sens + ((((int64_t)t * a.nparam + f + j) * ntile + b) * 6) * kTile;
+                    double* sd = dst + (36 + 6 * j) * kTile;
+                    for (int k = lane; k < 6 * kTile / 2; k += kTile) cp_async16(sd + 2 * k, ss + 2 * k);
                 }
-            }
-            if (alive) {
-                const double* J = jt + ((int64_t)t * (npe + 1) + c) * 36 * n + p;
-                double out[6];
-#pragma unroll
-                for (int k = 0; k < 6; k++) {
-                    double acc = 0.0;
-#pragma unroll
-                    for (int i = 0; i < 6; i++) acc = fma(J[(6 * i + k) * n], lam[i], acc);
-                    out[k] = acc;
-                }
-#pragma unroll
-                for (int k = 0; k < 6; k++) lam[k] = out[k];
             }
         }
+        cp_async_commit();
+    };
+    for (int i = 0; i < kSweepStages; i++) issue(U - 1 - i, i);
+    for (int i = 0; i < U; i++) {
+        const int u = U - 1 - i, st = i % kSweepStages;
+        const int t = u / (npe + 1), c = u - t * (npe + 1);
+        cp_async_wait<kSweepStages - 1>();
+        __syncwarp();
+        const double* S = stage + st * kStageDoubles;
+        if (c < npe && alive) {
+            const int e = pelem[c], np = a.pcount[e], f = a.pfirst[e];
+            for (int j = 0; j < np; j++) {
+                double v = 0.0;
+#pragma unroll
+                for (int k = 0; k < 6; k++) v = fma(S[(36 + 6 * j + k) * kTile + lane], lam[k], v);
+                rows[(f + j) * kTile + lane] += v;
+            }
+        }
+        if (alive) {
+            double out[6];
+#pragma unroll
+            for (int k = 0; k < 6; k++) {
+                double acc = 0.0;
+#pragma unroll
+                for (int m = 0; m < 6; m++) acc = fma(S[(6 * m + k) * kTile + lane], lam[m], acc);
+                out[k] = acc;
+            }
+#pragma unroll
+            for (int k = 0; k < 6; k++) lam[k] = out[k];
+        }
+        __syncwarp();
+        issue(u - kSweepStages, st);
     }
+    cp_async_wait<0>();
     if (alive) store6(a.lam, n, p, lam);
-    __syncthreads();
-    for (int j = threadIdx.x; j < a.nparam; j += blockDim.x) {
-        double s = 0;
-        for (int w = 0; w < nwarps; w++) s += rows[w * a.nparam + j];
-        a.pgrad_part[(int64_t)blockIdx.x * a.nparam + j] += s;
+    __syncwarp();
+    for (int q = lane; q < a.nparam; q += kTile) {
+        double sum = 0.0;
+        for (int w = 0; w < kTile; w++) sum += rows[q * kTile + w];
+        a.pgrad_part[b * a.nparam + q] += sum;
     }
 }
 
@@ -397,6 +462,13 @@ void launch_adj_forward(const AdjParams& a, double* ckpt, int nturn, int every, 
 void launch_adj_recompute(const AdjParams& a, const double* ck, double* turn_tape, int nt, cudaStream_t s) {
     k_adj_recompute<<<adj_blocks(a.n), kAdjThreads, 0, s>>>(a, ck, turn_tape, nt);
 }
+void launch_adj_recompute_all(const AdjParams& a, const double* ckpt, double* turn_tape, int nturn, int every,
+                              cudaStream_t s) {
+    const int64_t threads = (int64_t)((nturn + every - 1) / every) * a.n;
+    k_adj_recompute_all<<<(unsigned)((threads + kAdjThreads - 1) / kAdjThreads), kAdjThreads, 0, s>>>(
+        a, ckpt, turn_tape, nturn, every);
+}
+int adj_part_rows(int64_t n) { return (int)std::max<int64_t>((n + kTile - 1) / kTile, adj_blocks(n)); }
 void launch_adj_turn_reverse(const AdjParams& a, const double* r_start, const double* final_x, cudaStream_t s) {
     const size_t sh = sizeof(double) * (kAdjThreads / 32) * (size_t)a.nparam;
     k_adj_turn_reverse<<<adj_blocks(a.n), kAdjThreads, sh, s>>>(a, r_start, final_x);
@@ -433,9 +505,12 @@ void launch_adj_jtape(const AdjParams& a, const double* turn_tape, int j0, int n
         k_adj_jtape<false><<<(unsigned)((threads + 127) / 128), 128, 0, s>>>(a, turn_tape, j0, nt, final_x, npe, jt, sens);
 }
 void launch_adj_jsweep(const AdjParams& a, int nt, const double* final_x, int npe, const int32_t* pelem,
-                       const double* jt, const double* sens, cudaStream_t s) {
-    const size_t sh = sizeof(double) * (kAdjThreads / 32) * (size_t)a.nparam;
-    k_adj_jsweep<<<adj_blocks(a.n), kAdjThreads, sh, s>>>(a, nt, final_x, npe, pelem, jt, sens);
+                       const double* jt, const double* sens, double* grow, cudaStream_t s) {
+    const int64_t ntile = (a.n + kTile - 1) / kTile;
+    size_t sh = sizeof(double) * (size_t)kSweepStages * kStageDoubles;
+    if (a.nparam <= kSweepSmemParams) sh += sizeof(double) * (size_t)a.nparam * kTile;
+    cudaFuncSetAttribute(k_adj_jsweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+    k_adj_jsweep<<<(unsigned)ntile, kTile, sh, s>>>(a, nt, final_x, npe, pelem, jt, sens, grow);
 }
 void launch_adj_reduce(const double* part, int nblk, int nparam, double* out, cudaStream_t s) {
     if (nparam > 0) k_adj_reduce<<<(nparam + 127) / 128, 128, 0, s>>>(part, nblk, nparam, out);

@@ -100,7 +100,16 @@ void launch_adj_jtape(const AdjParams& a, const double* turn_tape, int j0, int n
                       int npe, double* jt, double* sens, bool general, cudaStream_t s);
 bool jtape_needs_general(const DevElem* host_tbl, int ne, const int32_t* pcount, const int32_t* pfirst,
                          const int32_t* pkind);
+// grow: per-lane gradient rows in global memory, ntile x nparam x 32 doubles, used only past
+// 384 parameters (null otherwise)
 void launch_adj_jsweep(const AdjParams& a, int nt, const double* final_x, int npe, const int32_t* pelem,
-                       const double* jt, const double* sens, cudaStream_t s);
+                       const double* jt, const double* sens, double* grow, cudaStream_t s);
+// every segment recomputed in one launch: turn_tape holds all nturn turn-start states
+void launch_adj_recompute_all(const AdjParams& a, const double* ckpt, double* turn_tape, int nturn, int every,
+                              cudaStream_t s);
+// rows of the per-block gradient partials (covers both the sweep's tiles and the reverse kernel's blocks)
+int adj_part_rows(int64_t n);
+// doubles of the tiled tapes per turn and unit (ceil(n / 32) * 32 particles)
+inline int64_t adj_tile_span(int64_t n) { return (n + 31) / 32 * 32; }
 
 }  // namespace accel
