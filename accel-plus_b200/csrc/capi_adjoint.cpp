@@ -62,11 +62,11 @@ struct accel_adjoint {
     int chunk = 0;               // turns per block-Jacobian tape; 0: per-turn element reversal
     bool general = true;         // the tape needs the dual-number fallback (jtape_needs_general)
     bool all_turns = false;      // turn_tape holds every turn of the run (one recompute launch)
-    DevBuf st, lam, aos, tape, ckpt, turn_tape, part, meta, final_x, grad, jt, rt, pel, grow;
+    DevBuf st, lam, aos, tape, ckpt, turn_tape, part, meta, final_x, grad, jt, rt, pel, grow, uzd;
     bool have_forward = false;
     ~accel_adjoint() {
         for (DevBuf* b : {&st, &lam, &aos, &tape, &ckpt, &turn_tape, &part, &meta, &final_x, &grad, &jt, &rt, &pel,
-                          &grow})
+                          &grow, &uzd})
             b->release();
     }
 };
@@ -86,6 +86,8 @@ static AdjParams params_of(accel_adjoint* J) {
     a.pkind = m + 2 * J->ne;
     a.pindex = m + 2 * J->ne + std::max(1, J->nparam);
     a.nparam = J->nparam;
+    a.pelem = (const int32_t*)J->pel.p;
+    a.unit_zd = (const int32_t*)J->uzd.p;
     return a;
 }
 
@@ -186,10 +188,14 @@ int accel_adjoint_create(accel_line* L, int N, int nturn, int every, const int32
         if ((s = J->jt.ensure(sizeof(double) * c * (size_t)(J->npe + 1) * 36 * nn)) ||
             (s = J->rt.ensure(sizeof(double) * std::max<size_t>(1, c * (size_t)nparam * 6 * nn))) ||
             (nparam > 384 && (s = J->grow.ensure(sizeof(double) * nn * (size_t)nparam))) ||
-            (s = J->pel.ensure(sizeof(int32_t) * (size_t)std::max(1, J->npe))))
+            (s = J->pel.ensure(sizeof(int32_t) * (size_t)std::max(1, J->npe))) ||
+            (s = J->uzd.ensure(sizeof(int32_t) * (size_t)(J->npe + 1))))
             return s;
         if (J->npe > 0)
             CK(cudaMemcpy(J->pel.p, J->pelem.data(), sizeof(int32_t) * J->pelem.size(), cudaMemcpyHostToDevice));
+        std::vector<int32_t> uz((size_t)J->npe + 1);
+        jtape_unit_zd(L->host_tbl.data(), ne, J->pelem.data(), J->npe, uz.data());
+        CK(cudaMemcpy(J->uzd.p, uz.data(), sizeof(int32_t) * uz.size(), cudaMemcpyHostToDevice));
     } else {
         J->chunk = 0;
         if ((s = J->tape.ensure(s6 * (size_t)ne))) return s;
@@ -273,7 +279,8 @@ int accel_adjoint_backward(accel_adjoint* J, const double* g, double* dr0, doubl
     AdjParams a = params_of(J);
     int64_t launches = 1;
     if (J->all_turns) {
-        launch_adj_recompute_all(a, (const double*)J->ckpt.p, (double*)J->turn_tape.p, J->nturn, J->every, s);
+        launch_adj_recompute(a, (const double*)J->ckpt.p, (double*)J->turn_tape.p, J->nturn, J->every, 0, J->nseg,
+                             s);
         launches++;
     }
     for (int seg = J->nseg - 1; seg >= 0; seg--) {
@@ -283,8 +290,7 @@ int accel_adjoint_backward(accel_adjoint* J, const double* g, double* dr0, doubl
         if (J->all_turns) {
             tt += (size_t)t0 * 6 * J->n;
         } else {
-            const double* ck = (const double*)J->ckpt.p + (size_t)seg * 6 * J->n;
-            launch_adj_recompute(a, ck, (double*)J->turn_tape.p, nt, s);
+            launch_adj_recompute(a, (const double*)J->ckpt.p, (double*)J->turn_tape.p, J->nturn, J->every, seg, 1, s);
             launches++;
         }
         if (J->chunk > 0) {

@@ -21,6 +21,11 @@
 // kick.  Rows are updated from the unchanged rows of the inputs, so no copy of the matrix is
 // needed.  The values follow the fused tracker's maps (elem_fast.cuh) in exact arithmetic; the
 // tape only needs them as linearisation points.
+//
+// ZD = false is for a run of elements in which nothing reads z or changes delta (no cavity):
+// there the z column stays the unit vector e_z and the delta row stays e_delta, so the row
+// updates skip column z and a term "a * row(delta)" only adds a to column delta.  Adding a * 0
+// changes nothing, so this is the same arithmetic with the zero terms left out.
 #pragma once
 #include "engine.h"
 #include "adjoint_params.h"
@@ -30,14 +35,17 @@ namespace jac {
 
 enum { X = 0, PX = 1, Y = 2, PY = 3, Z = 4, D = 5 };
 
-template <int NC>
+template <int NC, bool ZD = true>
 struct JS {
     double s[6];
     double m[6 * NC];
 };
 
-template <int NC>
-__device__ __forceinline__ void set_identity(JS<NC>& j) {
+// columns the row updates touch
+__host__ __device__ constexpr bool live_col(bool zd, int k) { return zd || k != Z; }
+
+template <int NC, bool ZD>
+__device__ __forceinline__ void set_identity(JS<NC, ZD>& j) {
 #pragma unroll
     for (int i = 0; i < 6 * NC; i++) j.m[i] = 0.0;
 #pragma unroll
@@ -45,58 +53,70 @@ __device__ __forceinline__ void set_identity(JS<NC>& j) {
 }
 
 // row[dst] += a * row[src]
-template <int NC>
-__device__ __forceinline__ void axpy(JS<NC>& j, int dst, int src, double a) {
+template <int NC, bool ZD>
+__device__ __forceinline__ void axpy(JS<NC, ZD>& j, int dst, int src, double a) {
 #pragma unroll
-    for (int k = 0; k < NC; k++) j.m[dst * NC + k] = fma(a, j.m[src * NC + k], j.m[dst * NC + k]);
+    for (int k = 0; k < NC; k++)
+        if (live_col(ZD, k)) j.m[dst * NC + k] = fma(a, j.m[src * NC + k], j.m[dst * NC + k]);
+}
+
+// row[dst] += a * row[delta]
+template <int NC, bool ZD>
+__device__ __forceinline__ void dterm(JS<NC, ZD>& j, int dst, double a) {
+    if (ZD) axpy(j, dst, D, a);
+    else j.m[dst * NC + D] += a;
 }
 
 // row[dst] += a * row[s1] + b * row[s2]
-template <int NC>
-__device__ __forceinline__ void add2(JS<NC>& j, int dst, int s1, double a, int s2, double b) {
+template <int NC, bool ZD>
+__device__ __forceinline__ void add2(JS<NC, ZD>& j, int dst, int s1, double a, int s2, double b) {
 #pragma unroll
     for (int k = 0; k < NC; k++)
-        j.m[dst * NC + k] = fma(b, j.m[s2 * NC + k], fma(a, j.m[s1 * NC + k], j.m[dst * NC + k]));
+        if (live_col(ZD, k))
+            j.m[dst * NC + k] = fma(b, j.m[s2 * NC + k], fma(a, j.m[s1 * NC + k], j.m[dst * NC + k]));
 }
 
 // row[dst] += a * row[s1] + b * row[s2] + e * row[s3]
-template <int NC>
-__device__ __forceinline__ void add3(JS<NC>& j, int dst, int s1, double a, int s2, double b, int s3, double e) {
+template <int NC, bool ZD>
+__device__ __forceinline__ void add3(JS<NC, ZD>& j, int dst, int s1, double a, int s2, double b, int s3, double e) {
 #pragma unroll
     for (int k = 0; k < NC; k++)
-        j.m[dst * NC + k] =
-            fma(e, j.m[s3 * NC + k], fma(b, j.m[s2 * NC + k], fma(a, j.m[s1 * NC + k], j.m[dst * NC + k])));
+        if (live_col(ZD, k))
+            j.m[dst * NC + k] =
+                fma(e, j.m[s3 * NC + k], fma(b, j.m[s2 * NC + k], fma(a, j.m[s1 * NC + k], j.m[dst * NC + k])));
 }
 
-// row[dst] = c * row[dst] + a * row[s1] + b * row[s2] (+ e * row[s3] with add3's form)
-template <int NC>
-__device__ __forceinline__ void scale_add2(JS<NC>& j, int dst, double c, int s1, double a, int s2, double b) {
+// row[dst] = c * row[dst] + a * row[s1] (+ b * row[s2])
+template <int NC, bool ZD>
+__device__ __forceinline__ void scale_add1(JS<NC, ZD>& j, int dst, double c, int s1, double a) {
 #pragma unroll
     for (int k = 0; k < NC; k++)
-        j.m[dst * NC + k] = fma(b, j.m[s2 * NC + k], fma(a, j.m[s1 * NC + k], c * j.m[dst * NC + k]));
+        if (live_col(ZD, k)) j.m[dst * NC + k] = fma(a, j.m[s1 * NC + k], c * j.m[dst * NC + k]);
 }
-template <int NC>
-__device__ __forceinline__ void scale_add3(JS<NC>& j, int dst, double c, int s1, double a, int s2, double b, int s3,
-                                           double e) {
+template <int NC, bool ZD>
+__device__ __forceinline__ void scale_add2(JS<NC, ZD>& j, int dst, double c, int s1, double a, int s2, double b) {
 #pragma unroll
     for (int k = 0; k < NC; k++)
-        j.m[dst * NC + k] = fma(e, j.m[s3 * NC + k],
-                                fma(b, j.m[s2 * NC + k], fma(a, j.m[s1 * NC + k], c * j.m[dst * NC + k])));
+        if (live_col(ZD, k))
+            j.m[dst * NC + k] = fma(b, j.m[s2 * NC + k], fma(a, j.m[s1 * NC + k], c * j.m[dst * NC + k]));
 }
 
 __device__ __forceinline__ bool lost(const double* s) { return s[X] != s[X]; }
 
 // fastdrift with NormL = N = L * inv, inv = 1 / (1 + delta)
-template <int NC>
-__device__ __forceinline__ void drift(JS<NC>& j, double N, double inv) {
+template <int NC, bool ZD>
+__device__ __forceinline__ void drift(JS<NC, ZD>& j, double N, double inv) {
     double* s = j.s;
     const double px = s[PX], py = s[PY];
     const double q = fma(px, px, py * py);
     const double w = 0.5 * N * inv;
     // z first: it reads the px, py, delta rows only, like x and y
-    add3(j, Z, PX, -2.0 * w * px, PY, -2.0 * w * py, D, 2.0 * w * q * inv);
-    add2(j, X, PX, N, D, -N * inv * px);
-    add2(j, Y, PY, N, D, -N * inv * py);
+    add2(j, Z, PX, -2.0 * w * px, PY, -2.0 * w * py);
+    dterm(j, Z, 2.0 * w * q * inv);
+    axpy(j, X, PX, N);
+    dterm(j, X, -N * inv * px);
+    axpy(j, Y, PY, N);
+    dterm(j, Y, -N * inv * py);
     s[X] = fma(N, px, s[X]);
     s[Y] = fma(N, py, s[Y]);
     s[Z] = fma(-w, q, s[Z]);
@@ -127,8 +147,8 @@ __device__ __forceinline__ void poly(const double* __restrict__ A, const double*
 // thin kick of weight K; with NC = 7 and a parameter (kind PK_B / PK_A of order pn), its explicit
 // partial is added to column 6: d px/d B_n = -K Re z^n, d py/d B_n = K Im z^n,
 // d px/d A_n = K Im z^n, d py/d A_n = K Re z^n.
-template <int NC>
-__device__ __forceinline__ void kick(JS<NC>& j, const double* A, const double* B, int M, double K, int pkind,
+template <int NC, bool ZD>
+__device__ __forceinline__ void kick(JS<NC, ZD>& j, const double* A, const double* B, int M, double K, int pkind,
                                      int pn) {
     double* s = j.s;
     const double x = s[X], y = s[Y];
@@ -157,8 +177,8 @@ __device__ __forceinline__ void kick(JS<NC>& j, const double* A, const double* B
 }
 
 // StrMPole (accel.cpp:800-847), Yoshida slices; delta is constant inside the element
-template <int NC>
-__device__ __forceinline__ void strmpole(JS<NC>& j, const DevElem& e, int pkind, int pn) {
+template <int NC, bool ZD>
+__device__ __forceinline__ void strmpole(JS<NC, ZD>& j, const DevElem& e, int pkind, int pn) {
     const double* A = e.v + V_A;
     const double* B = e.v + V_B;
     const int M = e.order_eff;
@@ -177,7 +197,8 @@ __device__ __forceinline__ void strmpole(JS<NC>& j, const DevElem& e, int pkind,
 }
 
 // hx drift of length L with curvature h at fixed delta (inv = 1 / (1 + delta))
-__device__ __forceinline__ void hxdrift(JS<6>& j, double L, double h, double inv) {
+template <bool ZD>
+__device__ __forceinline__ void hxdrift(JS<6, ZD>& j, double L, double h, double inv) {
     double* s = j.s;
     const double px = s[PX], py = s[PY];
     const double a = inv * L, b = 0.25 * h * L * L * inv * inv, c = 0.5 * h * L * inv;
@@ -187,12 +208,13 @@ __device__ __forceinline__ void hxdrift(JS<6>& j, double L, double h, double inv
     const double gp = fma(g, px, 1.0);
     // z and y read the old x, px, py, delta rows; x then reads old px, py; px last
     add3(j, Z, X, -h * dd * q, PX, -2.0 * hx1 * dd * px, PY, -2.0 * hx1 * dd * py);
-    axpy(j, Z, D, 2.0 * inv * hx1 * dd * q);
+    dterm(j, Z, 2.0 * inv * hx1 * dd * q);
     add3(j, Y, X, h * a * py * gp, PX, hx1 * a * py * g, PY, hx1 * a * gp);
-    axpy(j, Y, D, -inv * hx1 * a * py * gp);
-    scale_add3(j, X, fma(h * px, a, 1.0), PX, fma(2.0 * b, px, hx1 * a), PY, -2.0 * b * py, D,
-               -inv * fma(hx1 * px, a, 2.0 * b * (pxx - pyy)));
-    scale_add2(j, PX, fma(-2.0 * c, px, 1.0), PY, -2.0 * c * py, D, c * inv * q);
+    dterm(j, Y, -inv * hx1 * a * py * gp);
+    scale_add2(j, X, fma(h * px, a, 1.0), PX, fma(2.0 * b, px, hx1 * a), PY, -2.0 * b * py);
+    dterm(j, X, -inv * fma(hx1 * px, a, 2.0 * b * (pxx - pyy)));
+    scale_add1(j, PX, fma(-2.0 * c, px, 1.0), PY, -2.0 * c * py);
+    dterm(j, PX, c * inv * q);
     s[X] = fma(hx1 * px, a, fma(b, pxx - pyy, s[X]));
     s[PX] = fma(-c, q, px);
     s[Y] = fma(hx1 * a * py, gp, s[Y]);
@@ -200,7 +222,8 @@ __device__ __forceinline__ void hxdrift(JS<6>& j, double L, double h, double inv
 }
 
 // curved kick of weight L (atpass.cpp:199-235, no radiation), field B[0..M] (no skew terms)
-__device__ __forceinline__ void bend_kick(JS<6>& j, const double* B, int M, double h, double K1, double K2,
+template <bool ZD>
+__device__ __forceinline__ void bend_kick(JS<6, ZD>& j, const double* B, int M, double h, double K1, double K2,
                                           double L) {
     double* s = j.s;
     const double x = s[X], y = s[Y], x2 = x * x, y2 = y * y;
@@ -214,7 +237,8 @@ __device__ __forceinline__ void bend_kick(JS<6>& j, const double* B, int M, doub
     const double ax = fma(h, t1x, dr), ay = fma(h, t1y, -di), ad = -h;
     const double t2 = fma(x * y, fma(c43K2, x, K1), c3 * y2 * y);
     const double t2x = y * fma(2.0 * c43K2, x, K1), t2y = fma(x, fma(c43K2, x, K1), 3.0 * c3 * y2);
-    add3(j, PX, X, -L * ax, Y, -L * ay, D, -L * ad);
+    add2(j, PX, X, -L * ax, Y, -L * ay);
+    dterm(j, PX, -L * ad);
     add2(j, PY, X, L * fma(h, t2x, di), Y, L * fma(h, t2y, dr));
     axpy(j, Z, X, -L * h);
     s[PX] = fma(-L, av, s[PX]);
@@ -223,7 +247,8 @@ __device__ __forceinline__ void bend_kick(JS<6>& j, const double* B, int M, doub
 }
 
 // BendMPole without radiation (accel.cpp:649-705): edge, Yoshida slices, edge
-__device__ __forceinline__ void bendmpole(JS<6>& j, const DevElem& e) {
+template <bool ZD>
+__device__ __forceinline__ void bendmpole(JS<6, ZD>& j, const DevElem& e) {
     const double* B = e.v + V_B;
     const int M = e.order_eff;
     const double h = e.v[V_IRHO], K1b = e.v[V_BK1], K2b = e.v[V_BK2];
@@ -249,14 +274,14 @@ __device__ __forceinline__ void bendmpole(JS<6>& j, const DevElem& e) {
     j.s[PY] = fma(-j.s[Y], psi2, j.s[PY]);
 }
 
-template <int NC>
-__device__ __forceinline__ void drift_len(JS<NC>& j, double L) {
+template <int NC, bool ZD>
+__device__ __forceinline__ void drift_len(JS<NC, ZD>& j, double L) {
     const double inv = 1.0 / (1.0 + j.s[D]);
     drift(j, L * inv, inv);
 }
 
-// Cavity (accel.cpp:903-923)
-__device__ __forceinline__ void cavity(JS<6>& j, const DevElem& e) {
+// Cavity (accel.cpp:903-923): reads z and changes delta, so only with ZD = true
+__device__ __forceinline__ void cavity(JS<6, true>& j, const DevElem& e) {
     const double len = e.v[V_LEN];
     if (len != 0) drift_len(j, 0.5 * len);
     if (e.flags) {

@@ -120,34 +120,22 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_fwd(const AdjParams a, doub
     store6(a.st, a.n, p, r);
 }
 
-// Recompute nt turns from a checkpoint, storing each turn's starting state.
-__global__ void __launch_bounds__(kAdjThreads) k_adj_recompute(const AdjParams a, const double* ck,
-                                                               double* turn_tape, int nt) {
-    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= a.n) return;
-    double r[6];
-    load6(ck, a.n, p, r);
-    for (int j = 0; j < nt; j++) {
-        store6(turn_tape + (int64_t)j * 6 * a.n, a.n, p, r);
-        if (j + 1 < nt && !(r[0] != r[0])) fast_turn(a, r);
-    }
-}
-
-// Recompute every checkpoint segment at once, (segment, particle) per thread: turn_tape holds
-// the starting state of every turn of the run.  The segments are independent given their
-// checkpoints, so this is nseg times wider than recomputing one segment before its reversal.
-__global__ void __launch_bounds__(kAdjThreads) k_adj_recompute_all(const AdjParams a, const double* ckpt,
-                                                                   double* turn_tape, int nturn, int every) {
+// Recompute checkpoint segments seg0 .. seg0+nseg-1 at once, (segment, particle) per thread,
+// storing the starting state of each of their turns at turn_tape[turn - tape_t0].  The segments
+// are independent given their checkpoints, so recomputing all of them in one launch (when their
+// turn starts fit in memory) is nseg times wider than one segment before its reversal.
+__global__ void __launch_bounds__(kAdjThreads) k_adj_recompute(const AdjParams a, const double* ckpt,
+                                                               double* turn_tape, int nturn, int every, int seg0,
+                                                               int nseg, int tape_t0) {
     const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int nseg = (nturn + every - 1) / every;
     if (gid >= (int64_t)nseg * a.n) return;
-    const int seg = (int)(gid / a.n);
-    const int64_t p = gid - (int64_t)seg * a.n;
+    const int seg = seg0 + (int)(gid / a.n);
+    const int64_t p = gid - (int64_t)(seg - seg0) * a.n;
     const int t0 = seg * every, nt = min(every, nturn - t0);
     double r[6];
     load6(ckpt + (int64_t)seg * 6 * a.n, a.n, p, r);
     for (int j = 0; j < nt; j++) {
-        store6(turn_tape + (int64_t)(t0 + j) * 6 * a.n, a.n, p, r);
+        store6(turn_tape + (int64_t)(t0 + j - tape_t0) * 6 * a.n, a.n, p, r);
         if (j + 1 < nt && !(r[0] != r[0])) fast_turn(a, r);
     }
 }
@@ -226,9 +214,11 @@ __device__ __noinline__ jac::JS<6> dual_elem(jac::JS<6> j, const DevElem* __rest
 
 // GENERAL = false: the line holds only the element kinds below and every parameter element is a
 // multipole with one B or A coefficient (the host checks, jtape_needs_general), so no call is
-// made and the kernel keeps the small register budget of the explicit maps.
-template <bool GENERAL>
-__device__ __forceinline__ void jac_elem(jac::JS<6>& j, const DevElem* __restrict__ e) {
+// made and the kernel keeps the small register budget of the explicit maps.  ZD = false: the
+// unit has no element that reads z or changes delta (unit_zd, set by the host), so the cavity
+// case cannot occur in it.
+template <bool GENERAL, bool ZD>
+__device__ __forceinline__ void jac_elem(jac::JS<6, ZD>& j, const DevElem* __restrict__ e) {
     if (jac::lost(j.s)) return;
     switch (e->op) {
     case OP_NOP: return;
@@ -239,7 +229,9 @@ __device__ __forceinline__ void jac_elem(jac::JS<6>& j, const DevElem* __restric
         if (e->flags) break;  // radiation (refused by the adjoint; kept general here)
         jac::bendmpole(j, *e);
         return;
-    case OP_CAVITY: jac::cavity(j, *e); return;
+    case OP_CAVITY:
+        if constexpr (ZD) jac::cavity(j, *e);
+        return;
     case OP_APERTURE:
         if (jac::aperture_hit(j.s, *e)) return;
         if (e->v[V_LEN] != 0) {
@@ -249,7 +241,7 @@ __device__ __forceinline__ void jac_elem(jac::JS<6>& j, const DevElem* __restric
         return;
     default: break;
     }
-    if constexpr (GENERAL) j = dual_elem(j, e);
+    if constexpr (GENERAL && ZD) j = dual_elem(j, e);
 }
 
 // A parameter element outside the explicit path (several parameters, Quad K, ...): dual numbers
@@ -293,37 +285,23 @@ __device__ __noinline__ fast::St param_elem_dual(jac::JS<6> j, const DevElem* __
 // Every turn of the chunk is independent, so this runs nt x n threads wide; the sequential part
 // of the reverse sweep (k_adj_jsweep) is left with 6x6 products and dot products.  A particle lost
 // by the end of the forward run carries no adjoint and is skipped.
-template <bool GENERAL>
-__global__ void __launch_bounds__(128, GENERAL ? 1 : 3) k_adj_jtape(const AdjParams a, const double* turn_tape, int j0, int nt,
-                                                   const double* final_x, int npe, double* jt, double* sens) {
-    const int64_t n = a.n;
-    const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (gid >= n * nt) return;
-    const int t = (int)(gid / n);
-    const int64_t p = gid - (int64_t)t * n;
-    if (final_x[p] != final_x[p]) return;
-    const int64_t ntile = (n + kTile - 1) / kTile, b = p / kTile;
-    const int l = (int)(p % kTile);
-    const double* s0 = turn_tape + (int64_t)(j0 + t) * 6 * n;
-    jac::JS<6> j;
+// One unit: the plain elements [e0, e1), then parameter element pe (or none, pe < 0); stores the
+// unit's Jacobian at J and the parameter sensitivities at S (tiled, stride kTile per entry and
+// pstride per parameter) and advances the state s.
+template <bool GENERAL, bool ZD>
+__device__ __forceinline__ void jtape_unit(const AdjParams& a, double* s, int e0, int e1, int pe,
+                                           double* __restrict__ J, double* __restrict__ S, int64_t pstride) {
+    jac::JS<6, ZD> j;
 #pragma unroll
-    for (int i = 0; i < 6; i++) j.s[i] = s0[i * n + p];
+    for (int i = 0; i < 6; i++) j.s[i] = s[i];
     jac::set_identity(j);
-    int c = 0;
-    for (int e = 0; e < a.ne; e++) {
-        const int np = a.pcount[e];
-        if (np == 0) {
-            jac_elem<GENERAL>(j, a.tbl + e);
-            continue;
-        }
-        const int f = a.pfirst[e];
-        const DevElem* el = a.tbl + e;
-        double* J = jt + ((((int64_t)t * (npe + 1) + c) * ntile + b) * 36) * kTile + l;
-        double* S = sens + ((((int64_t)t * a.nparam + f) * ntile + b) * 6) * kTile + l;
-        const int kind = a.pkind[f];
+    for (int e = e0; e < e1; e++) jac_elem<GENERAL, ZD>(j, a.tbl + e);
+    if (pe >= 0) {
+        const DevElem* el = a.tbl + pe;
+        const int np = a.pcount[pe], f = a.pfirst[pe], kind = a.pkind[f];
         if (np == 1 && (el->op == OP_STRMPOLE || el->op == OP_STRKICK) && (kind == adj::PK_B || kind == adj::PK_A) &&
             !jac::lost(j.s)) {
-            jac::JS<7> q;
+            jac::JS<7, ZD> q;
 #pragma unroll
             for (int i = 0; i < 6; i++) {
                 q.s[i] = j.s[i];
@@ -337,20 +315,55 @@ __global__ void __launch_bounds__(128, GENERAL ? 1 : 3) k_adj_jtape(const AdjPar
 #pragma unroll
                 for (int k = 0; k < 6; k++) J[(6 * i + k) * kTile] = q.m[7 * i + k];
                 S[i * kTile] = q.m[7 * i + 6];
-                j.s[i] = q.s[i];
+                s[i] = q.s[i];
             }
-        } else if constexpr (GENERAL) {
-            const fast::St o = param_elem_dual(j, el, np, a.pkind + f, a.pindex + f, J, S, kTile, ntile * 6 * kTile);
-            j.s[0] = o.x; j.s[1] = o.px; j.s[2] = o.y; j.s[3] = o.py; j.s[4] = o.z; j.s[5] = o.d;
+            return;
         }
-        jac::set_identity(j);
-        c++;
+        if constexpr (GENERAL && ZD) {
+            const fast::St o = param_elem_dual(j, el, np, a.pkind + f, a.pindex + f, J, S, kTile, pstride);
+            s[0] = o.x; s[1] = o.px; s[2] = o.y; s[3] = o.py; s[4] = o.z; s[5] = o.d;
+            return;
+        }
     }
-    double* J = jt + ((((int64_t)t * (npe + 1) + npe) * ntile + b) * 36) * kTile + l;
 #pragma unroll
-    for (int i = 0; i < 6; i++)
+    for (int i = 0; i < 6; i++) {
 #pragma unroll
         for (int k = 0; k < 6; k++) J[(6 * i + k) * kTile] = j.m[6 * i + k];
+        s[i] = j.s[i];
+    }
+}
+
+template <bool GENERAL>
+__global__ void __launch_bounds__(128, GENERAL ? 1 : 3) k_adj_jtape(const AdjParams a, const double* turn_tape, int j0,
+                                                                    int nt, const double* final_x, int npe, double* jt,
+                                                                    double* sens) {
+    const int64_t n = a.n;
+    const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= n * nt) return;
+    const int t = (int)(gid / n);
+    const int64_t p = gid - (int64_t)t * n;
+    if (final_x[p] != final_x[p]) return;
+    const int64_t ntile = (n + kTile - 1) / kTile, b = p / kTile;
+    const int l = (int)(p % kTile);
+    const double* s0 = turn_tape + (int64_t)(j0 + t) * 6 * n;
+    double s[6];
+#pragma unroll
+    for (int i = 0; i < 6; i++) s[i] = s0[i * n + p];
+    const int64_t pstride = ntile * 6 * kTile;
+    int e0 = 0;
+    for (int c = 0; c <= npe; c++) {
+        const int pe = c < npe ? a.pelem[c] : -1;
+        const int e1 = c < npe ? pe : a.ne;
+        double* J = jt + ((((int64_t)t * (npe + 1) + c) * ntile + b) * 36) * kTile + l;
+        double* S = pe >= 0 ? sens + ((((int64_t)t * a.nparam + a.pfirst[pe]) * ntile + b) * 6) * kTile + l : nullptr;
+        if constexpr (GENERAL) {
+            jtape_unit<true, true>(a, s, e0, e1, pe, J, S, pstride);
+        } else {
+            if (a.unit_zd[c]) jtape_unit<false, true>(a, s, e0, e1, pe, J, S, pstride);
+            else jtape_unit<false, false>(a, s, e0, e1, pe, J, S, pstride);
+        }
+        e0 = e1 + 1;
+    }
 }
 
 // Reverse sweep over the chunk's turns, last to first: at each unit's output the parameter
@@ -459,20 +472,33 @@ __global__ void k_adj_reduce(const double* part, int nblk, int nparam, double* o
 void launch_adj_forward(const AdjParams& a, double* ckpt, int nturn, int every, cudaStream_t s) {
     k_adj_fwd<<<adj_blocks(a.n), kAdjThreads, 0, s>>>(a, ckpt, nturn, every);
 }
-void launch_adj_recompute(const AdjParams& a, const double* ck, double* turn_tape, int nt, cudaStream_t s) {
-    k_adj_recompute<<<adj_blocks(a.n), kAdjThreads, 0, s>>>(a, ck, turn_tape, nt);
-}
-void launch_adj_recompute_all(const AdjParams& a, const double* ckpt, double* turn_tape, int nturn, int every,
-                              cudaStream_t s) {
-    const int64_t threads = (int64_t)((nturn + every - 1) / every) * a.n;
-    k_adj_recompute_all<<<(unsigned)((threads + kAdjThreads - 1) / kAdjThreads), kAdjThreads, 0, s>>>(
-        a, ckpt, turn_tape, nturn, every);
+void launch_adj_recompute(const AdjParams& a, const double* ckpt, double* turn_tape, int nturn, int every,
+                          int seg0, int nseg, cudaStream_t s) {
+    const int64_t threads = (int64_t)nseg * a.n;
+    k_adj_recompute<<<(unsigned)((threads + kAdjThreads - 1) / kAdjThreads), kAdjThreads, 0, s>>>(
+        a, ckpt, turn_tape, nturn, every, seg0, nseg, seg0 * every);
 }
 int adj_part_rows(int64_t n) { return (int)std::max<int64_t>((n + kTile - 1) / kTile, adj_blocks(n)); }
 void launch_adj_turn_reverse(const AdjParams& a, const double* r_start, const double* final_x, cudaStream_t s) {
     const size_t sh = sizeof(double) * (kAdjThreads / 32) * (size_t)a.nparam;
     k_adj_turn_reverse<<<adj_blocks(a.n), kAdjThreads, sh, s>>>(a, r_start, final_x);
 }
+void jtape_unit_zd(const DevElem* t, int ne, const int32_t* pelem, int npe, int32_t* unit_zd) {
+    int e0 = 0;
+    for (int c = 0; c <= npe; c++) {
+        const int e1 = c < npe ? pelem[c] : ne - 1;  // inclusive: the parameter element too
+        int zd = 0;
+        for (int e = e0; e <= e1 && e < ne; e++) {
+            const int op = t[e].op;
+            const bool plain = op == OP_NOP || op == OP_DRIFT || op == OP_STRMPOLE || op == OP_STRKICK ||
+                               op == OP_APERTURE || (op == OP_BENDMPOLE && t[e].flags == 0);
+            if (!plain) zd = 1;
+        }
+        unit_zd[c] = zd;
+        e0 = e1 + 1;
+    }
+}
+
 bool jtape_needs_general(const DevElem* t, int ne, const int32_t* pcount, const int32_t* pfirst,
                          const int32_t* pkind) {
     for (int e = 0; e < ne; e++) {

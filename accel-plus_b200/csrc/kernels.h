@@ -86,10 +86,14 @@ struct AdjParams {
     const int32_t* pkind;   // [nparam] adj::ParamKind
     const int32_t* pindex;  // [nparam] multipole index
     int nparam;
+    const int32_t* pelem;   // [npe] the parameter elements in line order
+    const int32_t* unit_zd; // [npe + 1] 1 where a tape unit has an element that reads z or changes delta
 };
 int adj_blocks(int64_t n);
 void launch_adj_forward(const AdjParams& a, double* ckpt, int nturn, int every, cudaStream_t s);
-void launch_adj_recompute(const AdjParams& a, const double* ck, double* turn_tape, int nt, cudaStream_t s);
+// turn-start states of checkpoint segments seg0 .. seg0+nseg-1 into turn_tape, from turn seg0 * every on
+void launch_adj_recompute(const AdjParams& a, const double* ckpt, double* turn_tape, int nturn, int every,
+                          int seg0, int nseg, cudaStream_t s);
 void launch_adj_turn_reverse(const AdjParams& a, const double* r_start, const double* final_x, cudaStream_t s);
 void launch_adj_reduce(const double* part, int nblk, int nparam, double* out, cudaStream_t s);
 // block-Jacobian tape of nt turns (unit Jacobians and parameter sensitivities) and the reverse
@@ -100,13 +104,13 @@ void launch_adj_jtape(const AdjParams& a, const double* turn_tape, int j0, int n
                       int npe, double* jt, double* sens, bool general, cudaStream_t s);
 bool jtape_needs_general(const DevElem* host_tbl, int ne, const int32_t* pcount, const int32_t* pfirst,
                          const int32_t* pkind);
+// per tape unit (npe + 1 of them): 1 if any of its elements is not a drift, straight multipole,
+// radiation-free bend, aperture or marker
+void jtape_unit_zd(const DevElem* host_tbl, int ne, const int32_t* pelem, int npe, int32_t* unit_zd);
 // grow: per-lane gradient rows in global memory, ntile x nparam x 32 doubles, used only past
 // 384 parameters (null otherwise)
 void launch_adj_jsweep(const AdjParams& a, int nt, const double* final_x, int npe, const int32_t* pelem,
                        const double* jt, const double* sens, double* grow, cudaStream_t s);
-// every segment recomputed in one launch: turn_tape holds all nturn turn-start states
-void launch_adj_recompute_all(const AdjParams& a, const double* ckpt, double* turn_tape, int nturn, int every,
-                              cudaStream_t s);
 // rows of the per-block gradient partials (covers both the sweep's tiles and the reverse kernel's blocks)
 int adj_part_rows(int64_t n);
 // doubles of the tiled tapes per turn and unit (ceil(n / 32) * 32 particles)
