@@ -44,7 +44,7 @@ def richardson(f, h):
     return (4 * d2 - d1) / 3
 
 
-def converged_difference(f, steps=(1e-2, 1e-3, 1e-4, 1e-5, 3e-6)):
+def converged_difference(f, steps=(1e-2, 1e-3, 1e-4, 3e-5, 1e-5, 3e-6)):
     """The first Richardson estimate that agrees with the one at a third of its step to 3e-7
     relative (a fifth of the test's tolerance): large steps are truncation-limited where the multi-turn map is tune-sensitive
     (quadrupoles), tiny ones round-off-limited where the gradient is a small sum of cancelling
@@ -56,17 +56,53 @@ def converged_difference(f, steps=(1e-2, 1e-3, 1e-4, 1e-5, 3e-6)):
     raise AssertionError(f"finite differences did not converge: {a} vs {b}")
 
 
-@pytest.mark.parametrize("ringname", ["fodo", "dba4d"])
-def test_adjoint_against_finite_differences(A, ctx, O, LT, ringname):
+def ring_and_params(A, LT, ringname):
+    """The test rings: the FODO and the 4D DBA with two parameters on one element (the tape's
+    dual-number path), the DBA with its cavity on and radiation off (synchrotron motion: the
+    explicit tape's units that read z and change delta), the 4D DBA with one parameter per
+    element (the explicit tape alone), and a FODO whose quadrupoles are thick linear Quad
+    elements with a corrector and a matrix (element kinds the tape takes on dual numbers, and a
+    Quad K parameter)."""
     if ringname == "fodo":
-        ring = LT.config1_ring()
-        nturn, every = 24, 8
-    else:
-        ring = LT.config4_ring()
-        nturn, every = 40, 16  # 40 = 2 x 16 + 8: a short last segment
+        ring, nturn, every = LT.config1_ring(), 24, 8
+    elif ringname == "dba4d":
+        ring, nturn, every = LT.config4_ring(), 40, 16  # 40 = 2 x 16 + 8: a short last segment
+    elif ringname == "dba6d":
+        ring, nturn, every = LT.config2_ring(), 40, 16
+        for d in ring:
+            if d.type == A.BENDMPOLE:
+                d.flags = A.RAD_OFF
+            if d.type == A.CAVITY:
+                d.f[2] = 0.0  # without radiation the synchronous phase is 0
+    elif ringname == "dba4d_single":
+        ring, nturn, every = LT.config4_ring(), 40, 16
+    else:  # "fodo_quad"
+        ring, nturn, every = [], 24, 8
+        for d in LT.config1_ring():
+            if d.type == A.STRMPOLE and d.poly_b[2] == 0 and d.poly_b[1] != 0 and d.len > 0:
+                ring.append(A.elem(A.QUAD, d.name, d.len, f=[d.poly_b[1]]))
+            else:
+                ring.append(d)
+        ring.insert(3, A.elem(A.CORRECTOR, "C", 0.1, f=[2e-5, -1e-5]))
+        m = np.eye(6)
+        m[0, 1], m[2, 3] = 0.05, 0.05  # a short drift in x and y
+        ring.insert(7, A.elem(A.MATRIX, "M", 0.0, mat=m.ravel()))
     sx = [i for i, d in enumerate(ring) if d.type == A.STRMPOLE and d.poly_b[2] != 0][:3]
-    qx = [i for i, d in enumerate(ring) if d.type == A.STRMPOLE and d.poly_b[2] == 0 and d.poly_b[1] != 0][:2]
-    params = [(i, A.F_POLYNOMB, 2) for i in sx] + [(i, A.F_POLYNOMB, 1) for i in qx] + [(sx[0], A.F_POLYNOMA, 1)]
+    if ringname == "fodo_quad":
+        qx = [i for i, d in enumerate(ring) if d.type == A.QUAD][:2]
+        params = [(i, A.F_POLYNOMB, 2) for i in sx] + [(i, A.F_K, 0) for i in qx]
+    elif ringname == "dba4d_single":
+        qx = [i for i, d in enumerate(ring) if d.type == A.STRMPOLE and d.poly_b[2] == 0 and d.poly_b[1] != 0][:2]
+        params = [(i, A.F_POLYNOMB, 2) for i in sx] + [(i, A.F_POLYNOMB, 1) for i in qx]
+    else:
+        qx = [i for i, d in enumerate(ring) if d.type == A.STRMPOLE and d.poly_b[2] == 0 and d.poly_b[1] != 0][:2]
+        params = [(i, A.F_POLYNOMB, 2) for i in sx] + [(i, A.F_POLYNOMB, 1) for i in qx] + [(sx[0], A.F_POLYNOMA, 1)]
+    return ring, nturn, every, params
+
+
+@pytest.mark.parametrize("ringname", ["fodo", "dba4d", "dba6d", "dba4d_single", "fodo_quad"])
+def test_adjoint_against_finite_differences(A, ctx, O, LT, ringname):
+    ring, nturn, every, params = ring_and_params(A, LT, ringname)
     n = 32
     r0 = small_particles(n)
     line = A.Line(ctx, ring)
@@ -92,7 +128,7 @@ def test_adjoint_against_finite_differences(A, ctx, O, LT, ringname):
     for j, (e, fld, idx) in enumerate(params):
         def f(dv, e=e, fld=fld, idx=idx):
             rr = [d.copy() for d in ring]
-            arr = rr[e].poly_b if fld == A.F_POLYNOMB else rr[e].poly_a
+            arr = rr[e].f if fld == A.F_K else (rr[e].poly_b if fld == A.F_POLYNOMB else rr[e].poly_a)
             arr[idx] += dv
             return loss_of(O, rr, r0, nturn)
         fd = converged_difference(f)
