@@ -122,6 +122,8 @@ def lib() -> C.CDLL:
         "accel_beam_stat_noalloc": (I, [P, I, C.c_int64, P, P]),
         "accel_naff": (I, [P, I, D, D, C.POINTER(D)]),
         "accel_fp64_peak": (I, [P, C.POINTER(D)]),
+        "accel_set_device_memory_limit": (I, [C.c_int64]),
+        "accel_device_memory_held": (I, [C.POINTER(C.c_int64)]),
         "accel_launch_count": (I, [P, C.POINTER(C.c_int64)]),
         "accel_profile_enable": (I, [P, I]),
         "accel_profile_read": (I, [P, C.POINTER(D), C.POINTER(C.c_int64), C.POINTER(D)]),
@@ -196,6 +198,20 @@ def elem(type_: int, famname: str = "undefined", length: float = 0.0, **kw) -> E
     if type_ in (BEND, BENDMPOLE) and length != 0:
         d.f[4] = d.f[0] / length
     return d
+
+
+def set_device_memory_limit(nbytes: int | None) -> None:
+    """Cap the device memory this process's library holds (None or a negative value: no cap);
+    a request beyond it fails with E_NOMEM before any allocation (accel_set_device_memory_limit)."""
+    _check(lib().accel_set_device_memory_limit(-1 if nbytes is None else int(nbytes)),
+           "accel_set_device_memory_limit")
+
+
+def device_memory_held() -> int:
+    """Bytes of device memory the library's buffers hold, all devices together."""
+    v = C.c_int64()
+    _check(lib().accel_device_memory_held(C.byref(v)), "accel_device_memory_held")
+    return v.value
 
 
 def wigtable(xl, yl, xkick, ykick) -> int:

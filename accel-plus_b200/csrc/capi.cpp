@@ -49,22 +49,45 @@ int fail(int status, const std::string& msg) {
 // ------------------------------------------------------------------------------------------
 // device buffers
 // ------------------------------------------------------------------------------------------
+// bytes of device memory held in DevBufs, and the budget (accel_set_device_memory_limit)
+static std::atomic<int64_t> g_held{0};
+static std::atomic<int64_t> g_limit{-1};
+
 int DevBuf::ensure(size_t nbytes) {
     if (nbytes <= bytes && p) return ACCEL_OK;
-    if (p) { cudaFree(p); p = nullptr; bytes = 0; }
     size_t want = std::max<size_t>(nbytes, 256);
+    const int64_t limit = g_limit.load();
+    if (limit >= 0 && g_held.load() - (int64_t)bytes + (int64_t)want > limit)
+        return fail(ACCEL_E_NOMEM, "a device buffer of " + std::to_string(want) + " bytes would take the library's " +
+                                       "device memory above its limit of " + std::to_string(limit) + " bytes");
+    release();
     cudaError_t e = cudaMalloc(&p, want);
     if (e != cudaSuccess) {
         p = nullptr;
         return fail(ACCEL_E_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
     }
     bytes = want;
+    g_held += (int64_t)want;
     return ACCEL_OK;
 }
 void DevBuf::release() {
-    if (p) cudaFree(p);
+    if (p) {
+        cudaFree(p);
+        g_held -= (int64_t)bytes;
+    }
     p = nullptr;
     bytes = 0;
+}
+
+extern "C" int accel_set_device_memory_limit(int64_t bytes) {
+    g_limit = bytes < 0 ? -1 : bytes;
+    return ACCEL_OK;
+}
+
+extern "C" int accel_device_memory_held(int64_t* bytes) {
+    if (!bytes) return fail(ACCEL_E_INVALID, "NULL argument");
+    *bytes = g_held.load();
+    return ACCEL_OK;
 }
 
 static bool is_device_ptr(const void* p) {

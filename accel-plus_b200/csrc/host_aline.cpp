@@ -478,13 +478,15 @@ double ALine::trackMA(double dppmax, double dppmin, int nturn, unsigned nstep, d
         }
     }
     double avg = 0;
-    double* d_soa = nullptr;
-    if (!status_ && cudaMalloc(&d_soa, soa.size() * sizeof(double)) == cudaSuccess) {
-        cudaMemcpy(d_soa, soa.data(), soa.size() * sizeof(double), cudaMemcpyHostToDevice);
-        status_ = accel_track_batched(lines.data(), (int)nfam, off.data(), d_soa, ntot, nturn, nullptr, mode, nullptr);
+    accel::DevBuf d_soa;  // counted against the library's device-memory limit
+    int ast = status_ ? status_ : d_soa.ensure(soa.size() * sizeof(double));
+    if (!status_ && !ast) {
+        cudaMemcpy(d_soa.p, soa.data(), soa.size() * sizeof(double), cudaMemcpyHostToDevice);
+        status_ = accel_track_batched(lines.data(), (int)nfam, off.data(), (double*)d_soa.p, ntot, nturn, nullptr, mode,
+                                      nullptr);
         cudaDeviceSynchronize();
-        cudaMemcpy(soa.data(), d_soa, sizeof(double) * (size_t)ntot, cudaMemcpyDeviceToHost);  // x row
-        cudaFree(d_soa);
+        cudaMemcpy(soa.data(), d_soa.p, sizeof(double) * (size_t)ntot, cudaMemcpyDeviceToHost);  // x row
+        d_soa.release();
         for (unsigned i = 0; i < nfam; i++) {
             dpp_plus[i] = dppmin;
             dpp_minus[i] = -dppmin;
@@ -496,7 +498,7 @@ double ALine::trackMA(double dppmax, double dppmin, int nturn, unsigned nstep, d
         }
         avg /= nfam;
     } else if (!status_) {
-        status_ = ACCEL_E_NOMEM;
+        status_ = ast;
     }
     for (accel_line* l : lines)
         if (l) accel_line_destroy(l);

@@ -298,6 +298,16 @@ int  accel_naff(const double* data, int n, double xlow, double xhi, double* nu);
 /* Device FP64 FMA throughput micro-benchmark (TFLOP/s, FMA = 2 flops). */
 int  accel_fp64_peak(accel_ctx* ctx, double* tflops);
 
+/* Device-memory budget of this process's library (no counterpart in the reference, which tracks
+ * in host memory).  Every device buffer the library keeps (particle state, element tables,
+ * tapes, scratch) is counted; a request that would take the total above the limit fails with
+ * ACCEL_E_NOMEM before any cudaMalloc, and the call that needed it returns that status with
+ * nothing tracked.  For a GPU shared with other work, and to exercise out-of-memory handling.
+ * bytes < 0: no limit (the default).  The limit applies to all devices together and to later
+ * requests only; buffers already held stay. */
+int  accel_set_device_memory_limit(int64_t bytes);
+int  accel_device_memory_held(int64_t* bytes);
+
 /* Number of this library's kernels launched since the context was created. */
 int  accel_launch_count(accel_ctx* ctx, int64_t* count);
 

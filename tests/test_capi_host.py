@@ -145,6 +145,16 @@ def test_reader_agrees_with_reference_deserialize(A, O, LT):
             assert ref.get_field(i, "Phis") == d.f[2]
 
 
+def test_device_memory_limit_without_a_device(A):
+    """The budget is host state: it can be set and read with no device (nothing is held)."""
+    assert A.device_memory_held() >= 0
+    A.set_device_memory_limit(1 << 20)
+    A.set_device_memory_limit(None)
+    with pytest.raises(A.AccelError) as ei:
+        A._check(A.lib().accel_device_memory_held(None), "accel_device_memory_held")
+    assert ei.value.status == A.E_INVALID
+
+
 def test_no_device_is_an_error_not_a_fallback(A):
     if A.device_count() > 0:
         pytest.skip("a device is present")

@@ -220,6 +220,36 @@ def test_errors_are_statuses(A, ctx):
     assert ei.value.status == A.E_INVALID
 
 
+def test_device_memory_limit_fails_cleanly(A, LT):
+    """Out of memory, simulated by the library's device-memory budget: tracking on a new context
+    needs new buffers, the budget refuses them, the call returns E_NOMEM with the particles
+    untouched, and with the budget lifted the same call tracks exactly as an unconstrained one."""
+    rng = np.random.default_rng(3)
+    r0 = np.zeros((3000, 6))
+    r0[:, 0] = rng.uniform(-2e-3, 2e-3, 3000)
+    r0[:, 2] = rng.uniform(-1e-3, 1e-3, 3000)
+    ref = r0.copy()
+    A.Line(A.Context(0), LT.config1_ring()).track(ref, 20)
+    c2 = A.Context(0)
+    line = A.Line(c2, LT.config1_ring())
+    held = A.device_memory_held()
+    try:
+        A.set_device_memory_limit(held)  # no new buffer fits
+        r = r0.copy()
+        with pytest.raises(A.AccelError) as ei:
+            line.track(r, 20)
+        assert ei.value.status == A.E_NOMEM and "limit" in str(ei.value)
+        assert np.array_equal(r, r0)
+        assert A.device_memory_held() == held
+    finally:
+        A.set_device_memory_limit(None)
+    r = r0.copy()
+    line.track(r, 20)
+    assert np.array_equal(np.isnan(r[:, 0]), np.isnan(ref[:, 0]))
+    assert rel_err(r, ref) < 1e-13
+    assert A.device_memory_held() > held
+
+
 def test_autotune_and_launch_count(A, ctx, LT):
     import torch
     base = LT.config2_ring()
