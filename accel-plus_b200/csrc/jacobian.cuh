@@ -185,14 +185,15 @@ __device__ __forceinline__ void strmpole(JS<NC, ZD>& j, const DevElem& e, int pk
     if (e.op == OP_STRKICK) { kick(j, A, B, M, 1.0, pkind, pn); return; }
     const double inv = 1.0 / (1.0 + j.s[D]);
     const double N1 = e.v[V_L1] * inv, N2 = e.v[V_L2] * inv, K1 = e.v[V_K1], K2 = e.v[V_K2];
+    // one copy of the drift and of the kick in the code, stepped through the slice's sequence
+    // D1 K1 D2 K2 D2 K1 D1 (the tape kernel is large enough for instruction fetch to stall it)
+#pragma unroll 1
     for (int m = 0; m < e.nslice; m++) {
-        drift(j, N1, inv);
-        kick(j, A, B, M, K1, pkind, pn);
-        drift(j, N2, inv);
-        kick(j, A, B, M, K2, pkind, pn);
-        drift(j, N2, inv);
-        kick(j, A, B, M, K1, pkind, pn);
-        drift(j, N1, inv);
+#pragma unroll 1
+        for (int k = 0; k < 4; k++) {
+            drift(j, (k == 0 || k == 3) ? N1 : N2, inv);
+            if (k < 3) kick(j, A, B, M, k == 1 ? K2 : K1, pkind, pn);
+        }
     }
 }
 
@@ -259,14 +260,13 @@ __device__ __forceinline__ void bendmpole(JS<6, ZD>& j, const DevElem& e) {
     j.s[PX] = fma(j.s[X], psi1, j.s[PX]);
     j.s[PY] = fma(-j.s[Y], psi1, j.s[PY]);
     const double inv = 1.0 / (1.0 + j.s[D]);
+#pragma unroll 1
     for (int m = 0; m < e.nslice; m++) {
-        hxdrift(j, L1, h, inv);
-        bend_kick(j, B, M, h, K1b, K2b, K1);
-        hxdrift(j, L2, h, inv);
-        bend_kick(j, B, M, h, K1b, K2b, K2);
-        hxdrift(j, L2, h, inv);
-        bend_kick(j, B, M, h, K1b, K2b, K1);
-        hxdrift(j, L1, h, inv);
+#pragma unroll 1
+        for (int k = 0; k < 4; k++) {
+            hxdrift(j, (k == 0 || k == 3) ? L1 : L2, h, inv);
+            if (k < 3) bend_kick(j, B, M, h, K1b, K2b, k == 1 ? K2 : K1);
+        }
     }
     axpy(j, PX, X, psi2);
     axpy(j, PY, Y, -psi2);
