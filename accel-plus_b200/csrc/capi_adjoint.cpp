@@ -61,7 +61,7 @@ struct accel_adjoint {
     int npe = 0;
     int chunk = 0;               // turns per block-Jacobian tape; 0: per-turn element reversal
     bool general = true;         // the tape needs the dual-number fallback (jtape_needs_general)
-    bool all_turns = false;      // turn_tape holds every turn of the run (one recompute launch)
+    bool all_turns = false;      // turn_tape holds every turn of the run, written by the forward
     DevBuf st, lam, aos, tape, ckpt, turn_tape, part, meta, final_x, grad, jt, rt, pel, grow, uzd;
     bool have_forward = false;
     ~accel_adjoint() {
@@ -177,9 +177,9 @@ int accel_adjoint_create(accel_line* L, int N, int nturn, int every, const int32
         if (J->pcount[(size_t)e] > 0) J->pelem.push_back(e);
     J->npe = (int)J->pelem.size();
     J->general = jtape_needs_general(L->host_tbl.data(), ne, J->pcount.data(), J->pfirst.data(), J->pkind.data());
-    // every turn-start state kept when that fits the tape budget: the segments are then
-    // recomputed together in one launch instead of one narrow launch each
-    J->all_turns = J->nseg > 1 && (double)s6 * nturn <= kTapeBudgetBytes;
+    // every turn-start state kept by the forward when that fits the tape budget: the reverse
+    // pass then recomputes nothing (otherwise each segment is recomputed from its checkpoint)
+    J->all_turns = (double)s6 * nturn <= kTapeBudgetBytes;
     const size_t span = (size_t)adj_tile_span(N);  // tiled tapes: 32-particle tiles
     const double per_turn = 8.0 * (double)span * (36.0 * (J->npe + 1) + 6.0 * nparam);
     J->chunk = (int)std::min<double>(std::min(every, nturn), std::floor(kTapeBudgetBytes / per_turn));
@@ -248,7 +248,8 @@ int accel_adjoint_forward(accel_adjoint* J, const double* r0, double* r_final) {
     }
     launch_aos_to_soa(in, (double*)J->st.p, J->n, s);
     AdjParams a = params_of(J);
-    launch_adj_forward(a, (double*)J->ckpt.p, J->nturn, J->every, s);
+    launch_adj_forward(a, (double*)J->ckpt.p, J->nturn, J->every, J->all_turns ? (double*)J->turn_tape.p : nullptr,
+                       s);
     CK(cudaMemcpyAsync(J->final_x.p, J->st.p, sizeof(double) * (size_t)J->n, cudaMemcpyDeviceToDevice, s));
     launch_soa_to_aos((const double*)J->st.p, (double*)J->aos.p, J->n, s);
     C->launches += 3;
@@ -278,11 +279,7 @@ int accel_adjoint_backward(accel_adjoint* J, const double* g, double* dr0, doubl
     if (J->nparam > 0) CK(cudaMemsetAsync(J->part.p, 0, sizeof(double) * (size_t)nblk * J->nparam, s));
     AdjParams a = params_of(J);
     int64_t launches = 1;
-    if (J->all_turns) {
-        launch_adj_recompute(a, (const double*)J->ckpt.p, (double*)J->turn_tape.p, J->nturn, J->every, 0, J->nseg,
-                             s);
-        launches++;
-    }
+    // with all_turns the forward kept every turn's starting state: nothing to recompute
     for (int seg = J->nseg - 1; seg >= 0; seg--) {
         const int t0 = seg * J->every;
         const int nt = std::min(J->every, J->nturn - t0);

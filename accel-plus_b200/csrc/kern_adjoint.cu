@@ -107,14 +107,18 @@ __device__ __forceinline__ void store6(double* s, int64_t n, int64_t p, const do
     for (int k = 0; k < 6; k++) s[k * n + p] = r[k];
 }
 
-// Forward: nturn turns from st, checkpoint every `every` turns; st ends at the final state.
-__global__ void __launch_bounds__(kAdjThreads) k_adj_fwd(const AdjParams a, double* ckpt, int nturn, int every) {
+// Forward: nturn turns from st, checkpoint every `every` turns; st ends at the final state.  With
+// turn_tape (the run's turn starts fit the tape budget) every turn's starting state is kept too,
+// so the reverse pass needs no recomputation; the states are the ones recomputing would give.
+__global__ void __launch_bounds__(kAdjThreads) k_adj_fwd(const AdjParams a, double* ckpt, int nturn, int every,
+                                                         double* turn_tape) {
     const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= a.n) return;
     double r[6];
     load6(a.st, a.n, p, r);
     for (int t = 0; t < nturn; t++) {
         if (t % every == 0) store6(ckpt + (int64_t)(t / every) * 6 * a.n, a.n, p, r);
+        if (turn_tape) store6(turn_tape + (int64_t)t * 6 * a.n, a.n, p, r);
         if (!(r[0] != r[0])) fast_turn(a, r);
     }
     store6(a.st, a.n, p, r);
@@ -469,8 +473,9 @@ __global__ void k_adj_reduce(const double* part, int nblk, int nparam, double* o
     }
 }
 
-void launch_adj_forward(const AdjParams& a, double* ckpt, int nturn, int every, cudaStream_t s) {
-    k_adj_fwd<<<adj_blocks(a.n), kAdjThreads, 0, s>>>(a, ckpt, nturn, every);
+void launch_adj_forward(const AdjParams& a, double* ckpt, int nturn, int every, double* turn_tape,
+                        cudaStream_t s) {
+    k_adj_fwd<<<adj_blocks(a.n), kAdjThreads, 0, s>>>(a, ckpt, nturn, every, turn_tape);
 }
 void launch_adj_recompute(const AdjParams& a, const double* ckpt, double* turn_tape, int nturn, int every,
                           int seg0, int nseg, cudaStream_t s) {

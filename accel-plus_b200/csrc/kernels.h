@@ -90,7 +90,9 @@ struct AdjParams {
     const int32_t* unit_zd; // [npe + 1] 1 where a tape unit has an element that reads z or changes delta
 };
 int adj_blocks(int64_t n);
-void launch_adj_forward(const AdjParams& a, double* ckpt, int nturn, int every, cudaStream_t s);
+// turn_tape: null, or room for every turn's starting state (nturn x 6 x n doubles)
+void launch_adj_forward(const AdjParams& a, double* ckpt, int nturn, int every, double* turn_tape,
+                        cudaStream_t s);
 // turn-start states of checkpoint segments seg0 .. seg0+nseg-1 into turn_tape, from turn seg0 * every on
 void launch_adj_recompute(const AdjParams& a, const double* ckpt, double* turn_tape, int nturn, int every,
                           int seg0, int nseg, cudaStream_t s);
