@@ -123,6 +123,7 @@ def lib() -> C.CDLL:
         "accel_naff": (I, [P, I, D, D, C.POINTER(D)]),
         "accel_fp64_peak": (I, [P, C.POINTER(D)]),
         "accel_set_device_memory_limit": (I, [C.c_int64]),
+        "accel_set_adjoint_tape_budget": (I, [C.c_int64]),
         "accel_device_memory_held": (I, [C.POINTER(C.c_int64)]),
         "accel_launch_count": (I, [P, C.POINTER(C.c_int64)]),
         "accel_profile_enable": (I, [P, I]),
@@ -205,6 +206,13 @@ def set_device_memory_limit(nbytes: int | None) -> None:
     a request beyond it fails with E_NOMEM before any allocation (accel_set_device_memory_limit)."""
     _check(lib().accel_set_device_memory_limit(-1 if nbytes is None else int(nbytes)),
            "accel_set_device_memory_limit")
+
+
+def set_adjoint_tape_budget(nbytes: int | None) -> None:
+    """Device memory each tape of an adjoint created afterwards may take (None or <= 0: the
+    default, 4e9 bytes); accel_set_adjoint_tape_budget."""
+    _check(lib().accel_set_adjoint_tape_budget(0 if nbytes is None else int(nbytes)),
+           "accel_set_adjoint_tape_budget")
 
 
 def device_memory_held() -> int:

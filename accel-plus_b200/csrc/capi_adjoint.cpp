@@ -17,6 +17,7 @@
 // wake elements (their maps are not differentiated): ACCEL_E_UNSUPPORTED otherwise.
 #include <cuda_runtime.h>
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -40,7 +41,8 @@ using namespace accel;
 
 namespace {
 constexpr int kMaxAdjParams = 2048;
-constexpr double kTapeBudgetBytes = 4.0e9;  // block-Jacobian tape of one chunk of turns
+constexpr double kTapeBudgetDefault = 4.0e9;  // each tape: the turn starts; one chunk of Jacobians
+std::atomic<double> g_tape_budget{kTapeBudgetDefault};  // accel_set_adjoint_tape_budget
 
 bool dev_ptr(const void* p) {
     cudaPointerAttributes a;
@@ -92,6 +94,11 @@ static AdjParams params_of(accel_adjoint* J) {
 }
 
 extern "C" {
+
+int accel_set_adjoint_tape_budget(int64_t bytes) {
+    g_tape_budget = bytes <= 0 ? kTapeBudgetDefault : (double)bytes;
+    return ACCEL_OK;
+}
 
 int accel_adjoint_create(accel_line* L, int N, int nturn, int every, const int32_t* pe,
                          const int32_t* pf, const int32_t* pi, int nparam, accel_adjoint** out) {
@@ -179,10 +186,11 @@ int accel_adjoint_create(accel_line* L, int N, int nturn, int every, const int32
     J->general = jtape_needs_general(L->host_tbl.data(), ne, J->pcount.data(), J->pfirst.data(), J->pkind.data());
     // every turn-start state kept by the forward when that fits the tape budget: the reverse
     // pass then recomputes nothing (otherwise each segment is recomputed from its checkpoint)
-    J->all_turns = (double)s6 * nturn <= kTapeBudgetBytes;
+    const double budget = g_tape_budget.load();
+    J->all_turns = (double)s6 * nturn <= budget;
     const size_t span = (size_t)adj_tile_span(N);  // tiled tapes: 32-particle tiles
     const double per_turn = 8.0 * (double)span * (36.0 * (J->npe + 1) + 6.0 * nparam);
-    J->chunk = (int)std::min<double>(std::min(every, nturn), std::floor(kTapeBudgetBytes / per_turn));
+    J->chunk = (int)std::min<double>(std::min(every, nturn), std::floor(budget / per_turn));
     if (J->chunk >= 1) {
         const size_t c = (size_t)J->chunk, nn = span;
         if ((s = J->jt.ensure(sizeof(double) * c * (size_t)(J->npe + 1) * 36 * nn)) ||

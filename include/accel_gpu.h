@@ -256,7 +256,11 @@ int  accel_m66_at(accel_line* line, int st, int ed, const double* r0, int method
  * accel_adjoint_forward tracks r0 (host or device, AoS, N particles) for nturn turns, keeping a
  * checkpoint of the state every `ckpt_every` turns on the device, and writes r_final.
  * accel_adjoint_backward takes dL/dr_final (AoS, 6N) and returns dL/dr0 (AoS, 6N) and
- * dL/dparams (nparam), recomputing each segment from its checkpoint.
+ * dL/dparams (nparam).  The reverse pass needs every turn's starting state: the forward keeps
+ * them all when they fit the tape budget, else each segment is recomputed from its checkpoint.
+ * It then tapes the Jacobians of a chunk of turns at once, as many as fit the budget, or, when not
+ * even one turn fits, reverses turn by turn.  The three ways give the same gradient (the last to
+ * round-off).
  */
 typedef struct accel_adjoint accel_adjoint;  /* holds its line (and context) until destroyed */
 int  accel_adjoint_create(accel_line* line, int N, int nturn, int ckpt_every,
@@ -266,6 +270,10 @@ int  accel_adjoint_destroy(accel_adjoint* adj);
 int  accel_adjoint_forward(accel_adjoint* adj, const double* r0, double* r_final);
 int  accel_adjoint_backward(accel_adjoint* adj, const double* dl_drfinal, double* dl_dr0,
                             double* dl_dparams);
+/* Device memory an adjoint created afterwards may give to each of its tapes (the turn starts,
+ * and one chunk of Jacobians); bytes <= 0 restores the default of 4e9.  A smaller budget trades
+ * speed for memory.  No counterpart in the reference (which has no reverse mode). */
+int  accel_set_adjoint_tape_budget(int64_t bytes);
 
 /* Beam moments of live particles (calc_beam_stat, utility.cpp:387-438): mean[6], sigma[6],
  * cross[6] = <xx'>,<yy'>,<x d>,<x' d>,<y z>,<y' z>; returns the live count in *nlive.       */

@@ -135,6 +135,40 @@ def test_adjoint_against_finite_differences(A, ctx, O, LT, ringname):
         assert abs(dp[j] - fd) <= 1e-6 * max(abs(fd), 1e-9), (j, dp[j], fd)
 
 
+def test_tape_budget_paths_agree(A, ctx, LT):
+    """The three ways of the reverse pass give one gradient: every turn start kept by the forward
+    (the default here); checkpoint segments recomputed, with Jacobian tapes one turn at a time (a
+    budget below the run's turn starts but above one turn's Jacobians); and the turn-by-turn
+    reversal (a budget below one turn's Jacobians).  The first two take the same arithmetic for
+    the coordinates (bit-identical dL/dr0) and group the parameter sums by chunk (round-off), the
+    third another order of the arithmetic."""
+    ring, _, _, params = ring_and_params(A, LT, "dba4d_single")  # five one-parameter elements
+    nturn, every, n = 64, 16, 32
+    r0 = small_particles(n)
+    turn_starts = 48 * n * nturn                                # 98,304 bytes
+    per_turn = 8 * 32 * (36 * (len(params) + 1) + 6 * len(params))  # 62,976 bytes
+    assert per_turn < 80000 < turn_starts and 30000 < per_turn
+
+    def grad(budget):
+        A.set_adjoint_tape_budget(budget)
+        try:
+            adj = A.Adjoint(A.Line(ctx, ring), n, nturn, every, params)
+            rf = adj.forward(r0)
+            return adj.backward(grad_final(rf))
+        finally:
+            A.set_adjoint_tape_budget(None)
+
+    d0, p0 = grad(None)
+    d1, p1 = grad(80000)
+    d2, p2 = grad(30000)
+    assert np.array_equal(d1, d0)
+    assert np.max(np.abs(p1 - p0)) < 1e-13 * np.max(np.abs(p0))
+    # the turn-by-turn reversal rounds in another order; over 64 turns the map's growth makes
+    # that a few 1e-10 of the largest component
+    assert np.max(np.abs(d2 - d0)) < 1e-8 * np.max(np.abs(d0))
+    assert np.max(np.abs(p2 - p0)) < 1e-8 * np.max(np.abs(p0))
+
+
 def test_adjoint_one_turn_jacobian_is_exact(A, ctx, LT):
     """Six particles at the closed orbit (the origin of the 4D ring), seeded with unit adjoints:
     row i of the one-turn matrix is dL/dr0 of particle i for L = r_final[i]."""
