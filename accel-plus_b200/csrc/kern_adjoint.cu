@@ -405,29 +405,36 @@ __global__ void __launch_bounds__(kTile) k_adj_jsweep(const AdjParams a, int nt,
     const bool alive = p < n && !(final_x[p] != final_x[p]);
     double lam[6] = {0, 0, 0, 0, 0, 0};
     if (alive) load6(a.lam, n, p, lam);
-    const int U = nt * (npe + 1);  // units of the chunk; unit u = t * (npe + 1) + c
-    // issue unit u into stage slot st: its J tile and, for a parameter unit, its sens tiles
-    auto issue = [&](int u, int st) {
-        if (u >= 0) {
-            const int t = u / (npe + 1), c = u - t * (npe + 1);
-            double* dst = stage + st * kStageDoubles;
-            const double* src = jt + (((int64_t)u * ntile + b) * 36) * kTile;
-            for (int k = lane; k < 36 * kTile / 2; k += kTile) cp_async16(dst + 2 * k, src + 2 * k);
-            if (c < npe) {
-                const int e = pelem[c], np = a.pcount[e], f = a.pfirst[e];
+    const int U = nt * (npe + 1);  // units of the chunk; unit u = t * (npe + 1) + c, swept u = U-1 .. 0
+    const int64_t jstride = ntile * 36 * kTile;           // doubles between consecutive units' tiles
+    const int64_t sstride = ntile * 6 * kTile;            // between consecutive parameters' tiles
+    // the copy cursor runs kSweepStages units ahead of the sweep; (t, c) counters, no division
+    int it = nt - 1, ic = npe, ist = 0, iu = U - 1;
+    auto issue = [&]() {
+        if (iu >= 0) {
+            double* dst = stage + ist * kStageDoubles;
+            const double* src = jt + (int64_t)iu * jstride + b * 36 * kTile;
+#pragma unroll
+            for (int k = 0; k < 36 * kTile / 2 / kTile; k++) cp_async16(dst + 2 * (lane + k * kTile), src + 2 * (lane + k * kTile));
+            if (ic < npe) {
+                const int e = pelem[ic], np = a.pcount[e], f = a.pfirst[e];
+                const double* ss = sens + ((int64_t)it * a.nparam + f) * sstride + b * 6 * kTile;
                 for (int j = 0; j < np; j++) {
-                    const double* ss = sens + ((((int64_t)t * a.nparam + f + j) * ntile + b) * 6) * kTile;
                     double* sd = dst + (36 + 6 * j) * kTile;
-                    for (int k = lane; k < 6 * kTile / 2; k += kTile) cp_async16(sd + 2 * k, ss + 2 * k);
+#pragma unroll
+                    for (int k = 0; k < 6 * kTile / 2 / kTile; k++)
+                        cp_async16(sd + 2 * (lane + k * kTile), ss + j * sstride + 2 * (lane + k * kTile));
                 }
             }
+            iu--;
+            if (--ic < 0) { ic = npe; it--; }
         }
         cp_async_commit();
+        if (++ist == kSweepStages) ist = 0;
     };
-    for (int i = 0; i < kSweepStages; i++) issue(U - 1 - i, i);
+    for (int i = 0; i < kSweepStages; i++) issue();
+    int t = nt - 1, c = npe, st = 0;
     for (int i = 0; i < U; i++) {
-        const int u = U - 1 - i, st = i % kSweepStages;
-        const int t = u / (npe + 1), c = u - t * (npe + 1);
         cp_async_wait<kSweepStages - 1>();
         __syncwarp();
         const double* S = stage + st * kStageDoubles;
@@ -453,7 +460,9 @@ __global__ void __launch_bounds__(kTile) k_adj_jsweep(const AdjParams a, int nt,
             for (int k = 0; k < 6; k++) lam[k] = out[k];
         }
         __syncwarp();
-        issue(u - kSweepStages, st);
+        issue();  // into the slot just read (the cursor is kSweepStages units ahead)
+        if (--c < 0) { c = npe; t--; }
+        if (++st == kSweepStages) st = 0;
     }
     cp_async_wait<0>();
     if (alive) store6(a.lam, n, p, lam);
