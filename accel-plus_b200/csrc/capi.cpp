@@ -267,7 +267,7 @@ template <class Mark>
 static int emit_part(accel_ctx* C, const CoreReq& q, int part, int turns, cudaStream_t s,
                      Mark mark, int& launches) {
     accel_line* L0 = q.lines[0];
-    int32_t* cnt = (int32_t*)C->cnt.p;  // [0] nlive [2] chunk [3] turn [4] err
+    int32_t* cnt = (int32_t*)C->cnt.p;  // [0] nlive [2] chunk [3] turn [4] err [5] lost since compaction
     int32_t* live = (int32_t*)C->live0.p;
     TrackParams P{};
     P.tables = q.tables;
@@ -281,6 +281,7 @@ static int emit_part(accel_ctx* C, const CoreReq& q, int part, int turns, cudaSt
     P.chunk_ctr = cnt + 2;
     P.turn_dev = cnt + 3;
     P.err = cnt + 4;
+    P.lost_flag = cnt + 5;
     P.seed = L0->seed;
     P.rng_base = (int32_t*)L0->d_rng.p;
     P.turn0 = 0;
@@ -288,7 +289,7 @@ static int emit_part(accel_ctx* C, const CoreReq& q, int part, int turns, cudaSt
     P.sched = q.sched;
     if (part == PART_PRE) {
         launch_init_live(q.st, q.ntot, q.loss, live, cnt + 0, cnt + 2, 1, s);
-        launch_fill_i32(cnt + 3, 0, 1, s);
+        launch_fill_i32(cnt + 3, 0, 3, s);  // turn counter, error word, lost flag
         launches += 2;
         return ACCEL_OK;
     }
@@ -361,7 +362,7 @@ static int emit_part(accel_ctx* C, const CoreReq& q, int part, int turns, cudaSt
                 a = b;
             }
         }
-        launch_compact(live, cnt + 0, q.st, live, cnt + 0, cnt + 2, cnt + 3, turns, s);
+        launch_compact(live, cnt + 0, q.st, cnt + 2, cnt + 3, turns, cnt + 5, s);
         launches++;
     } else {
         for (int k = q.e0; k < q.e1; k++) {

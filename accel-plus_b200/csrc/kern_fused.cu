@@ -103,6 +103,7 @@ __global__ void __launch_bounds__(BS, MINB) k_fused(const TrackParams P) {
                 if (nan_(s.x)) {
                     alive = false;
                     P.loss_turn[p] = P.turn0 + tbase + t;
+                    if (P.lost_flag) *P.lost_flag = 1;
                 }
             }
         }
@@ -152,17 +153,20 @@ void launch_rng_advance(int32_t* base, int nturn, cudaStream_t s) {
 }
 
 // ---- stable stream compaction of the live list (one block, blocked tiles) --------------------
-// In place (live_in == live_out) is safe: each tile is read into registers before any thread
-// writes, and an item is written at or before the index it was read from.
-__global__ void __launch_bounds__(1024) k_compact(const int32_t* live_in, const int32_t* nin,
-                                                  const double* __restrict__ x, int32_t* live_out,
-                                                  int32_t* nout, int32_t* chunk_ctr, int32_t* turn_ctr,
-                                                  int turns) {
+// In place is safe: each tile is read into registers before any thread writes, and an item is
+// written at or before the index it was read from.  When nothing was lost since the last
+// compaction (lost_flag clear) the list is already compact and is left as it is.
+__global__ void __launch_bounds__(1024) k_compact(int32_t* live, int32_t* nlive, const double* __restrict__ x,
+                                                  int32_t* chunk_ctr, int32_t* turn_ctr, int turns,
+                                                  int32_t* lost_flag) {
     constexpr int ITEMS = 8;
     constexpr int TILE = 1024 * ITEMS;
     __shared__ int warp_tot[32];
     __shared__ int s_carry;
-    const int n = *nin;
+    const int32_t* live_in = live;
+    int32_t* live_out = live;
+    const bool scan = !lost_flag || *lost_flag != 0;
+    const int n = scan ? *nlive : 0;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (threadIdx.x == 0) s_carry = 0;
     __syncthreads();
@@ -208,15 +212,18 @@ __global__ void __launch_bounds__(1024) k_compact(const int32_t* live_in, const 
         __syncthreads();
     }
     if (threadIdx.x == 0) {
-        *nout = s_carry;
+        if (scan) {
+            *nlive = s_carry;
+            if (lost_flag) *lost_flag = 0;
+        }
         *chunk_ctr = 0;
         if (turn_ctr) *turn_ctr += turns;
     }
 }
 
-void launch_compact(const int32_t* live_in, const int32_t* nin, const double* x, int32_t* live_out,
-                    int32_t* nout, int32_t* chunk_ctr, int32_t* turn_ctr, int turns, cudaStream_t s) {
-    k_compact<<<1, 1024, 0, s>>>(live_in, nin, x, live_out, nout, chunk_ctr, turn_ctr, turns);
+void launch_compact(int32_t* live, int32_t* nlive, const double* x, int32_t* chunk_ctr, int32_t* turn_ctr,
+                    int turns, int32_t* lost_flag, cudaStream_t s) {
+    k_compact<<<1, 1024, 0, s>>>(live, nlive, x, chunk_ctr, turn_ctr, turns, lost_flag);
 }
 
 __global__ void k_init_live(const double* __restrict__ x, int64_t n, int32_t* loss_turn,

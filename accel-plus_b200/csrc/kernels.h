@@ -18,6 +18,7 @@ struct TrackParams {
     const int32_t* nlive;    // device count of live entries
     int32_t* chunk_ctr;      // fused: atomic chunk counter, zero at launch
     int32_t* err;            // error word (bounded waits)
+    int32_t* lost_flag;      // set to 1 by a launch that loses a particle (may be null)
     int e0, e1;              // element range
     int nturn;               // turns in this launch (fused)
     int turn0;               // turn index (loss record) of the launch's first turn
@@ -36,10 +37,11 @@ struct VariantInfo { int block; int min_blocks; };
 VariantInfo fused_variant_info(int v);
 int fused_blocks_per_sm(int variant);                     // occupancy at the variant's block
 void launch_fused(const TrackParams& p, int variant, int grid, cudaStream_t s);
-// Stable compaction; live_in == live_out (in place) is allowed.  Resets the chunk counter and
-// adds `turns` to the device turn counter.
-void launch_compact(const int32_t* live_in, const int32_t* nin, const double* x, int32_t* live_out,
-                    int32_t* nout, int32_t* chunk_ctr, int32_t* turn_ctr, int turns, cudaStream_t s);
+// Stable compaction, in place (live == the list it compacts).  Resets the chunk counter and adds
+// `turns` to the device turn counter.  With lost_flag, the list is scanned only when the flag is
+// set (a particle was lost since the last compaction), and the flag is cleared.
+void launch_compact(int32_t* live, int32_t* nlive, const double* x, int32_t* chunk_ctr, int32_t* turn_ctr,
+                    int turns, int32_t* lost_flag, cudaStream_t s);
 void launch_init_live(const double* x, int64_t n, int32_t* loss_turn, int32_t* live, int32_t* nlive,
                       int32_t* chunk_ctr, int init_loss, cudaStream_t s);
 void launch_aos_to_soa(const double* aos, double* soa, int64_t n, cudaStream_t s);
