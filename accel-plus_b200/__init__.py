@@ -34,7 +34,7 @@ MAX_MPOLE = 10
 RAD_OFF, RAD_RAD, RAD_RADQE, RAD_LUMP, RAD_LUMP_DAMP, RAD_LUMP_QE = range(6)
 (F_LENGTH, F_K, F_POLYNOMB, F_POLYNOMA, F_NSLICE, F_MAXNPOLE, F_ANGLE, F_E1, F_E2, F_VOLTAGE,
  F_FREQUENCY, F_PHIS, F_ENERGY, F_KICKX, F_KICKY, F_XLIM, F_YLIM) = range(1, 18)
-MODE_FUSED, MODE_PLAIN = 0, 1
+MODE_FUSED, MODE_PLAIN, MODE_EXACT = 0, 1, 2
 LAYOUT_AOS, LAYOUT_SOA = 0, 1
 
 

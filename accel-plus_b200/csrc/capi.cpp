@@ -247,9 +247,12 @@ struct Plan {
 // constant so graphs that captured the scratch pointer never see it reallocated.
 constexpr size_t kScratchDoubles = 65536;
 
+constexpr int kExactSegTurns = 16;  // turns per exact-mode launch (a line without wakes)
+
 static Plan make_plan(const CoreReq& q, bool has_coll) {
     Plan p;
     if (q.mode == ACCEL_MODE_FUSED && !has_coll) p.seg = std::max(1, std::min(q.seg, q.nturn));
+    else if (q.mode == ACCEL_MODE_EXACT && !has_coll) p.seg = std::max(1, std::min(kExactSegTurns, q.nturn));
     else p.seg = 1;
     p.nbody = q.nturn / p.seg;
     p.tail = q.nturn - p.nbody * p.seg;
@@ -364,6 +367,30 @@ static int emit_part(accel_ctx* C, const CoreReq& q, int part, int turns, cudaSt
         }
         launch_compact(live, cnt + 0, q.st, cnt + 2, cnt + 3, turns, cnt + 5, s);
         launches++;
+    } else if (q.mode == ACCEL_MODE_EXACT) {
+        if (!has_collective(L0, q.e0, q.e1)) {
+            mark(0);
+            launch_exact(P, q.e0, q.e1, turns, cnt + 3, true, s);
+            mark(1);
+            launches += 2;
+        } else {
+            // one turn: local ranges in one launch each, wake elements by their kernels
+            int a = q.e0;
+            while (a < q.e1) {
+                int b = a;
+                while (b < q.e1 && !is_collective(L0->desc[b].type)) b++;
+                if (b > a) {
+                    mark(0);
+                    launch_exact(P, a, b, 1, cnt + 3, false, s);
+                    mark(1);
+                    launches++;
+                }
+                if (b < q.e1) { coll(b); b++; }
+                a = b;
+            }
+            launch_plain_turn_end(P, cnt + 3, s);
+            launches += 2;
+        }
     } else {
         for (int k = q.e0; k < q.e1; k++) {
             if (is_collective(L0->desc[k].type)) {
@@ -751,7 +778,8 @@ int accel_track(accel_line* L, double* r, int layout, int N, int st, int ed, int
                 int32_t* loss_turn, int mode, void* stream) {
     if (!L || (!r && N > 0) || N < 0 || nturn < 0) return fail(ACCEL_E_INVALID, "bad argument");
     if (layout != ACCEL_LAYOUT_AOS && layout != ACCEL_LAYOUT_SOA) return fail(ACCEL_E_INVALID, "bad layout");
-    if (mode != ACCEL_MODE_FUSED && mode != ACCEL_MODE_PLAIN) return fail(ACCEL_E_INVALID, "bad mode");
+    if (mode != ACCEL_MODE_FUSED && mode != ACCEL_MODE_PLAIN && mode != ACCEL_MODE_EXACT)
+        return fail(ACCEL_E_INVALID, "bad mode");
     const int ne = (int)L->desc.size();
     if (st < 0 || ed > ne || st > ed) return fail(ACCEL_E_INVALID, "element range out of bounds");
     accel_ctx* C = L->ctx;
@@ -884,7 +912,8 @@ int accel_track_batched(accel_line* const* lines, int ninst, const int64_t* part
     int s = check_batch(lines, ninst, part_off, ntot);
     if (s) return s;
     if (!r_soa || nturn < 0) return fail(ACCEL_E_INVALID, "bad argument");
-    if (mode != ACCEL_MODE_FUSED && mode != ACCEL_MODE_PLAIN) return fail(ACCEL_E_INVALID, "bad mode");
+    if (mode != ACCEL_MODE_FUSED && mode != ACCEL_MODE_PLAIN && mode != ACCEL_MODE_EXACT)
+        return fail(ACCEL_E_INVALID, "bad mode");
     accel_ctx* C = lines[0]->ctx;
     std::lock_guard<std::mutex> lk(C->mu);
     CK(cudaSetDevice(C->device));

@@ -1,6 +1,6 @@
 // deck.cpp — `accel+gpu`: the reference's input-deck interpreter (src/process.cpp) over the GPU.
 //
-//   accel+gpu DECK [--device N] [--plain] [--seed S]
+//   accel+gpu DECK [--device N] [--plain | --exact] [--seed S]
 //
 // Blocks (process.cpp:40-107): Lattice, Optics, Track, DAMA, each ended by `End`; Survey is
 // accepted and ignored; STOP / RETURN end the deck.  Lines: '#' and '%' start comments, a trailing
@@ -824,7 +824,7 @@ void Deck::dama(std::istream& in) {
 
 int main(int argc, char** argv) {
     if (argc < 2) {
-        std::cerr << "usage: accel+gpu DECK [--device N] [--plain] [--seed S]" << std::endl;
+        std::cerr << "usage: accel+gpu DECK [--device N] [--plain | --exact] [--seed S]" << std::endl;
         return 1;
     }
     Deck D;
@@ -832,6 +832,7 @@ int main(int argc, char** argv) {
     for (int i = 2; i < argc; i++) {
         if (!std::strcmp(argv[i], "--device") && i + 1 < argc) device = std::atoi(argv[++i]);
         else if (!std::strcmp(argv[i], "--plain")) D.mode = ACCEL_MODE_PLAIN;
+        else if (!std::strcmp(argv[i], "--exact")) D.mode = ACCEL_MODE_EXACT;
         else if (!std::strcmp(argv[i], "--seed") && i + 1 < argc) D.rng.seed(std::strtoull(argv[++i], nullptr, 10));
     }
     std::ifstream fin(argv[1]);

@@ -47,6 +47,50 @@ void launch_plain_turn_end(const TrackParams& p, int32_t* turn_ctr, cudaStream_t
     k_inc<<<1, 1, 0, s>>>(turn_ctr);
 }
 
+// Exact mode: the same literal maps and the same --fmad=false arithmetic as k_plain_elem, so the
+// coordinates are bit-identical to the plain kernel's, but one thread carries its particle
+// through the elements [e0, e1) of `nturn` turns with the state in registers (no HBM round trip
+// and no launch per element).  The QE counters are the plain kernel's (turn = the line's base +
+// rng_turn0 + device turn counter, element index).  With record, a particle found lost at the
+// end of a turn gets that turn as its loss turn, as k_plain_turn_end records it; without it (a
+// range of a turn that a collective element splits) the caller's turn-end kernel does that.
+__global__ void __launch_bounds__(128) k_exact(const TrackParams P, int e0, int e1, int nturn,
+                                               const int32_t* __restrict__ turn_ctr, int record) {
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t n = P.ntot;
+    if (p >= n) return;
+    double* __restrict__ st = P.st;
+    double r[6];
+    r[0] = st[p];
+    if (r[0] != r[0]) return;
+    r[1] = st[n + p]; r[2] = st[2 * n + p]; r[3] = st[3 * n + p]; r[4] = st[4 * n + p]; r[5] = st[5 * n + p];
+    const int inst = P.pinst ? P.pinst[p] : 0;
+    const DevElem* __restrict__ T = P.tables + (P.tbl_off ? P.tbl_off[inst] : 0);
+    const int t0 = *turn_ctr;
+    const uint32_t rbase = (uint32_t)((P.rng_base ? *P.rng_base : 0) + P.rng_turn0);
+    for (int t = 0; t < nturn; t++) {
+        for (int e = e0; e < e1; e++) {
+            lit::QeSource q{P.seed, (uint32_t)p, rbase + (uint32_t)(t0 + t), (uint32_t)T[e].elem, 0u};
+            lit::pass<double>(T[e], r, q);
+            if (r[0] != r[0]) break;
+        }
+        if (r[0] != r[0]) {
+            if (record && P.loss_turn[p] < 0) P.loss_turn[p] = P.turn0 + t0 + t;
+            break;
+        }
+    }
+    st[p] = r[0]; st[n + p] = r[1]; st[2 * n + p] = r[2];
+    st[3 * n + p] = r[3]; st[4 * n + p] = r[4]; st[5 * n + p] = r[5];
+}
+__global__ void k_add(int32_t* c, int v) { *c += v; }
+
+void launch_exact(const TrackParams& p, int e0, int e1, int nturn, int32_t* turn_ctr, bool record,
+                  cudaStream_t s) {
+    if (p.ntot > 0)
+        k_exact<<<(unsigned)((p.ntot + 127) / 128), 128, 0, s>>>(p, e0, e1, nturn, turn_ctr, record ? 1 : 0);
+    if (record) k_add<<<1, 1, 0, s>>>(turn_ctr, nturn);
+}
+
 // One-turn matrix.  method 0: exact tangent map — the literal maps on Dual<6> seeded with the
 // identity; method 1: twelve particles at +/-delta, m_ij = (r+_i - r-_i)/2/delta (aline.cpp:900-927).
 __global__ void k_m66_exact(const DevElem* __restrict__ tbl, int e0, int e1, const double* r0, double* m) {

@@ -70,6 +70,10 @@ double fp64_peak_run(int sm_count, cudaStream_t s, float* ms_out);
 // ---- plain (kern_plain.cu) ----------------------------------------------------------------
 void launch_plain_elem(const TrackParams& p, int e, const int32_t* turn_ctr, cudaStream_t s);
 void launch_plain_turn_end(const TrackParams& p, int32_t* turn_ctr, cudaStream_t s);
+// exact mode: the plain kernel's arithmetic over [e0, e1) for nturn turns in one launch; with
+// record, loss turns are recorded and the turn counter advanced by nturn (a second, tiny launch)
+void launch_exact(const TrackParams& p, int e0, int e1, int nturn, int32_t* turn_ctr, bool record,
+                  cudaStream_t s);
 // exact tangent map (Dual<6>) / central differences through [e0, e1) of one table
 void launch_m66(const DevElem* tbl, int e0, int e1, const double* r0_dev, double delta, int method,
                 double* m_dev, cudaStream_t s);

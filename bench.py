@@ -438,13 +438,31 @@ def engine_arm(args):
         torch.cuda.synchronize()
         pms = max_over_ranks(p0.elapsed_time(p1))
         lp = loss.cpu().numpy()
+        sp = state.cpu().numpy()
+        pt_plain = sum_over_ranks(float(tracked_turns(lp, args.turns).sum()))
         diff = lp != loss_np
-        plain = {"value": total_pt / (pms / 1e3), "ms_per_step": pms,
-                 "fused_over_plain": (total_pt / (ms_step / 1e3)) / (total_pt / (pms / 1e3)),
+        plain = {"value": pt_plain / (pms / 1e3), "ms_per_step": pms,
+                 "fused_over_plain": value / (pt_plain / (pms / 1e3)),
                  "loss_turn_mismatches": int(diff.sum()),
                  "mismatch_note": "particles whose loss turn differs between the two kernels; the "
                                   "parity tests confine such differences to the chaotic aperture edge",
                  "survival_mismatches": int(((lp < 0) != (loss_np < 0)).sum())}
+        # the exact mode: the plain kernel's arithmetic with the state in registers over turns
+        step(mode=A.MODE_EXACT)
+        torch.cuda.synchronize()
+        x0, x1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        x0.record()
+        step(mode=A.MODE_EXACT)
+        x1.record()
+        torch.cuda.synchronize()
+        xms = max_over_ranks(x0.elapsed_time(x1))
+        lx = loss.cpu().numpy()
+        sx = state.cpu().numpy()
+        pt_exact = sum_over_ranks(float(tracked_turns(lx, args.turns).sum()))
+        same = bool(np.array_equal(lx, lp) and np.array_equal(sx.view(np.int64), sp.view(np.int64)))
+        plain["exact"] = {"value": pt_exact / (xms / 1e3), "ms_per_step": xms,
+                          "exact_over_plain": (pt_exact / (xms / 1e3)) / (pt_plain / (pms / 1e3)),
+                          "bit_identical_to_plain": same}
 
     # ---- end to end through the C-ABI with host buffers ----
     e2e = None

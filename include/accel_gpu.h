@@ -136,6 +136,9 @@ typedef struct accel_elem_desc {
 /* track modes */
 #define ACCEL_MODE_FUSED  0  /* persistent batched kernel: registers across turns, compaction */
 #define ACCEL_MODE_PLAIN  1  /* one launch per element, state in HBM, reference operation order */
+#define ACCEL_MODE_EXACT  2  /* the plain mode's arithmetic, bit-identical to it, with the state
+                                in registers over whole turns (one launch per 16 turns, or per
+                                range between wake elements); no counterpart in the reference  */
 
 /* state layouts */
 #define ACCEL_LAYOUT_AOS  0  /* r[6*i + k]  (the reference's layout) */

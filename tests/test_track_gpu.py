@@ -35,30 +35,83 @@ def _flags(line, A, name):
         line.set_flags(rad=A.RAD_LUMP_DAMP)
 
 
-@pytest.mark.parametrize("mode", ["plain", "fused"])
+MODES = {"plain": 1, "exact": 2, "fused": 0}  # A.MODE_PLAIN / MODE_EXACT / MODE_FUSED
+
+
+@pytest.mark.parametrize("mode", ["plain", "exact", "fused"])
 def test_elements_against_reference(A, ctx, G, MG, mode):
-    m = A.MODE_PLAIN if mode == "plain" else A.MODE_FUSED
+    m = MODES[mode]
     for name, elems in MG.element_cases().items():
         line = A.Line(ctx, elems)
         _flags(line, A, name)
         r = G["elem_in"].copy()
         line.track(r, 1, mode=m)
         ref = G[f"elem_{name}"]
-        if mode == "plain" and name not in TRANSCENDENTAL:
+        if mode != "fused" and name not in TRANSCENDENTAL:
             assert same_bits(r, ref), name
-        elif mode == "plain":
+        elif mode != "fused":
             assert rel_err(r, ref) < 1e-14, name
         else:
             assert rel_err(r, ref) < 1e-12, (name, rel_err(r, ref))
         assert np.array_equal(np.isnan(r[:, 0]), np.isnan(ref[:, 0])), name
 
 
-def test_plain_fodo_bit_exact(A, ctx, G, LT):
+@pytest.mark.parametrize("mode", ["plain", "exact"])
+def test_plain_fodo_bit_exact(A, ctx, G, LT, mode):
     line = A.Line(ctx, LT.config1_ring())
     for turns, key in ((1, "fodo_t1"), (100, "fodo_t100")):
         r = G["fodo_in"].copy()
-        line.track(r, turns, mode=A.MODE_PLAIN)
+        line.track(r, turns, mode=MODES[mode])
         assert same_bits(r, G[key]), key
+
+
+def _exact_vs_plain(A, lines, off, aos, nturn):
+    """Track the same particles in plain and in exact mode (batched over `lines`); return both
+    final states and loss turns.  Each run restarts the lines' QE sequences (set_seed), which
+    every tracking call otherwise advances."""
+    import torch
+    out = []
+    for m in (A.MODE_PLAIN, A.MODE_EXACT):
+        for k, l in enumerate(lines):
+            l.set_seed(4242 + k)
+        soa = torch.tensor(aos.T.copy(), device="cuda", dtype=torch.float64).contiguous()
+        loss = torch.empty(len(aos), device="cuda", dtype=torch.int32)
+        A.track_batched(lines, off, soa, nturn, loss=loss, mode=m)
+        torch.cuda.synchronize()
+        out.append((soa.cpu().numpy().T.copy(), loss.cpu().numpy()))
+    return out
+
+
+def test_exact_mode_is_the_plain_kernel_bit_for_bit(A, ctx, G, LT):
+    """The exact mode keeps the state in registers over 16-turn launches but does the plain
+    kernel's arithmetic: coordinates, aperture codes and loss turns equal bit for bit, with
+    radiation and RF (the DA grid of the DBA, 200 turns, particles lost all along), with quantum
+    excitation (the same counter-based normals), over error-seeded copies in one batch, and on a
+    line whose longitudinal wake splits every turn into ranges."""
+    base = LT.config2_ring()
+    # radiation + RF, losses
+    line = A.Line(ctx, base)
+    g = G["dba_grid_in"]
+    (rp, lp), (re, le) = _exact_vs_plain(A, [line], np.array([0, len(g)]), g, 200)
+    assert same_bits(re, rp) and np.array_equal(le, lp) and (lp >= 0).any() and (lp < 0).any()
+    # quantum excitation
+    qline = A.Line(ctx, base)
+    qline.set_flags(rad=A.RAD_RADQE)
+    r0 = LT.config5_particles(2048, line.m66(), seed=3)
+    (rp, lp), (re, le) = _exact_vs_plain(A, [qline], np.array([0, 2048]), r0, 40)
+    assert same_bits(re, rp) and np.array_equal(le, lp)
+    # error copies, one batch
+    rings = [LT.error_copy(base, k) for k in (0, 1, 7)]
+    grids = [G["c3_0_in"], G["c3_1_in"], LT.da_grid(7, 3)]
+    off = np.zeros(4, dtype=np.int64)
+    off[1:] = np.cumsum([x.shape[0] for x in grids])
+    (rp, lp), (re, le) = _exact_vs_plain(A, [A.Line(ctx, r) for r in rings], off, np.concatenate(grids), 100)
+    assert same_bits(re, rp) and np.array_equal(le, lp)
+    # a wake element every turn
+    wline = A.Line(ctx, base + [LT.longwake_elem()])
+    wline.set_flags(wake=1)
+    (rp, lp), (re, le) = _exact_vs_plain(A, [wline], np.array([0, 2048]), r0, 20)
+    assert same_bits(re, rp) and np.array_equal(le, lp)
 
 
 def test_fused_fodo_tolerance(A, ctx, G, LT):
