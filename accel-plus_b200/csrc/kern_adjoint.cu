@@ -433,7 +433,7 @@ __global__ void __launch_bounds__(kTile) k_adj_jsweep(const AdjParams a, int nt,
         if (++ist == kSweepStages) ist = 0;
     };
     for (int i = 0; i < kSweepStages; i++) issue();
-    int t = nt - 1, c = npe, st = 0;
+    int c = npe, st = 0;
     for (int i = 0; i < U; i++) {
         cp_async_wait<kSweepStages - 1>();
         __syncwarp();
@@ -461,7 +461,7 @@ __global__ void __launch_bounds__(kTile) k_adj_jsweep(const AdjParams a, int nt,
         }
         __syncwarp();
         issue();  // into the slot just read (the cursor is kSweepStages units ahead)
-        if (--c < 0) { c = npe; t--; }
+        if (--c < 0) c = npe;
         if (++st == kSweepStages) st = 0;
     }
     cp_async_wait<0>();
