@@ -77,6 +77,25 @@ def test_deck_matches_reference(deck):
     compare(run_deck(deck), ref)
 
 
+@pytest.mark.gpu
+def test_exact_corrections_reach_their_targets():
+    """correct_tune / correct_chrom with EXACT (an extension of the reference's commands): Newton
+    iterations on tunes and chromaticities from exact one-turn tangent maps land on the targets
+    to the printed six digits, where the reference's fit (one step of a difference-based
+    response) leaves a residual; the following print_tune shows the corrected tunes."""
+    out = run_deck("engine_only/correct_exact")  # no reference output: EXACT is this engine's
+    tunes = [l for l in out if l.startswith("corrected tunes:")]
+    chrom = [l for l in out if l.startswith("corrected chromaticities:")]
+    assert len(tunes) == 1 and len(chrom) == 1
+    t = [float(x) for x in NUM.findall(tunes[0])]
+    c = [float(x) for x in NUM.findall(chrom[0])]
+    assert abs(t[0] - 0.19) < 2e-6 and abs(t[1] - 0.36) < 2e-6, tunes
+    assert abs(c[0] - 1.0) < 2e-5 and abs(c[1] - 1.5) < 2e-5, chrom
+    printed = [l for l in out if l.startswith("Tunes:")][-1]
+    p = [float(x) for x in NUM.findall(printed)]
+    assert abs(p[0] - 0.19) < 2e-5 and abs(p[1] - 0.36) < 2e-5, printed
+
+
 def test_deck_compare_accepts_reference_against_itself():
     """The comparison's own logic, on the golden outputs alone (no GPU)."""
     for deck in ("dba_deck", "fodo_deck", "ops_deck", "dist_deck"):
