@@ -509,9 +509,13 @@ static int run_core(accel_ctx* C, const CoreReq& q, cudaStream_t user) {
     return ACCEL_OK;
 }
 
+// Untuned jobs run variant 4 (128 threads, 5 blocks per SM; the autotuner's choice on the batched
+// DA benchmark and the fastest on a 2^20-particle bunch with a per-turn wake) with 8-turn segments.
+constexpr int kDefaultVariant = 4, kDefaultSeg = 8;
+
 static void default_tile(accel_ctx* C, int& variant, int& seg, int& sched) {
-    variant = C->tile_variant >= 0 ? C->tile_variant : 0;
-    seg = C->tile_seg > 0 ? C->tile_seg : 16;
+    variant = C->tile_variant >= 0 ? C->tile_variant : kDefaultVariant;
+    seg = C->tile_seg > 0 ? C->tile_seg : kDefaultSeg;
     sched = C->tile_sched >= 0 ? C->tile_sched : 0;
 }
 

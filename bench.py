@@ -557,11 +557,15 @@ def wake_leg(A, LT, ctx, nturn: int = 200, n: int = 1 << 20) -> dict:
             "timing": "CUDA events on the launching stream, state resident on the device"}
 
 
-def wake_only(turns: int):
+def wake_only(turns: int, variant: int = -1):
     A = importlib.import_module("accel-plus_b200")
     LT = importlib.import_module("accel-plus_b200.lattices")
     ctx = A.Context(0)
-    print(json.dumps({"wake": wake_leg(A, LT, ctx, nturn=turns)}), flush=True)
+    if variant >= 0:
+        ctx.set_tile(0, 0, variant)
+    out = wake_leg(A, LT, ctx, nturn=turns)
+    out["tile"] = ctx.get_tile()
+    print(json.dumps({"wake": out}), flush=True)
     ctx.close()
 
 
@@ -579,7 +583,7 @@ def main():
         adjoint_only()
         return
     if args.wake_only:
-        wake_only(args.wake_turns)
+        wake_only(args.wake_turns, args.variant)
         return
     if args.impl == "reference":
         reference_arm(args)
