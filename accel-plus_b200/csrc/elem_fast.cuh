@@ -121,11 +121,11 @@ struct HxCoef { double a, b, c, dd, g; };
 
 __device__ __forceinline__ HxCoef hx_coef(double L, double h, double inv) {
     HxCoef k;
-    double hs = h * L;
+    const double hs = h * L, inv2 = inv * inv;
     k.a = inv * L;
-    k.b = 0.25 * hs * L * inv * inv;
-    k.c = 0.5 * hs * inv;
-    k.dd = 0.5 * L * inv * inv;
+    k.b = (0.25 * hs * L) * inv2;
+    k.c = (0.5 * hs) * inv;
+    k.dd = (0.5 * L) * inv2;
     k.g = 0.5 * hs;
     return k;
 }
@@ -169,12 +169,14 @@ struct BkCoef {
 
 // With K1 = K2 = 0 (a pure dipole field plus B[0..M]) the curved kick reduces to
 // px -= L (re + h (h x - delta)), py += L im, z -= L h x.
-template <bool PURE>
+// NOIM: the field has no imaginary part at all (a dipole field B[0] alone, M = 0, and K1 = K2 =
+// 0), so the vertical kick is zero and is skipped (fma(L, 0, py) = py for finite L).
+template <bool PURE, bool NOIM = false>
 __device__ __forceinline__ void bend_kick_core(St& s, const BkCoef& c, double re, double im,
                                                double L) {
     if (PURE) {
         s.px = fma(-L, fma(c.h, fma(c.h, s.x, -s.d), re), s.px);
-        s.py = fma(L, im, s.py);
+        if (!NOIM) s.py = fma(L, im, s.py);
         s.z = fma(-L * c.h, s.x, s.z);
         return;
     }
@@ -207,8 +209,11 @@ __device__ __forceinline__ double bend_kick_rad(St& s, const double* B, const Bk
     double vq = fma(xpr, xpr, ypr * ypr);
     double vn2 = rcp(fma(hx1, hx1, vq));
     double by = re + c.h, bx = im;
-    double cr = fma(bx, ypr, -by * xpr);
-    double b2p = fma(by * hx1, by * hx1, fma(bx * hx1, bx * hx1, cr * cr)) * vn2;
+    // with no imaginary field (M = 0, PURE) bx is exactly 0 and its terms are +0: left out
+    constexpr bool NOIM = (M == 0) && PURE;
+    double cr = NOIM ? -by * xpr : fma(bx, ypr, -by * xpr);
+    double b2p = (NOIM ? fma(by * hx1, by * hx1, cr * cr)
+                       : fma(by * hx1, by * hx1, fma(bx * hx1, bx * hx1, cr * cr))) * vn2;
     double opd = 1.0 + s.d;
     double mean = crad * (opd * opd) * b2p * fma(0.5, vq, hx1) * L;
     double loss;
@@ -222,7 +227,7 @@ __device__ __forceinline__ double bend_kick_rad(St& s, const double* B, const Bk
     double opd2 = 1.0 + s.d;
     s.px = xpr * opd2;
     s.py = ypr * opd2;
-    bend_kick_core<PURE>(s, c, re, im, L);
+    bend_kick_core<PURE, NOIM>(s, c, re, im, L);
     const double u = loss * inv;  // 1/(1+d-D) = inv (1 + u + u^2 + u^3 + ...)
     if (fabs(u) < 1e-4) return fma(inv * u, fma(u, u, u) + 1.0, inv);
     return rcp(opd2);
@@ -256,11 +261,11 @@ __device__ __forceinline__ void bendmpole(St& s, const DevElem* __restrict__ e,
         for (int m = 0; m < ns; m++) {
             double re, im;
             hxdrift(s, c.h, k1);
-            horner_b<M>(s, B, re, im); bend_kick_core<PURE>(s, c, re, im, K1);
+            horner_b<M>(s, B, re, im); bend_kick_core<PURE, (M == 0) && PURE>(s, c, re, im, K1);
             hxdrift(s, c.h, k2);
-            horner_b<M>(s, B, re, im); bend_kick_core<PURE>(s, c, re, im, K2);
+            horner_b<M>(s, B, re, im); bend_kick_core<PURE, (M == 0) && PURE>(s, c, re, im, K2);
             hxdrift(s, c.h, k2);
-            horner_b<M>(s, B, re, im); bend_kick_core<PURE>(s, c, re, im, K1);
+            horner_b<M>(s, B, re, im); bend_kick_core<PURE, (M == 0) && PURE>(s, c, re, im, K1);
             hxdrift(s, c.h, k1);
         }
     } else if (rad == 1) {
