@@ -231,6 +231,29 @@ def test_range_pass_and_layouts(A, ctx, O, G, LT):
     assert same_bits(dev.cpu().numpy(), ref)
 
 
+@pytest.mark.parametrize("mode", ["fused", "exact"])
+def test_range_pass_other_modes(A, ctx, O, G, LT, mode):
+    """pass(r, N, st, ed) in the fused and exact modes: a sub-range against the reference's
+    pass_line (1e-12 fused, bit for bit exact), and a turn tracked as two ranges equal to the
+    turn in one call (each element's arithmetic does not depend on where a call starts)."""
+    ring = LT.config1_ring()
+    line = A.Line(ctx, ring)
+    p = G["fodo_in"].copy()
+    ref = p.copy()
+    O.port_pass_line(ring, ref, 17, 211)
+    r = p.copy()
+    line.track(r, 1, st=17, ed=211, mode=MODES[mode])
+    if mode == "exact":
+        assert same_bits(r, ref)
+    else:
+        assert rel_err(r, ref) < 1e-12
+    whole, split = p.copy(), p.copy()
+    line.track(whole, 1, mode=MODES[mode])
+    line.track(split, 1, st=0, ed=123, mode=MODES[mode])
+    line.track(split, 1, st=123, ed=len(ring), mode=MODES[mode])
+    assert same_bits(split, whole)
+
+
 def test_beam_stat_matches_calc_beam_stat(A, ctx, O, G):
     r = G["dba_grid_out"].copy()
     mean, sig, cross, nl = ctx.beam_stat(r)
