@@ -22,8 +22,8 @@ DECKS = os.path.join(ROOT, "tests", "decks")
 NUM = re.compile(r"[-+]?(?:\d+\.?\d*|\.\d+)(?:[eE][-+]?\d+)?")
 
 
-def run_deck(name):
-    out = subprocess.run([EXE, os.path.join(DECKS, name + ".in")], cwd=ROOT, capture_output=True,
+def run_deck(name, *flags):
+    out = subprocess.run([EXE, os.path.join(DECKS, name + ".in"), *flags], cwd=ROOT, capture_output=True,
                          text=True, timeout=600)
     assert out.returncode == 0, out.stdout[-2000:] + out.stderr[-2000:]
     return [l for l in out.stdout.splitlines() if not l.startswith("#UTC")]
@@ -75,6 +75,15 @@ def test_deck_matches_reference(deck):
     with open(os.path.join(GOLDEN, deck + ".ref.out")) as f:
         ref = [l for l in f.read().splitlines() if not l.startswith("#UTC")]
     compare(run_deck(deck), ref)
+
+
+@pytest.mark.gpu
+def test_deck_in_exact_mode_matches_reference():
+    """The DBA deck (optics, DA and MA scans, tracking) with --exact: the reference's operation
+    order throughout, against the reference's own output."""
+    with open(os.path.join(GOLDEN, "dba_deck.ref.out")) as f:
+        ref = [l for l in f.read().splitlines() if not l.startswith("#UTC")]
+    compare(run_deck("dba_deck", "--exact"), ref)
 
 
 @pytest.mark.gpu
