@@ -91,6 +91,10 @@ def lib() -> C.CDLL:
         "accel_lattice_parse": (I, [C.c_char_p, C.POINTER(pd), C.POINTER(I)]),
         "accel_lattice_write": (I, [C.c_char_p, pd, I, I]),
         "accel_lattice_free": (None, [pd]),
+        "accel_state_write": (I, [C.c_char_p, P, C.c_int64, C.c_int64, P]),
+        "accel_state_read": (I, [C.c_char_p, C.POINTER(C.POINTER(D)), C.POINTER(C.c_int64),
+                                 C.POINTER(C.c_int64), C.POINTER(C.POINTER(C.c_int32))]),
+        "accel_state_free": (None, [P]),
         "accel_wigtable_create": (I, [I, I, P, P, P, P, C.POINTER(C.c_int32)]),
         "accel_wigtable_info": (I, [C.c_int32, C.POINTER(I), C.POINTER(I)]),
         "accel_wigtable_get": (I, [C.c_int32, P, P, P, P]),
@@ -199,6 +203,29 @@ def elem(type_: int, famname: str = "undefined", length: float = 0.0, **kw) -> E
     if type_ in (BEND, BENDMPOLE) and length != 0:
         d.f[4] = d.f[0] / length
     return d
+
+
+def write_state(path: str, r, turn: int = 0, loss=None) -> None:
+    """Lossless particle-state checkpoint (accel_state_write): r is (N, 6) float64 on the host."""
+    r = np.ascontiguousarray(r, dtype=np.float64)
+    lt = None if loss is None else np.ascontiguousarray(loss, dtype=np.int32)
+    _check(lib().accel_state_write(path.encode(), C.c_void_p(r.ctypes.data), r.size // 6, int(turn),
+                                   None if lt is None else C.c_void_p(lt.ctypes.data)), "accel_state_write")
+
+
+def read_state(path: str):
+    """(r (N, 6), turn, loss turns or None) from a checkpoint written by write_state."""
+    pr, pl = C.POINTER(C.c_double)(), C.POINTER(C.c_int32)()
+    n, turn = C.c_int64(), C.c_int64()
+    _check(lib().accel_state_read(path.encode(), C.byref(pr), C.byref(n), C.byref(turn), C.byref(pl)),
+           "accel_state_read")
+    r = np.ctypeslib.as_array(pr, shape=(max(1, n.value) * 6,))[: 6 * n.value].reshape(n.value, 6).copy()
+    loss = None
+    if pl:
+        loss = np.ctypeslib.as_array(pl, shape=(max(1, n.value),))[: n.value].copy()
+        lib().accel_state_free(C.cast(pl, C.c_void_p))
+    lib().accel_state_free(C.cast(pr, C.c_void_p))
+    return r, turn.value, loss
 
 
 def set_device_memory_limit(nbytes: int | None) -> None:

@@ -11,7 +11,8 @@
 //            on exact one-turn matrices)  set_max_num_threads  modify_element  set_flags
 //   Optics   print_tune  print_chrom  print_matrix  print_optics
 //   Track    Distribution (none | Zero NPar= | Coordinate r=(..;..) | Gaussian .. | Linear ..
-//            | Load F[, format=plain|accel-export]; shift=(..); Print)  Monitor  Do_Track  Transport
+//            | Load F[, format=plain|accel-export|binary]; shift=(..); Print)  Monitor
+//            Do_Track (+ save=F: a lossless binary checkpoint of the final distribution)  Transport
 //   DAMA     track_DA  track_MA  track_dNudJ
 // Differences: Gaussian distributions come from a seeded generator (--seed; the reference seeds
 // rand() with the time, process.cpp:42); a family member picked with index >= 2 is that member
@@ -601,6 +602,16 @@ int Deck::distribution(const string& line_in) {
         ss >> fname;
         if (!fname.empty() && fname.back() == ',') fname.pop_back();
         cout << fname << endl;
+        if (upper(sel).find("FORMAT=BINARY") != string::npos) {
+            // this engine's lossless checkpoint (Do_Track save=FILE, accel_state_write)
+            double* rr = nullptr;
+            int64_t n = 0, t = 0;
+            int st = accel_state_read(fname.c_str(), &rr, &n, &t, nullptr);
+            if (st) { cout << "cannot load " << fname << ": " << accel_last_error() << endl; return 0; }
+            r.assign(rr, rr + 6 * n);
+            accel_state_free(rr);
+            return (int)n;
+        }
         bool exported = upper(sel).find("ACCEL-EXPORT") != string::npos;
         std::ifstream f(fname);
         string sl;
@@ -717,6 +728,11 @@ void Deck::track(std::istream& in) {
                 } else if (iequal(pf, "Yes") || iequal(pf, "same")) {
                     L->monitor_print(r.data(), np, nturn, cout);
                 }
+                // save=FILE (an extension): the final distribution as a lossless checkpoint, read
+                // back by "Distribution : Load FILE, format=binary"
+                const string save = get(a, "SAVE");
+                if (!save.empty() && accel_state_write(save.c_str(), r.data(), np, nturn, nullptr))
+                    cout << "cannot save " << save << ": " << accel_last_error() << endl;
                 cout << "*************************************" << endl;
             }
         } else if (k == 3) {

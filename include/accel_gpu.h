@@ -178,6 +178,20 @@ int  accel_lattice_parse(const char* text, accel_elem_desc** elems, int* n);
 int  accel_lattice_write(const char* path, const accel_elem_desc* elems, int n, int precision);
 
 /*
+ * Particle-state checkpoints, lossless (no counterpart in the reference, whose only saved state is
+ * the 6-digit text of Do_Track's "Full export", process.cpp:2054-2066, read back by
+ * "Distribution: Load f, format=accel-export", process.cpp:1499-1546).  Host arrays, AoS
+ * (x px y py z delta per particle).  The file: a 32-byte header ("ACCELST1", uint32 version 1,
+ * uint32 flags (bit 0: loss turns present), int64 N, int64 turn), then 6N IEEE-754 doubles, then
+ * N int32 loss turns when present; all little-endian.  accel_state_read allocates *r (and
+ * *loss_turn, NULL when the file has none) with malloc: release with accel_state_free.
+ */
+int  accel_state_write(const char* path, const double* r, int64_t N, int64_t turn,
+                       const int32_t* loss_turn);
+int  accel_state_read(const char* path, double** r, int64_t* N, int64_t* turn, int32_t** loss_turn);
+void accel_state_free(void* p);
+
+/*
  * WigTable kick tables (AWigTable, accel.h:403-425; table read/written at accel.cpp:1247-1333).
  * A table is held in a process-wide registry and named from its elements' descriptors by id
  * (f0).  accel_lattice_read / accel_lattice_parse register one table per WigTable entry they read

@@ -145,6 +145,32 @@ def test_reader_agrees_with_reference_deserialize(A, O, LT):
             assert ref.get_field(i, "Phis") == d.f[2]
 
 
+def test_state_checkpoint_roundtrip(A, tmp_path):
+    """Particle states survive a checkpoint bit for bit (lost particles' NaN and codes included),
+    with and without loss turns; a foreign or truncated file is an I/O error."""
+    rng = np.random.default_rng(5)
+    r = rng.normal(0, 1e-3, (1000, 6))
+    r[7, 0], r[7, 4] = np.nan, 3.0
+    lt = rng.integers(-1, 500, 1000).astype(np.int32)
+    p = str(tmp_path / "s.bin")
+    A.write_state(p, r, turn=1234, loss=lt)
+    r2, t2, l2 = A.read_state(p)
+    assert t2 == 1234 and np.array_equal(r2.view(np.int64), r.view(np.int64)) and np.array_equal(l2, lt)
+    A.write_state(p, r[:3])
+    r3, t3, l3 = A.read_state(p)
+    assert t3 == 0 and l3 is None and np.array_equal(r3, r[:3])
+    with open(p, "r+b") as f:
+        f.truncate(40)
+    with pytest.raises(A.AccelError) as ei:
+        A.read_state(p)
+    assert ei.value.status == A.E_IO
+    q = str(tmp_path / "x.txt")
+    open(q, "w").write("not a state file, just text, long enough for a header\n")
+    with pytest.raises(A.AccelError) as ei:
+        A.read_state(q)
+    assert ei.value.status == A.E_IO
+
+
 def test_device_memory_limit_without_a_device(A):
     """The budget is host state: it can be set and read with no device (nothing is held)."""
     assert A.device_memory_held() >= 0

@@ -105,6 +105,31 @@ def test_exact_corrections_reach_their_targets():
     assert abs(p[0] - 0.19) < 2e-5 and abs(p[1] - 0.36) < 2e-5, printed
 
 
+@pytest.mark.gpu
+def test_deck_resumes_bit_for_bit_from_a_binary_checkpoint(tmp_path):
+    """Do_Track save=FILE then "Distribution : Load FILE, format=binary" (extensions of the
+    reference's decks, whose text export keeps six digits): 40 + 60 turns through the checkpoint
+    print the same final coordinates as 100 turns in one go."""
+    ckpt = str(tmp_path / "state.bin")
+    head = ("Lattice\n  file_name = tests/golden/dba18.lat, type=ERING\nEnd\nTrack\n"
+            "  Distribution = Coordinate r=(1e-3, 0, 5e-4, 0, 0, 0; 2e-3, 1e-5, 1e-3, 0, 0, 1e-3; "
+            "-3e-3, 2e-5, 2e-4, 0, 1e-3, -5e-4)\n")
+    one = head + "  Do_Track: radiation=rad, rfcavity=on, nturn=100, printfinal=Full\nEnd\nSTOP\n"
+    two = (head + f"  Do_Track: radiation=rad, rfcavity=on, nturn=40, save={ckpt}\nEnd\nTrack\n"
+           f"  Distribution : Load {ckpt}, format=binary\n"
+           "  Do_Track: radiation=rad, rfcavity=on, nturn=60, printfinal=Full\nEnd\nSTOP\n")
+    outs = []
+    for name, text in (("one", one), ("two", two)):
+        deck = tmp_path / f"{name}.in"
+        deck.write_text(text)
+        out = subprocess.run([EXE, str(deck)], cwd=ROOT, capture_output=True, text=True, timeout=600)
+        assert out.returncode == 0, out.stderr[-2000:]
+        lines = out.stdout.splitlines()
+        k = max(i for i, l in enumerate(lines) if l.startswith("$$$Track-Data: Full export"))
+        outs.append([l.split("\t", 1)[1] for l in lines[k + 2:k + 5]])  # the coordinates, turn column dropped
+    assert outs[0] == outs[1]
+
+
 def test_deck_compare_accepts_reference_against_itself():
     """The comparison's own logic, on the golden outputs alone (no GPU)."""
     for deck in ("dba_deck", "fodo_deck", "ops_deck", "dist_deck"):
