@@ -104,7 +104,7 @@ accel_ctx::~accel_ctx() {
     cudaSetDevice(device);
     graphs.clear();
     for (DevBuf* b : {&state, &aos, &loss, &live0, &cnt, &tables, &tbl_off, &pinst, &scratch,
-                      &iscratch, &probe_state})
+                      &iscratch, &probe_state, &tw_scratch})
         b->release();
     for (cudaEvent_t e : prof_events) cudaEventDestroy(e);
     if (ev0) cudaEventDestroy(ev0);
@@ -330,6 +330,10 @@ static int emit_part(accel_ctx* C, const CoreReq& q, int part, int turns, cudaSt
             launch_longwake_stage(3, P, w, scr, counts, s);
             launches += 4;
             if (r != ncclSuccess && coll_status == ACCEL_OK) coll_status = nccl_fail("ncclAllReduce (wake)", r);
+        } else if (q.mode == ACCEL_MODE_FUSED && C->tw_scratch.p) {
+            // fused mode: the O(N log N) sum (kern_tw.cu); plain and exact keep the pair sum
+            launch_transwake_sorted(P, L0->host_tbl[k], C->tw_scratch.p, C->tw_scratch.bytes, s);
+            launches += 8;
         } else {
             launch_transwake(P, q.tables + k, L0->host_tbl[k], nullptr, s);
             launches += 3;
@@ -427,6 +431,12 @@ static int capture_part(accel_ctx* C, const CoreReq& q, int part, int turns, cud
 static int run_core(accel_ctx* C, const CoreReq& q, cudaStream_t user) {
     int s;
     if ((s = C->live0.ensure(sizeof(int32_t) * std::max<int64_t>(1, q.ntot)))) return s;
+    if (q.mode == ACCEL_MODE_FUSED) {
+        // the transverse wake's sort and scan scratch, sized before any graph is captured
+        bool tw = false;
+        for (int k = q.e0; k < q.e1; k++) tw |= q.lines[0]->desc[k].type == ACCEL_TRANSWAKE;
+        if (tw && (s = C->tw_scratch.ensure(tw_sorted_scratch_bytes(std::max<int64_t>(1, q.ntot))))) return s;
+    }
     if ((s = C->cnt.ensure(sizeof(int32_t) * 16))) return s;
     if ((s = C->scratch.ensure(sizeof(double) * kScratchDoubles))) return s;
     if ((s = C->iscratch.ensure(sizeof(int32_t) * 4096))) return s;

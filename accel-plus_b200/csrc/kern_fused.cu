@@ -506,6 +506,10 @@ __global__ void k_tw_kick(TrackParams P, DevElem e) {
     }
 }
 
+void launch_tw_drift(const TrackParams& p, double half_len, cudaStream_t s) {
+    k_tw_drift<<<296, 256, 0, s>>>(p, half_len);
+}
+
 void launch_transwake(const TrackParams& p, const DevElem* e_dev, const DevElem& e, double* xsnap,
                       cudaStream_t s) {
     (void)e_dev; (void)xsnap;

@@ -54,6 +54,12 @@ void launch_longwake(const TrackParams& p, const DevElem* e_dev, const DevElem& 
 void launch_transwake(const TrackParams& p, const DevElem* e_dev, const DevElem& e_host,
                       double* xsnap, cudaStream_t s);
 size_t longwake_scratch_doubles(int nbins);
+// transverse wake in O(N log N) (kern_tw.cu): z-sorted prefix sums of the factorised resonator
+// wake; scratch from tw_sorted_scratch_bytes(ntot), allocated before any capture
+void launch_tw_drift(const TrackParams& p, double half_len, cudaStream_t s);
+size_t tw_sorted_scratch_bytes(int64_t n);
+void launch_transwake_sorted(const TrackParams& p, const DevElem& e, void* scratch, size_t scratch_bytes,
+                             cudaStream_t s);
 // the longitudinal wake in stages, for runs whose bunch is spread over several GPUs
 struct LwParams { double half, energy, charge, Rs, fr, Q; int nbins; bool on; };
 LwParams longwake_params(const DevElem& e_host);
