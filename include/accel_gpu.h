@@ -134,7 +134,9 @@ typedef struct accel_elem_desc {
 #define ACCEL_F_YLIM        17   /* two values */
 
 /* track modes */
-#define ACCEL_MODE_FUSED  0  /* persistent batched kernel: registers across turns, compaction */
+#define ACCEL_MODE_FUSED  0  /* persistent batched kernel: registers across turns, compaction;
+                                the transverse wake (ATransWake, accel.cpp:1603-1657) as z-sorted
+                                prefix sums, O(N log N), the same sum in another order */
 #define ACCEL_MODE_PLAIN  1  /* one launch per element, state in HBM, reference operation order */
 #define ACCEL_MODE_EXACT  2  /* the plain mode's arithmetic, bit-identical to it, with the state
                                 in registers over whole turns (one launch per 16 turns, or per
