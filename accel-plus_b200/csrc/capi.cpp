@@ -178,7 +178,7 @@ static int check_supported(const accel_line* L, int e0, int e1) {
 // ------------------------------------------------------------------------------------------
 // ---- NCCL, loaded at run time ----------------------------------------------------------------
 // The library links no NCCL; a context that is given a communicator (accel_ctx_set_comm) loads
-// libnccl.so.2 and resolves the five functions it uses.
+// libnccl.so.2 and resolves the six functions it uses.
 struct NcclApi {
     bool ok = false;
     std::string err;
@@ -187,6 +187,7 @@ struct NcclApi {
     ncclResult_t (*CommDestroy)(ncclComm_t) = nullptr;
     ncclResult_t (*AllReduce)(const void*, void*, size_t, ncclDataType_t, ncclRedOp_t, ncclComm_t,
                               cudaStream_t) = nullptr;
+    ncclResult_t (*AllGather)(const void*, void*, size_t, ncclDataType_t, ncclComm_t, cudaStream_t) = nullptr;
     const char* (*GetErrorString)(ncclResult_t) = nullptr;
 };
 
@@ -201,8 +202,10 @@ static NcclApi& nccl() {
         api.CommInitRank = (decltype(api.CommInitRank))dlsym(h, "ncclCommInitRank");
         api.CommDestroy = (decltype(api.CommDestroy))dlsym(h, "ncclCommDestroy");
         api.AllReduce = (decltype(api.AllReduce))dlsym(h, "ncclAllReduce");
+        api.AllGather = (decltype(api.AllGather))dlsym(h, "ncclAllGather");
         api.GetErrorString = (decltype(api.GetErrorString))dlsym(h, "ncclGetErrorString");
-        api.ok = api.GetUniqueId && api.CommInitRank && api.CommDestroy && api.AllReduce && api.GetErrorString;
+        api.ok = api.GetUniqueId && api.CommInitRank && api.CommDestroy && api.AllReduce && api.AllGather &&
+                 api.GetErrorString;
         if (!api.ok) api.err = "libnccl.so.2 lacks a required function";
     });
     return api;
@@ -330,10 +333,24 @@ static int emit_part(accel_ctx* C, const CoreReq& q, int part, int turns, cudaSt
             launch_longwake_stage(3, P, w, scr, counts, s);
             launches += 4;
             if (r != ncclSuccess && coll_status == ACCEL_OK) coll_status = nccl_fail("ncclAllReduce (wake)", r);
-        } else if (q.mode == ACCEL_MODE_FUSED && C->tw_scratch.p) {
-            // fused mode: the O(N log N) sum (kern_tw.cu); plain and exact keep the pair sum
-            launch_transwake_sorted(P, L0->host_tbl[k], C->tw_scratch.p, C->tw_scratch.bytes, s);
-            launches += 8;
+        } else if (q.mode == ACCEL_MODE_FUSED) {
+            // fused mode: the O(N log N) sum (kern_tw.cu), over all ranks' particles when a
+            // communicator is set; plain and exact keep the pair sum
+            const DevElem& e = L0->host_tbl[k];
+            const bool gather = C->comm != nullptr;
+            const TwLayout t = tw_layout(C->tw_scratch.p, C->tw_slots, gather ? C->nranks : 1, gather);
+            launch_transwake_sorted_stage(1, P, e, t, gather ? C->rank : 0, C->tw_ntot_all, s);
+            if (gather && e.flags) {
+                ncclComm_t cm = (ncclComm_t)C->comm;
+                const size_t m = (size_t)t.slots;
+                ncclResult_t r = nccl().AllGather(t.key_s, t.key_g, m, ncclFloat64, cm, s);
+                if (r == ncclSuccess) r = nccl().AllGather(t.x_s, t.x_g, m, ncclFloat64, cm, s);
+                if (r == ncclSuccess) r = nccl().AllGather(t.y_s, t.y_g, m, ncclFloat64, cm, s);
+                if (r == ncclSuccess) r = nccl().AllReduce(t.nvalid, t.nvalid + 1, 1, ncclInt32, ncclSum, cm, s);
+                if (r != ncclSuccess && coll_status == ACCEL_OK) coll_status = nccl_fail("nccl (transverse wake)", r);
+            }
+            launch_transwake_sorted_stage(2, P, e, t, gather ? C->rank : 0, C->tw_ntot_all, s);
+            launches += (e.flags ? 7 : 0) + (e.v[V_LEN] != 0 ? 2 : 0);
         } else {
             launch_transwake(P, q.tables + k, L0->host_tbl[k], nullptr, s);
             launches += 3;
@@ -431,14 +448,38 @@ static int capture_part(accel_ctx* C, const CoreReq& q, int part, int turns, cud
 static int run_core(accel_ctx* C, const CoreReq& q, cudaStream_t user) {
     int s;
     if ((s = C->live0.ensure(sizeof(int32_t) * std::max<int64_t>(1, q.ntot)))) return s;
-    if (q.mode == ACCEL_MODE_FUSED) {
-        // the transverse wake's sort and scan scratch, sized before any graph is captured
-        bool tw = false;
-        for (int k = q.e0; k < q.e1; k++) tw |= q.lines[0]->desc[k].type == ACCEL_TRANSWAKE;
-        if (tw && (s = C->tw_scratch.ensure(tw_sorted_scratch_bytes(std::max<int64_t>(1, q.ntot))))) return s;
-    }
     if ((s = C->cnt.ensure(sizeof(int32_t) * 16))) return s;
     if ((s = C->scratch.ensure(sizeof(double) * kScratchDoubles))) return s;
+    bool tw = false;
+    for (int k = q.e0; k < q.e1; k++) tw |= q.lines[0]->desc[k].type == ACCEL_TRANSWAKE;
+    if (tw && C->comm && C->nranks > 1 && q.mode != ACCEL_MODE_FUSED)
+        return fail(ACCEL_E_UNSUPPORTED, "the pair-sum transverse wake of the plain and exact modes acts within "
+                                         "one rank; a bunch spread over ranks takes the fused mode");
+    if (tw && q.mode == ACCEL_MODE_FUSED) {
+        // the transverse wake's entries per rank and the particles of all ranks (exchanged when a
+        // communicator is set: every rank takes this step, same lattice), then its sort and scan
+        // scratch, sized before any graph is captured
+        int64_t slots = q.ntot, all = q.ntot;
+        if (C->comm) {
+            int64_t* d = (int64_t*)C->scratch.p;
+            int64_t h[2] = {q.ntot, q.ntot};
+            CK(cudaMemcpyAsync(d, h, sizeof h, cudaMemcpyHostToDevice, C->stream));
+            ncclComm_t cm = (ncclComm_t)C->comm;
+            ncclResult_t r = nccl().AllReduce(d, d, 1, ncclInt64, ncclMax, cm, C->stream);
+            if (r == ncclSuccess) r = nccl().AllReduce(d + 1, d + 1, 1, ncclInt64, ncclSum, cm, C->stream);
+            if (r != ncclSuccess) return nccl_fail("ncclAllReduce (transverse wake sizes)", r);
+            CK(cudaMemcpyAsync(h, d, sizeof h, cudaMemcpyDeviceToHost, C->stream));
+            CK(cudaStreamSynchronize(C->stream));
+            slots = h[0];
+            all = h[1];
+        }
+        const int nr = C->comm ? C->nranks : 1;
+        if (std::max<int64_t>(1, slots) * nr > INT32_MAX)
+            return fail(ACCEL_E_TOO_LARGE, "transverse wake: more than 2^31 entries over all ranks");
+        C->tw_slots = std::max<int64_t>(1, slots);
+        C->tw_ntot_all = all;
+        if ((s = C->tw_scratch.ensure(tw_sorted_scratch_bytes(C->tw_slots, nr, C->comm != nullptr)))) return s;
+    }
     if ((s = C->iscratch.ensure(sizeof(int32_t) * 4096))) return s;
     if (q.variant < 0 || q.variant >= kNumFusedVariants) return fail(ACCEL_E_INVALID, "bad variant");
     if (C->bps[q.variant] == 0) {
@@ -482,6 +523,7 @@ static int run_core(accel_ctx* C, const CoreReq& q, cudaStream_t user) {
                  (int64_t)(intptr_t)q.tables, (int64_t)(intptr_t)q.tbl_off, (int64_t)(intptr_t)q.pinst,
                  (int64_t)q.probe, (int64_t)(intptr_t)C->live0.p, (int64_t)(intptr_t)C->cnt.p,
                  (int64_t)(intptr_t)C->scratch.p, (int64_t)(intptr_t)C->iscratch.p,
+                 (int64_t)(intptr_t)C->tw_scratch.p, (int64_t)C->tw_scratch.bytes, C->tw_slots, C->tw_ntot_all,
                  (int64_t)(intptr_t)C->comm};
         for (int i = 0; i < q.ninst && i < 4; i++) {
             key.v.push_back((int64_t)(intptr_t)q.lines[i]);
@@ -641,6 +683,7 @@ int accel_ctx_set_comm(accel_ctx* C, const unsigned char* id, int nranks, int ra
         api.CommDestroy((ncclComm_t)C->comm);
         C->comm = nullptr;
         C->nranks = 1;
+        C->rank = 0;
     }
     C->graphs.clear();
     ncclUniqueId u;
@@ -650,6 +693,7 @@ int accel_ctx_set_comm(accel_ctx* C, const unsigned char* id, int nranks, int ra
     if (r != ncclSuccess) return nccl_fail("ncclCommInitRank", r);
     C->comm = cm;
     C->nranks = nranks;
+    C->rank = rank;
     return ACCEL_OK;
 }
 

@@ -13,9 +13,14 @@
 // of operations; where ax (z_max - z_min) would make E_j overflow (above 600), each particle takes
 // the pair sum instead.  The plain and exact modes keep the reference's pair sum
 // (kern_fused.cu), whose order of operations they reproduce.
+//
+// A bunch spread over several GPUs: every rank offers the same number of entries (slots, at least
+// its particle count; z = -inf marks an empty one), the entries of all ranks are all-gathered
+// between the two stages, every rank sorts and scans the whole list and kicks its own particles;
+// the charge per particle is Ne over the particles of all ranks.
 #include <cuda_runtime.h>
 #include <cub/device/device_radix_sort.cuh>
-#include <cub/device/device_scan.cuh>
+#include <cub/block/block_scan.cuh>
 #include <cstdint>
 #include <cmath>
 #include <algorithm>
@@ -34,6 +39,55 @@ struct Quad4Sum {
         return Quad4{a.cx + b.cx, a.sx + b.sx, a.cy + b.cy, a.sy + b.sy};
     }
 };
+
+// The prefix sums in a fixed order of additions, so that a run is reproducible bit for bit (a
+// decoupled look-back scan adds its partial sums in an order that depends on timing): within a
+// tile of 1024 entries each thread sums its 4 in order and a block scan combines the threads;
+// one block scans the tile totals (each thread a contiguous run of them, in order); the kick adds
+// its tile's offset to the entry's in-tile prefix.
+constexpr int kScanThreads = 256, kScanItems = 4, kScanTile = kScanThreads * kScanItems;
+constexpr int kTileScanThreads = 1024;
+
+__global__ void __launch_bounds__(kScanThreads) k_tw_scan_tiles(const Quad4* in, Quad4* out, Quad4* tile_sum,
+                                                                int64_t total) {
+    using BS = cub::BlockScan<Quad4, kScanThreads>;
+    __shared__ typename BS::TempStorage ts;
+    const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+    Quad4 v[kScanItems];
+    Quad4 acc{0, 0, 0, 0};
+#pragma unroll
+    for (int j = 0; j < kScanItems; j++) {
+        const int64_t i = base + j;
+        const Quad4 x = i < total ? in[i] : Quad4{0, 0, 0, 0};
+        acc = j == 0 ? x : Quad4Sum()(acc, x);
+        v[j] = acc;
+    }
+    Quad4 excl, agg;
+    BS(ts).ExclusiveScan(acc, excl, Quad4{0, 0, 0, 0}, Quad4Sum(), agg);
+#pragma unroll
+    for (int j = 0; j < kScanItems; j++) {
+        const int64_t i = base + j;
+        if (i < total) out[i] = threadIdx.x == 0 ? v[j] : Quad4Sum()(excl, v[j]);
+    }
+    if (threadIdx.x == 0) tile_sum[blockIdx.x] = agg;
+}
+
+// in place: tile totals -> exclusive tile offsets
+__global__ void __launch_bounds__(kTileScanThreads) k_tw_scan_tile_sums(Quad4* tile_sum, int64_t ntiles) {
+    using BS = cub::BlockScan<Quad4, kTileScanThreads>;
+    __shared__ typename BS::TempStorage ts;
+    const int64_t per = (ntiles + kTileScanThreads - 1) / kTileScanThreads;
+    const int64_t b0 = (int64_t)threadIdx.x * per, b1 = b0 + per < ntiles ? b0 + per : ntiles;
+    Quad4 acc{0, 0, 0, 0};
+    for (int64_t b = b0; b < b1; b++) acc = b == b0 ? tile_sum[b] : Quad4Sum()(acc, tile_sum[b]);
+    Quad4 run, agg;
+    BS(ts).ExclusiveScan(acc, run, Quad4{0, 0, 0, 0}, Quad4Sum(), agg);
+    for (int64_t b = b0; b < b1; b++) {
+        const Quad4 t = tile_sum[b];
+        tile_sum[b] = run;
+        run = b == 0 ? t : Quad4Sum()(run, t);
+    }
+}
 
 struct TwConst {
     double q, energy, Wx, Wy, ax, ay, kbx, kby;
@@ -54,32 +108,48 @@ __host__ __device__ TwConst tw_const(const DevElem& e, int64_t n) {
     return c;
 }
 
-// sort keys: z of each live particle (-inf for one lost before the wake, sorted last)
-__global__ void k_tw_keys(const TrackParams P, double* keys, int32_t* vals, int32_t* nvalid) {
+// this rank's entries: slot i < nlive holds live particle live[i] (z, x, y), z = -inf when it was
+// lost before the wake; slots past nlive hold -inf.  Also the entry indices of all ranks' entries.
+__global__ void k_tw_entries(const TrackParams P, double* key, double* xs, double* ys, int64_t slots,
+                             int32_t* val, int64_t total, int32_t* nvalid_local) {
     const int nlive = *P.nlive;
     const int64_t n = P.ntot;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nlive; i += gridDim.x * blockDim.x) {
-        const int p = P.live[i];
-        const double x = P.st[p];
-        const bool ok = !(x != x);
-        keys[i] = ok ? P.st[4 * n + p] : -INFINITY;
-        vals[i] = p;
-        if (ok) atomicAdd(nvalid, 1);
+    const int64_t m = slots > total ? slots : total;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x) {
+        if (i < total) val[i] = (int32_t)i;
+        if (i >= slots) continue;
+        bool ok = false;
+        double z = -INFINITY, x = 0, y = 0;
+        if (i < nlive) {
+            const int p = P.live[i];
+            x = P.st[p];
+            ok = !(x != x);
+            if (ok) {
+                z = P.st[4 * n + p];
+                y = P.st[2 * n + p];
+            } else {
+                x = 0;
+            }
+        }
+        key[i] = z;
+        xs[i] = x;
+        ys[i] = y;
+        const unsigned act = __activemask();
+        const unsigned b = __ballot_sync(act, ok);
+        if ((threadIdx.x & 31) == __ffs(act) - 1 && b) atomicAdd(nvalid_local, __popc(b));
     }
 }
 
-// per sorted position: the particle's four terms E cos x, E sin x (and in y), zero when lost
-__global__ void k_tw_terms(const TrackParams P, const double* keys, const int32_t* vals, const int32_t* nvalid,
-                           TwConst c, Quad4* terms) {
+// per sorted position: the entry's four terms E cos x, E sin x (and in y), zero past the valid ones
+__global__ void k_tw_terms(const double* key, const int32_t* val, const double* xg, const double* yg,
+                           const int32_t* nvalid, int64_t total, TwConst c, Quad4* terms) {
     const int nv = *nvalid;
-    const int64_t n = P.ntot;
-    const double zr = nv > 0 ? keys[0] : 0.0;
-    // every one of the ntot entries the scan reads: zero past the valid ones
-    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+    const double zr = nv > 0 ? key[0] : 0.0;
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < total; k += (int64_t)gridDim.x * blockDim.x) {
         Quad4 t{0, 0, 0, 0};
         if (k < nv) {
-            const int p = vals[k];
-            const double z = keys[k], x = P.st[p], y = P.st[2 * n + p];
+            const int g = val[k];
+            const double z = key[k], x = xg[g], y = yg[g];
             const double ex = exp(c.ax * (zr - z)), ey = exp(c.ay * (zr - z));
             double sx, cx, sy, cy;
             sincos(c.kbx * z, &sx, &cx);
@@ -90,29 +160,36 @@ __global__ void k_tw_terms(const TrackParams P, const double* keys, const int32_
     }
 }
 
-// kick of sorted position k from the prefix sums (or, when the z range is too long for the
-// factorisation, from the pair sum over the sorted list)
-__global__ void k_tw_kick_sorted(const TrackParams P, const double* keys, const int32_t* vals,
-                                 const int32_t* nvalid, TwConst c, const Quad4* terms, const Quad4* prefix) {
+// kick of the sorted entries that are this rank's particles, from the prefix sums (or, when the z
+// range is too long for the factorisation, from the pair sum over the sorted entries)
+__global__ void k_tw_kick_sorted(const TrackParams P, const double* key, const int32_t* val, const double* xg,
+                                 const double* yg, const int32_t* nvalid, int64_t slots, int rank, TwConst c,
+                                 const Quad4* terms, const Quad4* prefix, const Quad4* tile_off) {
     const int nv = *nvalid;
+    const int nlive = *P.nlive;
     const int64_t n = P.ntot;
     if (nv == 0) return;
-    const double zr = keys[0], zmin = keys[nv - 1];
+    const double zr = key[0], zmin = key[nv - 1];
     const bool factor = c.ax * (zr - zmin) <= 600.0 && c.ay * (zr - zmin) <= 600.0;
     const double scale = c.q / c.energy / 1.0e6;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nv; k += gridDim.x * blockDim.x) {
-        const int p = vals[k];
-        const double zi = keys[k];
+        const int64_t g = val[k];
+        // this rank's live slots only (a slot past nlive can sort among the first nv only when a
+        // live particle carries a non-finite z)
+        if (g / slots != rank || g - (int64_t)rank * slots >= nlive) continue;
+        const int p = P.live[g - (int64_t)rank * slots];
+        const double zi = key[k];
         double dxp, dyp;
         if (factor) {
             // last position whose z >= zi: the end of zi's group in the descending order
             int lo = k, hi = nv - 1;
             while (lo < hi) {
                 const int mid = (lo + hi + 1) >> 1;
-                if (keys[mid] >= zi) lo = mid;
+                if (key[mid] >= zi) lo = mid;
                 else hi = mid - 1;
             }
-            const Quad4 a = prefix[lo], own = terms[k];
+            const int tile = lo / kScanTile;
+            const Quad4 a = tile == 0 ? prefix[lo] : Quad4Sum()(tile_off[tile], prefix[lo]), own = terms[k];
             const double Cx = a.cx - own.cx, Sx = a.sx - own.sx, Cy = a.cy - own.cy, Sy = a.sy - own.sy;
             double sx, cx, sy, cy;
             sincos(c.kbx * zi, &sx, &cx);
@@ -122,12 +199,12 @@ __global__ void k_tw_kick_sorted(const TrackParams P, const double* keys, const 
         } else {
             dxp = 0;
             dyp = 0;
-            for (int j = 0; j < nv && keys[j] >= zi; j++) {
+            for (int j = 0; j < nv && key[j] >= zi; j++) {
                 if (j == k) continue;
-                const int pj = vals[j];
-                const double zij = zi - keys[j];
-                dxp -= c.q * c.Wx * exp(c.ax * zij) * sin(c.kbx * zij) * P.st[pj] / c.energy / 1.0e6;
-                dyp -= c.q * c.Wy * exp(c.ay * zij) * sin(c.kby * zij) * P.st[2 * n + pj] / c.energy / 1.0e6;
+                const int gj = val[j];
+                const double zij = zi - key[j];
+                dxp -= c.q * c.Wx * exp(c.ax * zij) * sin(c.kbx * zij) * xg[gj] / c.energy / 1.0e6;
+                dyp -= c.q * c.Wy * exp(c.ay * zij) * sin(c.kby * zij) * yg[gj] / c.energy / 1.0e6;
             }
         }
         P.st[n + p] += dxp * (1 + P.st[5 * n + p]);
@@ -135,58 +212,84 @@ __global__ void k_tw_kick_sorted(const TrackParams P, const double* keys, const 
     }
 }
 
-__global__ void k_tw_zero(int32_t* c) { *c = 0; }
-__global__ void k_tw_fill(double* a, double v, int64_t n) {
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        a[i] = v;
+__global__ void k_tw_zero(int32_t* c) { c[0] = 0; c[1] = 0; }
+
+// carves the scratch (base may be null: offsets only); returns the bytes used
+size_t carve(char* base, int64_t slots, int nranks, bool gather, TwLayout& t) {
+    const int64_t total = slots * nranks;
+    size_t off = 0;
+    auto take = [&](size_t b) {
+        char* p = base ? base + off : nullptr;
+        off += (b + 255) / 256 * 256;
+        return p;
+    };
+    t.slots = slots;
+    t.total = total;
+    t.key_g = (double*)take(sizeof(double) * total);
+    t.x_g = (double*)take(sizeof(double) * total);
+    t.y_g = (double*)take(sizeof(double) * total);
+    if (gather) {
+        t.key_s = (double*)take(sizeof(double) * slots);
+        t.x_s = (double*)take(sizeof(double) * slots);
+        t.y_s = (double*)take(sizeof(double) * slots);
+    } else {
+        t.key_s = t.key_g;
+        t.x_s = t.x_g;
+        t.y_s = t.y_g;
+    }
+    t.key_sorted = (double*)take(sizeof(double) * total);
+    t.val_in = (int32_t*)take(sizeof(int32_t) * total);
+    t.val_sorted = (int32_t*)take(sizeof(int32_t) * total);
+    t.terms = take(sizeof(Quad4) * total);
+    t.prefix = take(sizeof(Quad4) * total);
+    t.tile_off = take(sizeof(Quad4) * ((total + kScanTile - 1) / kScanTile));
+    t.nvalid = (int32_t*)take(16);
+    t.tmp = base ? base + off : nullptr;
+    size_t sort_tmp = 0;
+    cub::DeviceRadixSort::SortPairsDescending(nullptr, sort_tmp, (const double*)nullptr, (double*)nullptr,
+                                              (const int32_t*)nullptr, (int32_t*)nullptr, (int)total);
+    t.tmp_bytes = sort_tmp;
+    return off + t.tmp_bytes;
 }
 }  // namespace
 
-size_t tw_sorted_scratch_bytes(int64_t n) {
-    size_t sort_tmp = 0, scan_tmp = 0;
-    cub::DeviceRadixSort::SortPairsDescending(nullptr, sort_tmp, (const double*)nullptr, (double*)nullptr,
-                                              (const int32_t*)nullptr, (int32_t*)nullptr, (int)n);
-    cub::DeviceScan::InclusiveScan(nullptr, scan_tmp, (const Quad4*)nullptr, (Quad4*)nullptr, Quad4Sum(), (int)n);
-    const size_t a = 256;
-    auto up = [&](size_t b) { return (b + a - 1) / a * a; };
-    return up(2 * n * sizeof(double)) + up(2 * n * sizeof(int32_t)) + up(2 * n * sizeof(Quad4)) + up(16) +
-           up(std::max(sort_tmp, scan_tmp));
+size_t tw_sorted_scratch_bytes(int64_t slots, int nranks, bool gather) {
+    TwLayout t;
+    return carve(nullptr, std::max<int64_t>(1, slots), nranks, gather, t);
 }
 
-void launch_transwake_sorted(const TrackParams& p, const DevElem& e, void* scratch, size_t scratch_bytes,
-                             cudaStream_t s) {
-    const int64_t n = p.ntot;
-    const size_t a = 256;
-    auto up = [&](size_t b) { return (b + a - 1) / a * a; };
-    char* base = (char*)scratch;
-    double* keys_in = (double*)base;
-    double* keys_out = keys_in + n;
-    base += up(2 * n * sizeof(double));
-    int32_t* vals_in = (int32_t*)base;
-    int32_t* vals_out = vals_in + n;
-    base += up(2 * n * sizeof(int32_t));
-    Quad4* terms = (Quad4*)base;
-    Quad4* prefix = terms + n;
-    base += up(2 * n * sizeof(Quad4));
-    int32_t* nvalid = (int32_t*)base;
-    base += up(16);
-    void* tmp = base;
-    size_t tmp_bytes = scratch_bytes - (size_t)(base - (char*)scratch);
-    const TwConst c = tw_const(e, n);
+TwLayout tw_layout(void* scratch, int64_t slots, int nranks, bool gather) {
+    TwLayout t;
+    carve((char*)scratch, std::max<int64_t>(1, slots), nranks, gather, t);
+    return t;
+}
+
+void launch_transwake_sorted_stage(int stage, const TrackParams& p, const DevElem& e, const TwLayout& t,
+                                   int rank, int64_t ntot_all, cudaStream_t s) {
     const double half = 0.5 * e.v[V_LEN];
-    // with length: the half drifts around the kick, as the pair-sum path
-    if (half != 0) launch_tw_drift(p, half, s);
+    const TwConst c = tw_const(e, ntot_all);
+    // with gathered entries the total count is nvalid[1], else this rank's nvalid[0]
+    const int32_t* nv = t.key_s != t.key_g ? t.nvalid + 1 : t.nvalid;
+    if (stage == 1) {
+        // with length: the half drifts around the kick, as the pair-sum path
+        if (half != 0) launch_tw_drift(p, half, s);
+        if (!e.flags) return;
+        k_tw_zero<<<1, 1, 0, s>>>(t.nvalid);
+        k_tw_entries<<<296, 256, 0, s>>>(p, t.key_s, t.x_s, t.y_s, t.slots, t.val_in, t.total, t.nvalid);
+        return;
+    }
     if (e.flags) {
-        k_tw_zero<<<1, 1, 0, s>>>(nvalid);
-        // the live count is on the device: size every pass for all ntot entries (entries past
-        // nlive are not read; the sort and scan run over ntot, with keys -inf past nlive)
-        k_tw_fill<<<296, 256, 0, s>>>(keys_in, -INFINITY, n);
-        k_tw_keys<<<296, 256, 0, s>>>(p, keys_in, vals_in, nvalid);
-        cub::DeviceRadixSort::SortPairsDescending(tmp, tmp_bytes, keys_in, keys_out, vals_in, vals_out, (int)n, 0,
-                                                  64, s);
-        k_tw_terms<<<296, 256, 0, s>>>(p, keys_out, vals_out, nvalid, c, terms);
-        cub::DeviceScan::InclusiveScan(tmp, tmp_bytes, terms, prefix, Quad4Sum(), (int)n, s);
-        k_tw_kick_sorted<<<296, 256, 0, s>>>(p, keys_out, vals_out, nvalid, c, terms, prefix);
+        size_t tmp_bytes = t.tmp_bytes;
+        cub::DeviceRadixSort::SortPairsDescending(t.tmp, tmp_bytes, t.key_g, t.key_sorted, t.val_in, t.val_sorted,
+                                                  (int)t.total, 0, 64, s);
+        k_tw_terms<<<296, 256, 0, s>>>(t.key_sorted, t.val_sorted, t.x_g, t.y_g, nv, t.total, c, (Quad4*)t.terms);
+        const int64_t ntiles = (t.total + kScanTile - 1) / kScanTile;
+        k_tw_scan_tiles<<<(unsigned)ntiles, kScanThreads, 0, s>>>((const Quad4*)t.terms, (Quad4*)t.prefix,
+                                                                 (Quad4*)t.tile_off, t.total);
+        k_tw_scan_tile_sums<<<1, kTileScanThreads, 0, s>>>((Quad4*)t.tile_off, ntiles);
+        k_tw_kick_sorted<<<296, 256, 0, s>>>(p, t.key_sorted, t.val_sorted, t.x_g, t.y_g, nv, t.slots, rank, c,
+                                             (const Quad4*)t.terms, (const Quad4*)t.prefix,
+                                             (const Quad4*)t.tile_off);
     }
     if (half != 0) launch_tw_drift(p, half, s);
 }

@@ -55,11 +55,31 @@ void launch_transwake(const TrackParams& p, const DevElem* e_dev, const DevElem&
                       double* xsnap, cudaStream_t s);
 size_t longwake_scratch_doubles(int nbins);
 // transverse wake in O(N log N) (kern_tw.cu): z-sorted prefix sums of the factorised resonator
-// wake; scratch from tw_sorted_scratch_bytes(ntot), allocated before any capture
+// wake.  Each rank offers `slots` entries (z, x, y; z = -inf for none), at least its particle
+// count and the same on every rank; the sum runs over all ranks' entries (`nranks` x `slots`),
+// gathered between the two stages, with the charge per particle Ne / ntot_all.  Scratch from
+// tw_sorted_scratch_bytes, allocated before any capture.
+struct TwLayout {
+    int64_t slots, total;             // entries per rank, over all ranks
+    double *key_s, *x_s, *y_s;        // this rank's entries (gather send buffers)
+    double *key_g, *x_g, *y_g;        // all ranks' entries (gather receive buffers)
+    double* key_sorted;
+    int32_t *val_in, *val_sorted;     // entry index, rank * slots + slot
+    void *terms, *prefix;             // four weighted sums per sorted entry, their in-tile scan
+    void* tile_off;                   // and the tiles' offsets
+    int32_t* nvalid;                  // [0] this rank's live entries, [1] all ranks'
+    void* tmp;
+    size_t tmp_bytes;
+};
+// gather: the entries are exchanged between the stages (a communicator is set); without it the
+// rank's entries are the whole list
+size_t tw_sorted_scratch_bytes(int64_t slots, int nranks, bool gather);
+TwLayout tw_layout(void* scratch, int64_t slots, int nranks, bool gather);
 void launch_tw_drift(const TrackParams& p, double half_len, cudaStream_t s);
-size_t tw_sorted_scratch_bytes(int64_t n);
-void launch_transwake_sorted(const TrackParams& p, const DevElem& e, void* scratch, size_t scratch_bytes,
-                             cudaStream_t s);
+// stage 1: first half drift, this rank's entries; stage 2 (after the gather): sort, scan, kick
+// of this rank's particles, second half drift
+void launch_transwake_sorted_stage(int stage, const TrackParams& p, const DevElem& e, const TwLayout& t,
+                                   int rank, int64_t ntot_all, cudaStream_t s);
 // the longitudinal wake in stages, for runs whose bunch is spread over several GPUs
 struct LwParams { double half, energy, charge, Rs, fr, Q; int nbins; bool on; };
 LwParams longwake_params(const DevElem& e_host);

@@ -67,6 +67,9 @@ struct accel_ctx {
     std::vector<cudaEvent_t> prof_events;  // [begin, end] per tracking launch, then whole call
     void* comm = nullptr;                  // NCCL communicator of a bunch spread over GPUs
     int nranks = 1;
+    int rank = 0;
+    int64_t tw_slots = 0;                  // transverse wake: entries per rank (max particles)
+    int64_t tw_ntot_all = 0;               // and the particles of all ranks, set per run
     ~accel_ctx();
 };
 
