@@ -66,6 +66,17 @@ extern "C" int accel_state_read(const char* path, double** r, int64_t* n, int64_
         std::fclose(f);
         return fail(ACCEL_E_IO, std::string("not a particle-state file (version 1): ") + path);
     }
+    // the particle count must match the file's length (also bounds the sizes computed from it)
+    const int64_t per = (int64_t)sizeof(double) * 6 + ((h.flags & 1u) ? (int64_t)sizeof(int32_t) : 0);
+    int64_t body = -1;
+    if (std::fseek(f, 0, SEEK_END) == 0) {
+        const long end = std::ftell(f);
+        if (end >= (long)sizeof(h)) body = (int64_t)end - (int64_t)sizeof(h);
+    }
+    if (body < 0 || std::fseek(f, (long)sizeof(h), SEEK_SET) != 0 || h.n > body / per || h.n * per != body) {
+        std::fclose(f);
+        return fail(ACCEL_E_IO, std::string("particle-state file length does not match its particle count: ") + path);
+    }
     double* rr = (double*)std::malloc(sizeof(double) * 6 * (size_t)std::max<int64_t>(1, h.n));
     int32_t* ll = (h.flags & 1u) ? (int32_t*)std::malloc(sizeof(int32_t) * (size_t)std::max<int64_t>(1, h.n))
                                  : nullptr;

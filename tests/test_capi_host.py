@@ -164,6 +164,15 @@ def test_state_checkpoint_roundtrip(A, tmp_path):
     with pytest.raises(A.AccelError) as ei:
         A.read_state(p)
     assert ei.value.status == A.E_IO
+    # a header whose particle count disagrees with the file's length (here one that would overflow
+    # the byte count) is refused before anything is allocated
+    A.write_state(p, r[:3])
+    with open(p, "r+b") as f:
+        f.seek(16)
+        f.write(np.int64(2**61).tobytes())
+    with pytest.raises(A.AccelError) as ei:
+        A.read_state(p)
+    assert ei.value.status == A.E_IO
     q = str(tmp_path / "x.txt")
     open(q, "w").write("not a state file, just text, long enough for a header\n")
     with pytest.raises(A.AccelError) as ei:
