@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--wake-only", action="store_true",
                     help="time the bunch workload with its per-turn wake (2^20 particles) and exit")
     ap.add_argument("--wake-turns", type=int, default=200)
+    ap.add_argument("--transwake-only", action="store_true",
+                    help="time the transverse wake (sorted prefix sum against the pair sum) and exit")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--small", action="store_true",
                     help="profiling case: 16 copies, 20 turns, one step (for ncu)")
@@ -557,6 +559,58 @@ def wake_leg(A, LT, ctx, nturn: int = 200, n: int = 1 << 20) -> dict:
             "timing": "CUDA events on the launching stream, state resident on the device"}
 
 
+def transwake_leg(A, ctx, sizes=(65536, 1 << 20), pair_n: int = 65536) -> dict:
+    """The transverse resonator wake (ATransWake: 3 GeV, Ne 2, Wx 50 / fRx 10 GHz / Qx 1.5,
+    Wy 40 / fRy 12 GHz / Qy 2, 0.5 m) between two drifts, on a Gaussian bunch (x 1 mm, y 0.5 mm,
+    z 3 mm, delta 1e-3): the fused mode's z-sorted prefix sum at each size, the plain mode's pair
+    sum (the reference's O(N^2) order of operations) at `pair_n`, and their agreement after one
+    pass there.  CUDA events on the launching stream, state resident on the device (SoA)."""
+    import torch
+    tw = A.elem(A.TRANSWAKE, "TW", 0.5, f=[3000, 2.0, 50.0, 10.0, 1.5, 40.0, 12.0, 2.0], flags=1)
+    line = A.Line(ctx, [A.elem(A.DRIFT, "D", 0.3), tw, A.elem(A.DRIFT, "D", 0.2)])
+    s = torch.cuda.current_stream()
+
+    def bunch(n):
+        rng = np.random.default_rng(3)
+        r = np.zeros((6, n))
+        r[0] = rng.normal(0, 1e-3, n)
+        r[2] = rng.normal(0, 5e-4, n)
+        r[4] = rng.normal(0, 3e-3, n)
+        r[5] = rng.normal(0, 1e-3, n)
+        return torch.tensor(r, device="cuda", dtype=torch.float64).contiguous()
+
+    def timed(st, mode, turns):
+        line.track(st, 3, layout=A.LAYOUT_SOA, mode=mode, stream=s.cuda_stream)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        line.track(st, turns, layout=A.LAYOUT_SOA, mode=mode, stream=s.cuda_stream)
+        e1.record(s)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / turns
+
+    out = {"workload": "transverse resonator wake between two drifts, Gaussian bunch", "sorted": {}}
+    for n in sizes:
+        out["sorted"][str(n)] = {"ms_per_pass": timed(bunch(n), A.MODE_FUSED, 20)}
+    out["pair"] = {str(pair_n): {"ms_per_pass": timed(bunch(pair_n), A.MODE_PLAIN, 3)}}
+    r0 = bunch(pair_n)
+    a, b = r0.clone(), r0.clone()
+    line.track(a, 1, layout=A.LAYOUT_SOA, mode=A.MODE_PLAIN, stream=s.cuda_stream)
+    line.track(b, 1, layout=A.LAYOUT_SOA, mode=A.MODE_FUSED, stream=s.cuda_stream)
+    torch.cuda.synchronize()
+    kick = (a[1] - r0[1]).abs().max().item()
+    out["sorted_vs_pair_rel"] = (b[1] - a[1]).abs().max().item() / kick
+    out["timing"] = "CUDA events on the launching stream, 20 passes (sorted) / 3 (pair) after 3 warm-up"
+    return out
+
+
+def transwake_only():
+    A = importlib.import_module("accel-plus_b200")
+    ctx = A.Context(0)
+    print(json.dumps({"transwake": transwake_leg(A, ctx)}), flush=True)
+    ctx.close()
+
+
 def wake_only(turns: int, variant: int = -1):
     A = importlib.import_module("accel-plus_b200")
     LT = importlib.import_module("accel-plus_b200.lattices")
@@ -584,6 +638,9 @@ def main():
         return
     if args.wake_only:
         wake_only(args.wake_turns, args.variant)
+        return
+    if args.transwake_only:
+        transwake_only()
         return
     if args.impl == "reference":
         reference_arm(args)
