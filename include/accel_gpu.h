@@ -164,7 +164,9 @@ int  accel_ctx_destroy(accel_ctx* ctx);
  * to the other ranks (e.g. over torch.distributed); every rank then calls accel_ctx_set_comm with
  * the same id.  From then on each longitudinal wake element of the context's tracking exchanges
  * the bunch's z range, live count and bin counts over NCCL, so every rank kicks its particles
- * with the whole bunch's wake.  libnccl.so.2 is loaded at run time; without it both calls return
+ * with the whole bunch's wake; each transverse wake element (fused mode) all-gathers every rank's
+ * (z, x, y) and sums over the whole bunch (the plain and exact modes' pair sum acts within a rank:
+ * ACCEL_E_UNSUPPORTED with more than one).  libnccl.so.2 is loaded at run time; without it both calls return
  * ACCEL_E_UNSUPPORTED.  A process holds one libnccl.so.2: where another component (PyTorch) links
  * its own, load that component first and the library uses its copy.  accel_ctx_set_comm blocks
  * until all nranks ranks have called it.  Every rank must then issue the same tracking calls in
