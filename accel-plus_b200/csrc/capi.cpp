@@ -350,7 +350,8 @@ static int emit_part(accel_ctx* C, const CoreReq& q, int part, int turns, cudaSt
                 if (r != ncclSuccess && coll_status == ACCEL_OK) coll_status = nccl_fail("nccl (transverse wake)", r);
             }
             launch_transwake_sorted_stage(2, P, e, t, gather ? C->rank : 0, C->tw_ntot_all, s);
-            launches += (e.flags ? 7 : 0) + (e.v[V_LEN] != 0 ? 2 : 0);
+            // this library's kernels (the radix sort's are CUB's, not counted)
+            launches += (e.flags ? 6 : 0) + (e.v[V_LEN] != 0 ? 2 : 0);
         } else {
             launch_transwake(P, q.tables + k, L0->host_tbl[k], nullptr, s);
             launches += 3;
