@@ -316,6 +316,25 @@ def test_transverse_wake_sorted_sum_matches_pair_sum(A, ctx, spread):
         assert np.max(np.abs(b[live, k] - a[live, k])) < 1e-10 * kick.max(), k
 
 
+def test_transverse_wake_ring_fused_matches_plain(A, ctx, LT):
+    """The sorted transverse wake inside the 4D DBA ring over 100 turns: the fused mode (fast maps,
+    z-sorted prefix sums, the order in z changing from turn to turn) against the plain mode (the
+    reference's operation order and pair sum) at the 1000-turn regular-orbit tolerance; and the
+    wake does act (the same ring without it ends elsewhere)."""
+    ring = LT.config4_ring()
+    m = A.Line(ctx, ring).m66()
+    tw = A.elem(A.TRANSWAKE, "TW", 0.0, f=[3000, 2.0, 5000.0, 10.0, 1.5, 4000.0, 12.0, 2.0], flags=1)
+    r0 = LT.config5_particles(2048, m, seed=9)
+    line = A.Line(ctx, ring + [tw])
+    a, b, c = r0.copy(), r0.copy(), r0.copy()
+    line.track(a, 100, mode=A.MODE_PLAIN)
+    line.track(b, 100, mode=A.MODE_FUSED)
+    A.Line(ctx, ring).track(c, 100, mode=A.MODE_FUSED)
+    assert not np.isnan(a[:, 0]).any() and not np.isnan(b[:, 0]).any()
+    assert rel_err(b, a) < 1e-9
+    assert rel_err(c, a) > 1e-6
+
+
 def test_errors_are_statuses(A, ctx):
     r = np.zeros((4, 6))
     with pytest.raises(A.AccelError) as ei:  # a WigTable that names no kick table
