@@ -387,11 +387,18 @@ def beam_stat_noalloc(r, out, layout=LAYOUT_AOS, n=None, stream=None):
     """accel_beam_stat_noalloc: beam moments of a device tensor into the device tensor `out`
     (19 float64: mean[6], sigma[6], cross[6], live count), without any device allocation.
     Returns once the kernels are queued on `stream` (None = the legacy default stream)."""
-    if not hasattr(r, "data_ptr") or not hasattr(out, "data_ptr"):
-        raise ValueError("r and out must be device tensors")
+    for name, t in (("r", r), ("out", out)):
+        if not hasattr(t, "data_ptr") or not getattr(t, "is_cuda", False):
+            raise ValueError(f"{name} must be a CUDA tensor")
+        if str(t.dtype) != "torch.float64" or not t.is_contiguous():
+            raise ValueError(f"{name} must be a contiguous float64 tensor")
+    if out.device != r.device:
+        raise ValueError("r and out must be on the same device")
     if out.numel() < 19:
         raise ValueError("out must hold 19 doubles")
     ptr, n = _ptr_and_n(r, n, layout)
+    if n <= 0 or 6 * n > r.numel():
+        raise ValueError(f"n = {n} particles needs {6 * n} doubles; r holds {r.numel()}")
     s = C.c_void_p(stream) if stream is not None else None
     _check(lib().accel_beam_stat_noalloc(ptr, layout, n, C.c_void_p(out.data_ptr()), s),
            "accel_beam_stat_noalloc")
@@ -521,12 +528,21 @@ def _line_array(lines: Sequence[Line]):
 
 def track_batched(lines: Sequence[Line], part_off: np.ndarray, r_soa, nturn: int, loss=None,
                   mode: int = MODE_FUSED, stream=None):
-    """Track many lattice instances in one launch; r_soa is a device tensor of 6 x Ntot."""
+    """Track many lattice instances in one launch; r_soa is 6 x Ntot (SoA), a device tensor or a
+    host array (numpy, or a pinned CPU tensor), updated in place; loss likewise host or device."""
     off = np.ascontiguousarray(part_off, dtype=np.int64)
     ntot = int(off[-1])
+    if isinstance(r_soa, np.ndarray):
+        if r_soa.dtype != np.float64 or not r_soa.flags.c_contiguous or r_soa.size != 6 * ntot:
+            raise ValueError("r_soa must be a C-contiguous float64 array of 6 x Ntot")
+        ptr = r_soa.ctypes.data
+    else:
+        if not r_soa.is_contiguous() or r_soa.numel() != 6 * ntot or str(r_soa.dtype) != "torch.float64":
+            raise ValueError("r_soa must be a contiguous float64 tensor of 6 x Ntot")
+        ptr = r_soa.data_ptr()
     s = C.c_void_p(stream) if stream is not None else None
     _check(lib().accel_track_batched(_line_array(lines), len(lines), C.c_void_p(off.ctypes.data),
-                                     C.c_void_p(r_soa.data_ptr()), ntot, nturn, _iptr(loss), mode, s),
+                                     C.c_void_p(ptr), ntot, nturn, _iptr(loss), mode, s),
            "accel_track_batched")
 
 

@@ -980,18 +980,35 @@ int accel_track_batched(accel_line* const* lines, int ninst, const int64_t* part
         if ((s = line_sync(lines[i]))) return s;
         if ((s = check_supported(lines[i], 0, (int)lines[i]->desc.size()))) return s;
     }
-    if (!is_device_ptr(r_soa)) return fail(ACCEL_E_INVALID, "r_soa must be device memory");
-    if (loss_turn && !is_device_ptr(loss_turn)) return fail(ACCEL_E_INVALID, "loss_turn must be device memory");
-    if (ntot == 0 || nturn == 0) return ACCEL_OK;
+    // host or device arrays: host ones are staged through the context's buffers, one
+    // cudaMemcpyAsync each way per array, and the call returns once they are copied back
+    const bool rdev = is_device_ptr(r_soa);
+    const bool ldev = loss_turn ? is_device_ptr(loss_turn) : false;
+    if (ntot == 0 || nturn == 0) {
+        if (loss_turn && ntot > 0) {  // nothing runs: no particle is recorded as lost
+            if (ldev) {
+                launch_fill_i32(loss_turn, -1, ntot, C->stream);
+                CK(cudaStreamSynchronize(C->stream));
+            } else {
+                for (int64_t i = 0; i < ntot; i++) loss_turn[i] = -1;
+            }
+        }
+        return ACCEL_OK;
+    }
     cudaStream_t user = (cudaStream_t)stream;  // NULL: the legacy default stream
+    const size_t nb = sizeof(double) * 6 * (size_t)ntot;
     if ((s = C->loss.ensure(sizeof(int32_t) * (size_t)ntot))) return s;
+    if (!rdev) {
+        if ((s = C->state.ensure(nb))) return s;
+        CK(cudaMemcpyAsync(C->state.p, r_soa, nb, cudaMemcpyHostToDevice, user));
+    }
     CoreReq q{};
     q.lines = lines;
     q.ninst = ninst;
     if ((s = stage_batch(C, lines, ninst, part_off, ntot, &q.tables, &q.tbl_off, &q.pinst, C->stream))) return s;
-    q.st = r_soa;
+    q.st = rdev ? r_soa : (double*)C->state.p;
     q.ntot = ntot;
-    q.loss = loss_turn ? loss_turn : (int32_t*)C->loss.p;
+    q.loss = ldev ? loss_turn : (int32_t*)C->loss.p;
     q.e0 = 0;
     q.e1 = (int)lines[0]->desc.size();
     q.nturn = nturn;
@@ -1002,6 +1019,10 @@ int accel_track_batched(accel_line* const* lines, int ninst, const int64_t* part
         q.variant = tk->second[0]; q.seg = tk->second[1]; q.sched = tk->second[2];
     }
     if ((s = run_core(C, q, user))) return s;
+    if (!rdev) CK(cudaMemcpyAsync(r_soa, q.st, nb, cudaMemcpyDeviceToHost, user));
+    if (loss_turn && !ldev)
+        CK(cudaMemcpyAsync(loss_turn, q.loss, sizeof(int32_t) * (size_t)ntot, cudaMemcpyDeviceToHost, user));
+    if (!rdev || (loss_turn && !ldev)) CK(cudaStreamSynchronize(user));
     CK(cudaGetLastError());
     return ACCEL_OK;
 }
@@ -1216,7 +1237,7 @@ int accel_fp64_peak(accel_ctx* C, double* tflops) {
     CK(cudaSetDevice(C->device));
     float ms = 0;
     *tflops = fp64_peak_run(C->sm_count, C->stream, &ms);
-    C->launches += 2;
+    C->launches += 4;  // the warm-up and three timed probes
     CK(cudaGetLastError());
     return ACCEL_OK;
 }

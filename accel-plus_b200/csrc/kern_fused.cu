@@ -599,37 +599,51 @@ void launch_beam_stat(const double* st, int64_t n, double* part, int nblk, doubl
 }
 
 // ---- FP64 FMA throughput probe --------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_fp64_peak(double* out, int iters, double b, double c) {
-    double a0 = threadIdx.x * 1e-9, a1 = a0 + 1, a2 = a0 + 2, a3 = a0 + 3;
-    double a4 = a0 + 4, a5 = a0 + 5, a6 = a0 + 6, a7 = a0 + 7;
+// FP64 roofline probe: 8 independent FMA chains per thread, 2,048 threads per SM (full
+// occupancy), a loop long enough (about 10 ms) that launch and tail effects vanish.  One DFMA
+// warp instruction occupies the SM sub-partition's FP64 unit for two cycles, so the issue slots
+// left over cover the loop's own instructions and the probe can reach the pipe's rate.
+constexpr int kPeakChains = 8;
+
+__global__ void __launch_bounds__(512, 4) k_fp64_peak(double* out, int iters, double b, double c) {
+    double a[kPeakChains];
+#pragma unroll
+    for (int j = 0; j < kPeakChains; j++) a[j] = threadIdx.x * 1e-9 + j;
+#pragma unroll 4
     for (int i = 0; i < iters; i++) {
-        a0 = fma(a0, b, c); a1 = fma(a1, b, c); a2 = fma(a2, b, c); a3 = fma(a3, b, c);
-        a4 = fma(a4, b, c); a5 = fma(a5, b, c); a6 = fma(a6, b, c); a7 = fma(a7, b, c);
+#pragma unroll
+        for (int j = 0; j < kPeakChains; j++) a[j] = fma(a[j], b, c);
     }
-    double r = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
+    double r = 0;
+#pragma unroll
+    for (int j = 0; j < kPeakChains; j++) r += a[j];
     if (r == 1234.5) out[0] = r;  // keeps the chains live
 }
 
 double fp64_peak_run(int sm_count, cudaStream_t s, float* ms_out) {
-    const int iters = 1 << 14, threads = 256, blocks = sm_count * 8;
+    const int iters = 1 << 16, threads = 512, blocks = sm_count * 4;  // about 9 ms
     double* dummy = nullptr;
     cudaMallocAsync(&dummy, sizeof(double), s);
     k_fp64_peak<<<blocks, threads, 0, s>>>(dummy, iters / 8, 0.999999, 1e-7);  // warm-up
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    cudaEventRecord(e0, s);
-    k_fp64_peak<<<blocks, threads, 0, s>>>(dummy, iters, 0.999999, 1e-7);
-    cudaEventRecord(e1, s);
-    cudaEventSynchronize(e1);
-    float ms = 0;
-    cudaEventElapsedTime(&ms, e0, e1);
+    float best = 1e30f;
+    for (int rep = 0; rep < 3; rep++) {  // the best of three
+        cudaEventRecord(e0, s);
+        k_fp64_peak<<<blocks, threads, 0, s>>>(dummy, iters, 0.999999, 1e-7);
+        cudaEventRecord(e1, s);
+        cudaEventSynchronize(e1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best) best = ms;
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     cudaFreeAsync(dummy, s);
-    if (ms_out) *ms_out = ms;
-    double flops = 2.0 * 8.0 * (double)iters * threads * (double)blocks;
-    return flops / (ms * 1e-3) / 1e12;
+    if (ms_out) *ms_out = best;
+    double flops = 2.0 * kPeakChains * (double)iters * threads * (double)blocks;
+    return flops / (best * 1e-3) / 1e12;
 }
 
 }  // namespace accel

@@ -1,11 +1,11 @@
 // noalloc.cu — beam moments of a device-resident particle array without any device allocation.
 //
 // accel_beam_stat (capi.cpp) stages its input and its block partials in buffers that the context
-// grows on demand with cudaMalloc.  Some callers cannot let a library allocate: code that runs
-// while a stream is being captured into a CUDA graph (an allocation there fails the capture or
-// breaks it), code whose device memory is fully reserved up front by a memory pool or another
-// framework's caching allocator, and loops that sample the beam every few turns, where a
-// cudaMalloc/cudaFree pair can synchronise the device and stall the tracking pipeline.
+// grows on demand with cudaMalloc.  Some callers cannot let a library allocate: code whose device
+// memory is fully reserved up front by a memory pool or another framework's caching allocator
+// (a cudaMalloc there fails, or takes memory the pool counted on), and loops that sample the beam
+// every few turns, where a cudaMalloc/cudaFree pair can synchronise the device and stall the
+// tracking pipeline.
 // accel_beam_stat_noalloc serves them: it reads the caller's array in place (either layout), keeps
 // its partial sums in the fixed device array below, and writes the result to a caller-provided
 // device buffer.  The cost is a hard capacity and one shared scratch per device.
@@ -15,7 +15,9 @@
 //
 // Moments follow calc_beam_stat (utility.cpp:387-438): particles whose x is NaN are lost and left
 // out; the means, the rms sizes sqrt(<d_k^2>) and the six cross moments <xx'>, <yy'>, <x dp>,
-// <x' dp>, <y z>, <y' z> about the means, and the live count.  The sums run in two passes (means,
+// <x' dp>, <y z>, <y' z> about the means, and the live count.  Like calc_beam_stat and
+// accel_beam_stat, the moments are divided by the live count, so with every particle lost they
+// are NaN (0/0) and the count is 0.  The sums run in two passes (means,
 // then centred second moments) over fixed blocks of 1024 particles, so a given N always adds in
 // the same order and the result is reproducible bit for bit from call to call.
 #include <cuda_runtime.h>
@@ -112,24 +114,27 @@ __global__ void __launch_bounds__(kThreads) k_na_sum2(const double* r, int64_t n
 
 __global__ void k_na_out(const double* s1, const double* s2, double* out) {
     if (threadIdx.x != 0) return;
-    const double c = s1[6];
+    const double c = s1[6];  // 0 when every particle is lost: the moments come out NaN
     for (int k = 0; k < 6; k++) {
-        out[k] = c > 0 ? s1[k] / c : 0.0;
-        out[6 + k] = c > 0 ? sqrt(s2[k] / c) : 0.0;
-        out[12 + k] = c > 0 ? s2[6 + k] / c : 0.0;
+        out[k] = s1[k] / c;
+        out[6 + k] = sqrt(s2[k] / c);
+        out[12 + k] = s2[6 + k] / c;
     }
     out[18] = c;
 }
 
-// One-time set-up per device: the scratch's device address, and every kernel of this file
-// loaded, so that later calls only launch.
+// Set-up per device: the scratch's device address, and every kernel of this file loaded, so
+// that later calls only launch.  Done on a device's first call and kept once it succeeds; a
+// failed set-up is retried by the next call on that device.
 constexpr int kMaxDevices = 64;
-std::once_flag g_once[kMaxDevices];
-double* g_scratch[kMaxDevices];
-cudaError_t g_setup_err[kMaxDevices];
+std::mutex g_setup_mu;
+double* g_scratch[kMaxDevices];  // non-null once the device's set-up succeeded
 
-void setup_device(int dev) {
-    cudaError_t e = cudaGetSymbolAddress((void**)&g_scratch[dev], g_stat_scratch);
+cudaError_t setup_device(int dev) {
+    std::lock_guard<std::mutex> lk(g_setup_mu);
+    if (g_scratch[dev]) return cudaSuccess;
+    double* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress((void**)&p, g_stat_scratch);
     cudaFuncAttributes fa;
     if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_na_sum1<ACCEL_LAYOUT_AOS>);
     if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_na_sum1<ACCEL_LAYOUT_SOA>);
@@ -138,10 +143,11 @@ void setup_device(int dev) {
     if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_na_total);
     if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_na_out);
     if (e != cudaSuccess) {
-        cudaGetLastError();
-        g_scratch[dev] = nullptr;
+        cudaGetLastError();  // this set-up's own error; the next call tries again
+        return e;
     }
-    g_setup_err[dev] = e;
+    g_scratch[dev] = p;
+    return cudaSuccess;
 }
 
 bool on_device(const void* p, int* dev) {
@@ -193,17 +199,21 @@ extern "C" int accel_beam_stat_noalloc(const double* r, int layout, int64_t N, d
         cudaGetLastError();
         return fail(ACCEL_E_CUDA, "accel_beam_stat_noalloc: cudaSetDevice failed");
     }
-    std::call_once(g_once[dev], setup_device, dev);
     int status = ACCEL_OK;
-    if (g_setup_err[dev] != cudaSuccess) {
+    const cudaError_t pending = cudaPeekAtLastError();  // left by earlier work; not consumed here
+    const cudaError_t se = pending == cudaSuccess ? setup_device(dev) : cudaSuccess;
+    if (pending != cudaSuccess) {
+        status = fail(ACCEL_E_CUDA, std::string("accel_beam_stat_noalloc: a CUDA error of earlier work is pending (") +
+                                        cudaGetErrorString(pending) + "); nothing launched");
+    } else if (se != cudaSuccess) {
         status = fail(ACCEL_E_CUDA, std::string("accel_beam_stat_noalloc: set-up (cudaGetSymbolAddress) failed: ") +
-                                        cudaGetErrorString(g_setup_err[dev]));
+                                        cudaGetErrorString(se));
     } else {
         const int nblk = (int)((N + kPerBlock - 1) / kPerBlock);
         cudaStream_t s = (cudaStream_t)stream;
         if (layout == ACCEL_LAYOUT_AOS) launch<ACCEL_LAYOUT_AOS>(r, N, nblk, g_scratch[dev], out, s);
         else launch<ACCEL_LAYOUT_SOA>(r, N, nblk, g_scratch[dev], out, s);
-        cudaError_t e = cudaGetLastError();
+        cudaError_t e = cudaGetLastError();  // no error was pending before these launches
         if (e != cudaSuccess)
             status = fail(ACCEL_E_CUDA, std::string("accel_beam_stat_noalloc: launch failed: ") + cudaGetErrorString(e));
     }

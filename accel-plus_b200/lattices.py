@@ -163,6 +163,23 @@ def feed_down(a: np.ndarray, b: np.ndarray, dx: float, dy: float) -> tuple[np.nd
     return out.imag.copy(), out.real.copy()
 
 
+def _strmpole_errors(rng, a: np.ndarray, b: np.ndarray, dk_rel: float, sigma_off: float):
+    """The errors of one StrMPole, drawn from `rng` in a fixed order: a gradient error when the
+    element is a pure quadrupole, then the x and y offsets (each redrawn until inside 2 sigma);
+    returns the feed-down (poly_a, poly_b) over MAX_MPOLE orders."""
+    b = b.copy()
+    is_quad = b[1] != 0 and not np.any(b[2:]) and not np.any(a)
+    if is_quad:
+        b[1] *= 1.0 + rng.normal(0.0, dk_rel)
+    offs = []
+    for _ in range(2):
+        v = rng.normal(0.0, sigma_off)
+        while abs(v) > 2 * sigma_off:
+            v = rng.normal(0.0, sigma_off)
+        offs.append(v)
+    return feed_down(a, b, offs[0], offs[1])
+
+
 def error_copy(base: Sequence, seed: int, dk_rel: float = 1e-3, sigma_off: float = 30e-6) -> list:
     """One error-seeded copy: quads get dK/K ~ N(0, dk_rel), quads and sextupoles get offsets
     N(0, sigma_off) truncated at 2 sigma (redrawn until inside), all from default_rng(seed)."""
@@ -173,21 +190,44 @@ def error_copy(base: Sequence, seed: int, dk_rel: float = 1e-3, sigma_off: float
         if d.type == A.STRMPOLE:
             b = np.array(d.poly_b[:], dtype=np.float64)
             a = np.array(d.poly_a[:], dtype=np.float64)
-            is_quad = b[1] != 0 and not np.any(b[2:]) and not np.any(a)
-            if is_quad:
-                b[1] *= 1.0 + rng.normal(0.0, dk_rel)
-            offs = []
-            for _ in range(2):
-                v = rng.normal(0.0, sigma_off)
-                while abs(v) > 2 * sigma_off:
-                    v = rng.normal(0.0, sigma_off)
-                offs.append(v)
-            a2, b2 = feed_down(a, b, offs[0], offs[1])
+            a2, b2 = _strmpole_errors(rng, a, b, dk_rel, sigma_off)
             for i in range(A.MAX_MPOLE):
                 d.poly_a[i] = float(a2[i])
                 d.poly_b[i] = float(b2[i])
         out.append(d)
     return out
+
+
+def error_copy_text(seed: int, base_text: str | None = None, dk_rel: float = 1e-3,
+                    sigma_off: float = 30e-6) -> str:
+    """The lattice file of error_copy(config2_ring(), seed), made from the text of dba18.lat in
+    pure Python (no engine library): the same draws in the same order, each StrMPole's two
+    coefficient lines rewritten with 17 significant digits, every other line kept.  The result
+    equals accel_lattice_write of the descriptor copy, character for character (the lattice
+    format carries no radiation or cavity flags)."""
+    if base_text is None:
+        with open(os.path.join(GOLDEN_DIR, "dba18.lat")) as f:
+            base_text = f.read()
+    rng = np.random.default_rng(seed)
+    lines = base_text.split("\n")
+    out = []
+    i = 0
+    while i < len(lines):
+        ln = lines[i]
+        head = ln.split()
+        out.append(ln)
+        i += 1
+        if len(head) >= 5 and head[1] == ":" and head[2] == "StrMPole":
+            npole = int(head[4])
+            b = np.zeros(A.MAX_MPOLE)
+            a = np.zeros(A.MAX_MPOLE)
+            b[:npole] = [float(x) for x in lines[i].split()]
+            a[:npole] = [float(x) for x in lines[i + 1].split()]
+            a2, b2 = _strmpole_errors(rng, a, b, dk_rel, sigma_off)
+            for arr in (b2, a2):
+                out.append("\t\t\t" + "".join("%.17g\t" % float(arr[k]) for k in range(npole)))
+            i += 2
+    return "\n".join(out)
 
 
 # ---- particle sets --------------------------------------------------------------------------

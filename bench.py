@@ -53,8 +53,12 @@ def parse():
     ap.add_argument("--wake-only", action="store_true",
                     help="time the bunch workload with its per-turn wake (2^20 particles) and exit")
     ap.add_argument("--wake-turns", type=int, default=200)
+    ap.add_argument("--no-wake", action="store_true",
+                    help="skip the bunch-wake and transverse-wake legs of the default line")
     ap.add_argument("--transwake-only", action="store_true",
                     help="time the transverse wake (sorted prefix sum against the pair sum) and exit")
+    ap.add_argument("--ref-seconds", type=float, default=8.0,
+                    help="CPU seconds of reference tracking per step of --impl reference")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--small", action="store_true",
                     help="profiling case: 16 copies, 20 turns, one step (for ncu)")
@@ -115,36 +119,64 @@ class Clocks:
                 "samples": len(sm)}
 
 
-def workload(copies: int, rank: int):
+def workload_shape(copies: int, rank: int):
+    """(per-copy grid sizes, particle offsets, AoS particles) of the batched DA workload; pure
+    numpy, no engine library."""
     LT = importlib.import_module("accel-plus_b200.lattices")
-    base = LT.config2_ring()
     sizes = LT.config3_sizes(copies, seed=12345 + rank)
-    rings = [LT.error_copy(base, rank * copies + k) for k in range(copies)]
     grids = [LT.da_grid(nx, ny) for nx, ny in sizes]
     off = np.zeros(copies + 1, dtype=np.int64)
     off[1:] = np.cumsum([g.shape[0] for g in grids])
-    return rings, off, np.concatenate(grids, axis=0), sizes
+    return sizes, off, np.concatenate(grids, axis=0)
+
+
+def workload(copies: int, rank: int):
+    LT = importlib.import_module("accel-plus_b200.lattices")
+    base = LT.config2_ring()
+    sizes, off, aos = workload_shape(copies, rank)
+    rings = [LT.error_copy(base, rank * copies + k) for k in range(copies)]
+    return rings, off, aos, sizes
 
 
 def tracked_turns(loss: np.ndarray, nturn: int) -> np.ndarray:
     return np.where(loss < 0, nturn, loss + 1).astype(np.int64)
 
 
-def cpu_reference_rate(rings, off, aos, turns_goal: float = 15.0):
-    """Time the reference library (oracle/_ref) — or, when it is absent, the C restatement —
-    on the first copies of the workload, OpenMP over all host threads.  Returns a dict."""
+def reference_copies(sizes, count: int = 8) -> list[int]:
+    """`count` copies spread over the grid-size range: the copies at evenly spaced quantiles of
+    the particle count, smallest and largest included."""
+    n = np.array([nx * ny for nx, ny in sizes])
+    order = np.argsort(n, kind="stable")
+    q = np.linspace(0, len(n) - 1, min(count, len(n)))
+    return sorted({int(order[int(round(x))]) for x in q})
+
+
+def cpu_reference_rate(sizes, off, aos, rank: int = 0, turns_goal: float = 15.0, count: int = 8,
+                       job_turns: int = 1000):
+    """Time the reference library (oracle/_ref) — or, when it is absent, the C restatement — on
+    `count` copies of the workload spread over its grid sizes, each on its full grid, OpenMP
+    over all host threads, for a number of turns calibrated to take about `turns_goal` seconds
+    in all.  The reference reads each copy's lattice file, written in pure Python
+    (lattices.error_copy_text), so this process maps no library of the engine.  The sample's
+    particle-turns/s stand for the whole job (every copy, every turn): an extrapolation.  Returns
+    a dict."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
-    A = importlib.import_module("accel-plus_b200")
+    LT = importlib.import_module("accel-plus_b200.lattices")
     threads = os.cpu_count() or 1
     kind = "reference" if O.ref_available() else "port"
+    copies = len(sizes)
+    picks = reference_copies(sizes, count)
+    if kind == "port":  # the C restatement takes descriptors (the engine's host-only reader)
+        base = LT.config2_ring()
 
     def run(k, nturn):
         r = aos[off[k]:off[k + 1]].copy()
+        seed = rank * copies + k
         if kind == "reference":
             fd, path = tempfile.mkstemp(suffix=".lat")
-            os.close(fd)
-            A.write_lattice(path, rings[k])
+            with os.fdopen(fd, "w") as f:
+                f.write(LT.error_copy_text(seed))
             ref = O.RefLine(path)
             os.unlink(path)
             ref.set_flags(rad=1, cavity=1)
@@ -152,23 +184,26 @@ def cpu_reference_rate(rings, off, aos, turns_goal: float = 15.0):
             lt = ref.track_loss(r, nturn, threads=threads)
             dt = time.perf_counter() - t
         else:
+            ring = LT.error_copy(base, seed)
             t = time.perf_counter()
-            lt = O.port_track(rings[k], r, nturn, nthreads=threads)
+            lt = O.port_track(ring, r, nturn, nthreads=threads)
             dt = time.perf_counter() - t
         return int(tracked_turns(lt, nturn).sum()), dt
 
-    pt, dt = run(0, 2)  # calibration
+    pt, dt = run(picks[0], 2)  # calibration
     rate0 = pt / max(dt, 1e-6)
-    nturn = int(max(5, min(200, turns_goal * rate0 / max(1, off[1] - off[0]) / 4)))
-    tot_pt, tot_dt, used = 0, 0.0, 0
-    for k in range(min(4, len(rings))):
+    nsample = int(sum(off[k + 1] - off[k] for k in picks))
+    nturn = int(max(5, min(200, turns_goal * rate0 / max(1, nsample))))
+    tot_pt, tot_dt = 0, 0.0
+    for k in picks:
         p, d = run(k, nturn)
         tot_pt += p
         tot_dt += d
-        used += 1
     return {"value": tot_pt / tot_dt, "unit": UNIT, "cores": threads, "kind": kind,
-            "sample": f"{used} of the error-seeded copies (their full DA grids, "
-                      f"{int(off[used])} particles) x {nturn} turns, radiation + cavity on",
+            "sample": f"extrapolated: {len(picks)} of the {copies} error-seeded copies spread over "
+                      f"the grid sizes (copies {picks}, their full DA grids, {nsample} particles) x "
+                      f"{nturn} of the {job_turns} turns, radiation + cavity on; the sample's rate "
+                      f"stands for the whole job",
             "seconds": round(tot_dt, 3)}
 
 
@@ -183,13 +218,13 @@ def reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    rings, off, aos, sizes = workload(args.copies, 0)
+    sizes, off, aos = workload_shape(args.copies, 0)
     vals = []
     for _ in range(max(1, args.warmup // 3)):
-        cpu_reference_rate(rings, off, aos, turns_goal=3.0)
+        cpu_reference_rate(sizes, off, aos, turns_goal=0.4 * args.ref_seconds, job_turns=args.turns)
     per_step = []
     for _ in range(args.steps):
-        b = cpu_reference_rate(rings, off, aos, turns_goal=8.0)
+        b = cpu_reference_rate(sizes, off, aos, turns_goal=args.ref_seconds, job_turns=args.turns)
         vals.append(b["value"])
         per_step.append(b)
     v = statistics.median(vals)
@@ -203,8 +238,18 @@ def reference_arm(args):
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": b["cores"], "kind": b["kind"],
                          "sample": b["sample"]},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "process_maps_engine_library": maps_engine_library(),
     }
     print(json.dumps(line), flush=True)
+
+
+def maps_engine_library() -> bool:
+    """Whether this process has the engine's shared library mapped (/proc/self/maps)."""
+    try:
+        with open("/proc/self/maps") as f:
+            return "libaccelgpu" in f.read()
+    except OSError:
+        return False
 
 
 def config_dict(args, off, aos):
@@ -216,7 +261,7 @@ def config_dict(args, off, aos):
             "seeds": "copy k of rank r: error seed r*copies+k; grid sizes default_rng(12345+r)"}
 
 
-def adjoint_leg(A, LT, ctx, steps: int = 3, ranks=None) -> dict:
+def adjoint_leg(A, LT, ctx, steps: int = 3, ranks=None, check: bool = True) -> dict:
     """Gradient of L = sum over particles of (x^2 + y^2) after 512 turns of the 4D DBA (no cavity,
     radiation off), 4,096 Gaussian particles (seed 1), with respect to the 6 x 4,096 initial
     coordinates and the 36 sextupole knobs (mirror pairs of the 72 sextupoles), checkpointed every
@@ -269,9 +314,10 @@ def adjoint_leg(A, LT, ctx, steps: int = 3, ranks=None) -> dict:
         t_adj, t_fwd, t_track = ranks.max(t_adj), ranks.max(t_fwd), ranks.max(t_track)
     t_fd = min(t_track, t_fwd)
     knob = {e: j for j, e in enumerate(elems)}
-    dknob = np.array([dp[knob[a]] + dp[knob[b]] for a, b in pairs])
-    if ranks:
-        dknob = ranks.sum_array(dknob)
+    dknob_local = np.array([dp[knob[a]] + dp[knob[b]] for a, b in pairs])
+    dknob = ranks.sum_array(dknob_local) if ranks else dknob_local
+    # the gradient at this size against finite differences (this rank's particles)
+    fd_check = adjoint_fd_check(A, LT, ctx, r0, nturn, pairs, dknob_local, dr0) if check else None
     n_in = 6 * n + len(pairs)
     naive, batched = 2 * n_in, 2 * (6 + len(pairs))
     adj.close()
@@ -286,7 +332,139 @@ def adjoint_leg(A, LT, ctx, steps: int = 3, ranks=None) -> dict:
             "fd_cost_ratio_batched": batched * t_fd / t_adj,
             "survivors": int((~np.isnan(rf[:, 0])).sum()),
             "knob_gradient_norm": float(np.linalg.norm(dknob)),
+            "fd_check": fd_check,
             "timing": "wall clock around synchronous C-ABI calls, mean of %d" % steps}
+
+
+def adjoint_fd_check(A, LT, ctx, r0, nturn, pairs, dknob, dr0, knob_step=1e-3, converge=False,
+                     coords=(0, 1, 2, 3, 5)) -> dict:
+    """The adjoint's gradient of L = sum over survivors of (x^2 + y^2) against central finite
+    differences of L taken on the GPU in the exact mode (the reference's operation order, bit for
+    bit the plain kernel), all differences of the job tracked together in one batched call:
+      knobs: each of the sextupole pairs moved by +-h and +-h/2 (Richardson-extrapolated central
+        difference, error O(h^4)), h = knob_step; with `converge`, also at h/3, the estimate at
+        h/3 taken and the two required to agree;
+      coordinates: particles are independent, so one copy of the whole bunch per coordinate and
+        step moves that coordinate of every particle, giving dL/dr0 of every particle at once;
+        steps 1e-6 of the coordinate's spread relative to x's (1e-6 for delta, whose spread is 0).
+    Relative error of a knob: |adjoint - fd| / |fd|; of a coordinate entry: |adjoint - fd| /
+    max(|fd|, 1e-3 x the largest |adjoint| of that coordinate), the bar of the smaller tests."""
+    import torch
+    n = len(r0)
+    ring = LT.config4_ring()
+    scale = np.sqrt(np.mean(r0 ** 2, axis=0))
+    steps = [knob_step] + ([knob_step / 3] if converge else [])
+    rings, particles, tags = [], [], []
+    for j, (ea, eb) in enumerate(pairs):
+        for h in steps:
+            for dv in (h, -h, h / 2, -h / 2):
+                rr = [d.copy() for d in ring]
+                rr[ea].poly_b[2] += dv
+                rr[eb].poly_b[2] += dv
+                rings.append(rr)
+                particles.append(r0)
+                tags.append(("knob", j, h, dv))
+    cstep = {}
+    for k in coords:
+        cstep[k] = 1e-6 * (scale[k] / scale[0] if scale[k] > 0 else 1.0)
+        for dv in (1.0, -1.0, 0.5, -0.5):
+            a = r0.copy()
+            a[:, k] += dv * cstep[k]
+            rings.append(ring)
+            particles.append(a)
+            tags.append(("coord", k, cstep[k], dv * cstep[k]))
+    lines = [A.Line(ctx, rr) for rr in rings]
+    off = np.arange(len(lines) + 1, dtype=np.int64) * n
+    soa = torch.tensor(np.ascontiguousarray(np.concatenate(particles).T), device="cuda",
+                       dtype=torch.float64).contiguous()
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    A.track_batched(lines, off, soa, nturn, mode=A.MODE_EXACT)
+    torch.cuda.synchronize()
+    secs = time.perf_counter() - t
+    for l in lines:
+        l.close()
+    out = soa.cpu().numpy()
+    x, y = out[0].reshape(-1, n), out[2].reshape(-1, n)
+    with np.errstate(invalid="ignore"):
+        lp = np.where(np.isnan(x), 0.0, x * x + y * y)  # per-particle loss, each copy
+    Lsum = lp.sum(axis=1)
+    f = {}
+    for i, tg in enumerate(tags):
+        f[tg] = Lsum[i] if tg[0] == "knob" else lp[i]
+
+    def rich(get, h):
+        d1 = (get(h) - get(-h)) / (2 * h)
+        d2 = (get(h / 2) - get(-h / 2)) / h
+        return (4 * d2 - d1) / 3
+
+    knob_fd = np.zeros(len(pairs))
+    conv = []
+    for j in range(len(pairs)):
+        est = [rich(lambda dv, j=j, h=h: f[("knob", j, h, dv)], h) for h in steps]
+        knob_fd[j] = est[-1]
+        if converge:
+            conv.append(abs(est[0] - est[1]) / abs(est[1]))
+    knob_rel = np.abs(dknob - knob_fd) / np.abs(knob_fd)
+    coord_rel = {}
+    for k in coords:
+        fd = rich(lambda dv, k=k: f[("coord", k, cstep[k], dv)], cstep[k])
+        floor = 1e-3 * np.max(np.abs(dr0[:, k]))
+        coord_rel[k] = float(np.max(np.abs(dr0[:, k] - fd) / np.maximum(np.abs(fd), floor)))
+    return {"fd_mode": "exact (the reference's operation order), all differences in one batched call",
+            "knobs": len(pairs), "knob_step": knob_step, "knob_max_rel_err": float(np.max(knob_rel)),
+            "knob_richardson_agreement": float(np.max(conv)) if conv else None,
+            "coords_checked_per_particle": [int(k) for k in coords], "particles": n,
+            "coord_max_rel_err": max(coord_rel.values()),
+            "coord_max_rel_err_by_coord": {str(k): v for k, v in coord_rel.items()},
+            "instances": len(lines), "seconds": round(secs, 2)}
+
+
+def parity_on_classified_copies(off, fused_soa, fused_loss, plain_soa=None, plain_loss=None):
+    """The timed fused run checked on the copies whose reference outputs and per-particle
+    classification are committed (tests/golden/config_golden.npz: four copies of this workload,
+    1,000 turns, by the reference library): loss turns off the chaotic boundary; regular
+    survivors within 1e-9 of the reference and of the plain kernel; every other survivor off the
+    boundary within the reference's own spread under a 1e-12 start perturbation."""
+    path = os.path.join(ROOT, "tests", "golden", "config_golden.npz")
+    if not os.path.exists(path):
+        return None
+    cg = np.load(path)
+    picks = [int(k) for k in cg["c3_copies"]]
+    tot = {"regular": 0, "reg_ref": 0, "reg_plain": 0, "surv": 0, "surv_ok": 0, "checked": 0,
+           "lt_ok": 0, "worst_regular_rel_err": 0.0}
+    for k in picks:
+        s = slice(int(off[k]), int(off[k + 1]))
+        ref, lt_ref = cg[f"c3_{k}_out"], cg[f"c3_{k}_loss"]
+        bnd, reg, amp, sc = (cg[f"c3_{k}_{x}"] for x in ("boundary", "regular", "amp", "scale"))
+        r, lt = fused_soa[:, s].T, fused_loss[s]
+        with np.errstate(invalid="ignore"):
+            err = np.max(np.abs(r - ref) / sc, axis=1)
+        err[np.isnan(err)] = np.inf
+        tot["checked"] += int((~bnd).sum())
+        tot["lt_ok"] += int(((lt == lt_ref) & ~bnd).sum())
+        tot["regular"] += int(reg.sum())
+        tot["reg_ref"] += int((err[reg] < 1e-9).sum())
+        if reg.any():
+            tot["worst_regular_rel_err"] = max(tot["worst_regular_rel_err"], float(err[reg].max()))
+        surv = (lt_ref < 0) & ~bnd
+        tot["surv"] += int(surv.sum())
+        tot["surv_ok"] += int((err[surv] <= np.maximum(1e-9, amp[surv])).sum())
+        if plain_soa is not None:
+            with np.errstate(invalid="ignore"):
+                ep = np.max(np.abs(r - plain_soa[:, s].T) / sc, axis=1)
+            tot["reg_plain"] += int((ep[reg] < 1e-9).sum())
+    return {"copies": picks, "turns": 1000, "particles_off_boundary": tot["checked"],
+            "loss_turns_equal_off_boundary": tot["lt_ok"] / max(1, tot["checked"]),
+            "regular_survivors": tot["regular"],
+            "regular_within_1e-9_of_reference": tot["reg_ref"] / max(1, tot["regular"]),
+            "regular_within_1e-9_of_plain": (tot["reg_plain"] / max(1, tot["regular"]))
+            if plain_soa is not None else None,
+            "worst_regular_rel_err": tot["worst_regular_rel_err"],
+            "survivors_off_boundary": tot["surv"],
+            "survivors_within_reference_sensitivity": tot["surv_ok"] / max(1, tot["surv"]),
+            "classification": "tests/golden/config_golden.npz (the reference re-tracked with x, y "
+                              "moved by +-1e-12)"}
 
 
 class Ranks:
@@ -351,9 +529,9 @@ def engine_arm(args):
     dev = torch.device("cuda", local)
     if args.small:
         args.copies, args.turns, args.steps, args.warmup = 16, 20, 1, 1
-        args.no_plain = args.no_cpu = args.no_e2e = args.no_adjoint = True
+        args.no_plain = args.no_cpu = args.no_e2e = args.no_adjoint = args.no_wake = True
     if args.engine_only:
-        args.no_plain = args.no_cpu = args.no_e2e = args.no_adjoint = True
+        args.no_plain = args.no_cpu = args.no_e2e = args.no_adjoint = args.no_wake = True
 
     rings, off, aos, sizes = workload(args.copies, rank)
     ntot = int(off[-1])
@@ -402,9 +580,13 @@ def engine_arm(args):
     total_pt = sum_over_ranks(pt_step)
     value = total_pt / (ms_step / 1e3)
     loss_np = loss.cpu().numpy()
+    fused_np = state.cpu().numpy()
 
     # ---- roofline of the dominant kernel: one profiled step with events around each launch ----
     peak = ctx.fp64_peak()
+    sms = torch.cuda.get_device_properties(local).multi_processor_count
+    mhz = clk.get("sm_mhz") or clk.get("sm_max_mhz")
+    peak_theory = sms * 64 * 2 * mhz * 1e6 / 1e12 if mhz else None
     ctx.profile(True)
     step(k=0)
     fused_ms, fused_n, call_ms = ctx.profile_read()
@@ -422,8 +604,13 @@ def engine_arm(args):
                 "kernel": "k_fused (persistent FP64 tracker)",
                 "launches": fused_n, "kernel_ms_per_step": fused_ms, "step_ms_profiled": call_ms,
                 "model_flops_per_step": flops,
-                "peak_source": "measured in this run: FP64 FMA-chain probe (accel_fp64_peak); "
-                               "MEASURED_PEAKS.json carries no FP64 figure",
+                "peak_source": "measured in this run: FP64 FMA-chain probe (accel_fp64_peak, best of "
+                               "three 9 ms runs at full occupancy); MEASURED_PEAKS.json carries "
+                               "no FP64 figure",
+                "peak_theoretical": peak_theory, "frac_theoretical": (achieved / peak_theory)
+                if achieved and peak_theory else None,
+                "peak_theoretical_basis": "SMs x 64 FP64 FMA per clock x 2 flops x the median SM "
+                                          "clock sampled in the timed region",
                 "flops_model": "add/sub/mul/div = 1 at the effective multipole order "
                                "(StrMPole slice 52+3(8m+4), BendMPole slice 4*46+3(90+7m) with "
                                "radiation, drift 14)"}
@@ -466,22 +653,29 @@ def engine_arm(args):
                           "exact_over_plain": (pt_exact / (xms / 1e3)) / (pt_plain / (pms / 1e3)),
                           "bit_identical_to_plain": same}
 
+    # ---- parity of the timed run on the copies the reference's outputs are committed for ----
+    parity = None
+    if rank == 0 and args.copies == 256 and args.turns == 1000:
+        parity = parity_on_classified_copies(off, fused_np, loss_np, None if plain is None else sp,
+                                             None if plain is None else lp)
+
     # ---- end to end through the C-ABI with host buffers ----
     e2e = None
     if not args.no_e2e:
+        # the user's call: page-locked host arrays handed straight to accel_track_batched, which
+        # copies them in, tracks, copies the state and loss turns back and returns when done
         h_in = torch.tensor(np.ascontiguousarray(aos.T), dtype=torch.float64).pin_memory()
-        h_out = torch.empty_like(h_in).pin_memory()
+        h_state = torch.empty_like(h_in).pin_memory()
         h_loss = torch.empty(ntot, dtype=torch.int32).pin_memory()
 
         def e2e_step(k):
             flush.fill_(float(k))
-            state.copy_(h_in, non_blocking=True)
-            A.track_batched(lines, off, state, args.turns, loss=loss, stream=stream)
-            h_out.copy_(state, non_blocking=True)
-            h_loss.copy_(loss, non_blocking=True)
+            h_state.copy_(h_in)  # this step's input (the call tracks in place)
+            A.track_batched(lines, off, h_state, args.turns, loss=h_loss, stream=stream)
 
         e2e_step(0)
         torch.cuda.synchronize()
+        same = bool(np.array_equal(h_loss.numpy(), loss_np))
         barrier()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
@@ -492,16 +686,26 @@ def engine_arm(args):
         ems = max_over_ranks(e0.elapsed_time(e1)) / args.steps
         e2e = {"value": total_pt / (ems / 1e3), "unit": UNIT,
                "h2d_bytes_per_step": int(h_in.numel() * 8),
-               "d2h_bytes_per_step": int(h_out.numel() * 8 + h_loss.numel() * 4),
-               "ms_per_step": ems, "path": "accel_track_batched (C-ABI) with pinned host in/out"}
+               "d2h_bytes_per_step": int(h_state.numel() * 8 + h_loss.numel() * 4),
+               "loss_turns_equal_device_run": same,
+               "ms_per_step": ems,
+               "path": "host pointers through accel_track_batched (C-ABI): page-locked SoA state "
+                       "and loss turns, copied in and out inside the call"}
 
     adjoint = None
     if not args.no_adjoint:
         adjoint = adjoint_leg(A, LT, ctx, ranks=ranks)
 
+    # the collective workloads: a 2^20-particle bunch with its per-turn longitudinal wake, and the
+    # transverse wake's sorted sum against the pair sum (each rank on its own GPU)
+    wake = transwake = None
+    if not args.no_wake:
+        wake = wake_leg(A, LT, ctx, nturn=args.wake_turns)
+        transwake = transwake_leg(A, ctx)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_reference_rate(rings, off, aos)
+        cpu = cpu_reference_rate(sizes, off, aos, job_turns=args.turns)
 
     if rank == 0:
         line = {
@@ -510,7 +714,7 @@ def engine_arm(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": config_dict(args, off, aos), "roofline": roofline, "cpu_baseline": cpu,
             "e2e": e2e, "gpu_launches": int(launches), "clocks": clk, "plain": plain,
-            "adjoint": adjoint,
+            "parity": parity, "adjoint": adjoint, "bunch_wake": wake, "transverse_wake": transwake,
             "tile": {"block": tile[0], "seg_turns": tile[1], "variant": tile[2] % 100,
                      "sched": ["atomic chunks per warp", "contiguous range per block"][tile[2] // 100]}
                     if tile else None,

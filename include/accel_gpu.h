@@ -246,7 +246,12 @@ int  accel_track(accel_line* line, double* r, int layout, int N, int st, int ed,
 /*
  * Batched tracking: `ninst` lines (same context) tracked in one persistent launch.  Particles are
  * grouped by instance: instance i owns particles [part_off[i], part_off[i+1]) of the SoA arrays
- * r_soa (6 x Ntot doubles, k-major, device memory).  All lines must have the same element count.
+ * r_soa (6 x Ntot doubles, k-major).  All lines must have the same element count.
+ * r_soa and loss_turn (optional, Ntot int32, as in accel_track) are host or device memory each.
+ * Device arrays are used in place on `stream` and the call returns without synchronising; a host
+ * array is copied in with one cudaMemcpyAsync, tracked in the context's buffer and copied back,
+ * and the call returns once the copies are done (page-locked host memory makes those copies
+ * asynchronous DMA transfers).
  */
 int  accel_track_batched(accel_line* const* lines, int ninst, const int64_t* part_off,
                          double* r_soa, int64_t ntot, int nturn, int32_t* loss_turn,
@@ -302,20 +307,24 @@ int  accel_beam_stat(accel_ctx* ctx, const double* r, int layout, int N, double*
                      double* sigma, double* cross, int* nlive);
 
 /* The same beam moments with no device allocation.  No counterpart in the reference: it exists
- * for callers that cannot let a library allocate (code running while a stream is captured,
- * device memory reserved up front by a pool or another framework, per-turn sampling loops that a
- * cudaMalloc/cudaFree synchronisation would stall).
+ * for callers that cannot let a library allocate: device memory reserved up front by a pool or
+ * another framework's caching allocator (a cudaMalloc there fails, or takes memory the pool
+ * counted on), and per-turn sampling loops that a cudaMalloc/cudaFree synchronisation would stall.
  *   r    device array of N particles in `layout`, read in place; out  device array of 19 doubles
  *        receiving mean[6], sigma[6], cross[6] and the live count (as a double), in that order.
+ *        As in calc_beam_stat, the moments are divided by the live count: with every particle
+ *        lost they are NaN and the count is 0.
  *   N    1 .. ACCEL_NOALLOC_STAT_MAX_N; larger N returns ACCEL_E_TOO_LARGE and launches nothing.
  *   stream  where the five small kernels run (NULL = the legacy default stream); the call
  *        returns without synchronising, and `out` is ready when that stream reaches it.
  * Partial sums live in one fixed device array per device (12 * 4096 + 32 doubles), which every
  * call overwrites before reading: nothing in it needs to start at zero.  Because that array is
- * shared, calls on the same device must not overlap: issue them on one stream, or order them
- * with events.  The first call on each device does a one-time set-up (the scratch's address via
- * cudaGetSymbolAddress, and the kernels loaded) with that device current; make that first call
- * before beginning any stream capture.                                                         */
+ * shared, calls on the same device that overlap on the GPU race: issue them on one stream, or
+ * order them with events.  The first call on each device does a one-time set-up (the scratch's
+ * address via cudaGetSymbolAddress, and the kernels loaded) with that device current; make that
+ * first call before beginning any stream capture.  A failed set-up is retried by the next call.
+ * A CUDA error already pending from earlier work is reported (ACCEL_E_CUDA) and left pending,
+ * and nothing is launched.                                                                     */
 #define ACCEL_NOALLOC_STAT_MAX_N 4194304
 int  accel_beam_stat_noalloc(const double* r, int layout, int64_t N, double* out, void* stream);
 

@@ -1,7 +1,7 @@
 """Run the reference's own input-deck executable on every deck under tests/decks/ and keep its
 output as a golden fixture (tests/golden/<deck>.ref.out), timestamp lines removed.
 
-    make -C oracle ref && python tests/golden/make_deck_golden.py
+    make -C oracle ref REF_SRC=<reference>/src/lib/accel && python tests/golden/make_deck_golden.py
 
 oracle/_ref/accel+ref is the reference's process.cpp compiled with its library sources; the decks
 name their lattice files relative to the repository root, so the decks run from there.

@@ -1,6 +1,6 @@
 """Reference outputs for the CrabCav, RFMult and IdealWig elements (oracle/_ref).
 
-    make -C oracle all && python tests/golden/make_elem_extra_golden.py
+    make -C oracle all REF_SRC=<reference>/src/lib/accel && python tests/golden/make_elem_extra_golden.py
 
 Each case is one element, written with the engine's lattice writer, read and tracked for one turn
 by the reference library on the 16 particles of make_golden.element_particles().  Crab cavities

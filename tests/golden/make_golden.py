@@ -3,7 +3,7 @@
 Run in a container where the reference sources exist (oracle/Makefile compiles them into
 oracle/_ref/libaccel_ref.so):
 
-    make -C oracle all && python tests/golden/make_golden.py
+    make -C oracle all REF_SRC=<reference>/src/lib/accel && python tests/golden/make_golden.py
 
 Writes, next to this script:
   fodo32.lat   32-cell FODO, sextupoles from the reference's correct_chrom to (1, 1), twice

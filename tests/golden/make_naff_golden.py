@@ -1,6 +1,6 @@
 """Tune fixtures from the reference's own naff (oracle/_ref), for the engine's host NAFF.
 
-    make -C oracle all && python tests/golden/make_naff_golden.py
+    make -C oracle all REF_SRC=<reference>/src/lib/accel && python tests/golden/make_naff_golden.py
 
 Writes naff.npz: turn-by-turn records (synthetic lines with harmonics and noise, and x / y of
 particles tracked through the 32-cell FODO by the oracle), the frequency windows, and the

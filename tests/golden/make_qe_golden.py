@@ -1,6 +1,6 @@
 """Quantum-excitation statistics from the reference library itself (oracle/_ref), as fixtures.
 
-    make -C oracle all && python tests/golden/make_qe_golden.py [growth | equilibrium [BATCH]]
+    make -C oracle all REF_SRC=<reference>/src/lib/accel && python tests/golden/make_qe_golden.py [growth | equilibrium [BATCH]]
 
 The 18-cell DBA with radiation + quantum excitation (RADQE) and the cavity on; every particle
 starts at the origin, so after T turns the spread is entirely the excitation's (the mean carries

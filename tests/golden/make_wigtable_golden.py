@@ -1,6 +1,6 @@
 """Reference outputs for the WigTable element (oracle/_ref).
 
-    make -C oracle all && python tests/golden/make_wigtable_golden.py
+    make -C oracle all REF_SRC=<reference>/src/lib/accel && python tests/golden/make_wigtable_golden.py
 
 Each case is one WigTable element whose kick tables are registered with the engine, written with
 the engine's lattice writer at 17 digits, then read and tracked for one turn by the reference

@@ -1,0 +1,48 @@
+"""Host-side checks of the benchmark's reference arm (no GPU).
+
+The reference arm times the reference's own CPU tracking on a sample of the batched DA workload.
+Its copies' lattice files are written in pure Python (lattices.error_copy_text), so the process
+that runs the reference maps no library of the engine: the text must equal the engine's own
+lattice writer's output for the same copy, character for character, and a short run of the arm
+must report the engine library unmapped.
+"""
+from __future__ import annotations
+
+import json
+import os
+import subprocess
+import sys
+import tempfile
+
+import pytest
+
+from conftest import ROOT
+
+
+@pytest.mark.parametrize("seed", [0, 5, 131, 255])
+def test_error_copy_text_equals_library_writer(A, LT, seed):
+    fd, path = tempfile.mkstemp(suffix=".lat")
+    os.close(fd)
+    try:
+        A.write_lattice(path, LT.error_copy(LT.config2_ring(), seed))
+        with open(path) as f:
+            want = f.read()
+    finally:
+        os.unlink(path)
+    assert LT.error_copy_text(seed) == want
+
+
+def test_reference_arm_maps_no_engine_library(O):
+    if not O.ref_available():
+        pytest.skip("oracle/_ref not built (reference sources absent)")
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
+                          "--steps", "1", "--warmup", "1", "--copies", "16", "--turns", "20",
+                          "--ref-seconds", "0.5"], capture_output=True, text=True, timeout=600,
+                         env={**os.environ, "OMP_NUM_THREADS": "2"})
+    assert out.returncode == 0, out.stderr[-2000:]
+    line = json.loads(out.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference"
+    assert line["cpu_baseline"]["kind"] == "reference"
+    assert "extrapolated" in line["cpu_baseline"]["sample"]
+    assert line["process_maps_engine_library"] is False
+    assert line["value"] > 0

@@ -1,0 +1,129 @@
+"""GPU parity at the workloads' stated sizes, against the reference's own outputs.
+
+tests/golden/config_golden.npz (made by tests/golden/make_config_golden.py with the reference
+library, all host threads) holds the reference's final states and loss turns for:
+  c1      the 32-cell FODO, 1,024 particles, 1,000 turns;
+  c2      the 18-cell DBA with radiation and RF, the full 101 x 51 grid, 1,024 turns;
+  c3_<k>  four error-seeded copies of that DBA on their full grids (the smallest, the largest and
+          two from the middle of the batched workload's grid sizes), 1,000 turns;
+with every particle classified by re-tracking it with x and y moved by +-1e-12: `boundary`
+(either fate is acceptable there: the fate changes under the perturbation, or a grid neighbour's
+fate differs) and `regular` (survives off the boundary with the perturbation grown to < 1e-9).
+
+Bars, for every mode:
+  loss turns equal to the reference's bit for bit at every particle off the boundary;
+  final coordinates of the regular particles within 1e-9 of the reference (relative to each
+      coordinate's RMS); bit for bit in the plain and exact modes where no transcendental
+      enters (the FODO), since they keep the reference's operation order;
+  every other survivor off the boundary no farther from the reference than the reference's own
+      run ends from itself under the 1e-12 start perturbation (in this chaotic lattice most
+      survivors after 1,000 turns amplify that perturbation past 1e-9);
+  the DA area by trackDA's triangle fan (aline.cpp:689-708, over each grid column's first lost
+      point) within one grid cell of the reference's.
+The GPU runs through the C-ABI (accel_track and accel_track_batched); nothing is re-tracked on
+the CPU.
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, rel_err_each, same_bits
+
+sys.path.insert(0, GOLDEN)
+import make_config_golden as MC  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+MODES = {"fused": 0, "plain": 1, "exact": 2}
+
+
+@pytest.fixture(scope="module")
+def CG():
+    path = os.path.join(GOLDEN, "config_golden.npz")
+    return dict(np.load(path))
+
+
+def case(CG, prefix):
+    return {k[len(prefix) + 1:]: v for k, v in CG.items() if k.startswith(prefix + "_")}
+
+
+def check_case(c, r, lt, mode, bit_exact=False):
+    """Loss turns off the boundary; regular orbits within 1e-9 (or bit for bit); every other
+    survivor off the boundary no farther from the reference than the reference's own run ends
+    from itself when x and y start 1e-12 away (its measured sensitivity, `amp`); and the aperture
+    codes of particles lost in the same turn as in the reference."""
+    ref_lt, bnd, reg = c["loss"], c["boundary"], c["regular"]
+    bad = (lt != ref_lt) & ~bnd
+    assert not bad.any(), (mode, np.nonzero(bad)[0][:20], lt[bad][:20], ref_lt[bad][:20])
+    assert reg.sum() > 0
+    surv = (ref_lt < 0) & ~bnd
+    if bit_exact:
+        assert same_bits(r[surv], c["out"][surv]), mode
+    else:
+        err = rel_err_each(r[reg], c["out"][reg], c["scale"])
+        assert np.max(err) < 1e-9, (mode, float(np.max(err)))
+        err = rel_err_each(r[surv], c["out"][surv], c["scale"])
+        bar = np.maximum(1e-9, c["amp"][surv])
+        assert np.all(err <= bar), (mode, int((err > bar).sum()), float(np.max(err / bar)))
+    lost_same = (lt >= 0) & (lt == ref_lt) & ~bnd
+    assert np.all(np.isnan(r[lt >= 0, 0]))
+    assert np.array_equal(r[lost_same, 4], c["out"][lost_same, 4], equal_nan=True)
+    return int(reg.sum()), int((lt != ref_lt).sum())
+
+
+def check_area(c, lt):
+    nx, ny = (int(v) for v in c["shape"])
+    cell = (0.05 / (nx - 1)) * (0.012 / (ny - 1))
+    a_ref = MC.grid_area(c["loss"], nx, ny)
+    a = MC.grid_area(lt, nx, ny)
+    assert abs(a - a_ref) <= cell, (a, a_ref, cell)
+
+
+@pytest.mark.parametrize("mode", ["fused", "plain", "exact"])
+def test_config1_full_size(A, ctx, LT, CG, mode):
+    """The FODO, 1,024 particles, 1,000 turns: no transcendental on the path, so the plain and
+    exact modes equal the reference bit for bit; the fused mode is within 1e-9."""
+    c = case(CG, "c1")
+    line = A.Line(ctx, LT.config1_ring())
+    r = LT.config1_particles()
+    lt = np.empty(len(r), dtype=np.int32)
+    line.track(r, 1000, loss=lt, mode=MODES[mode])
+    check_case(c, r, lt, mode, bit_exact=mode != "fused")
+
+
+@pytest.mark.parametrize("mode", ["fused", "plain", "exact"])
+def test_config2_full_grid(A, ctx, LT, CG, mode):
+    """The DBA with radiation and RF, its full 101 x 51 DA grid for 1,024 turns."""
+    c = case(CG, "c2")
+    line = A.Line(ctx, LT.config2_ring())
+    r = LT.da_grid(101, 51)
+    lt = np.empty(len(r), dtype=np.int32)
+    line.track(r, 1024, loss=lt, mode=MODES[mode])
+    check_case(c, r, lt, mode)
+    check_area(c, lt)
+
+
+@pytest.mark.parametrize("mode", ["fused", "plain", "exact"])
+def test_config3_copies_full_grids(A, ctx, LT, CG, mode):
+    """Four error-seeded copies of the batched workload on their full grids, tracked together in
+    one batched call with host arrays (staged inside the call) for 1,000 turns."""
+    picks = [int(k) for k in CG["c3_copies"]]
+    sizes = LT.config3_sizes(256, 12345)
+    base = LT.config2_ring()
+    lines = [A.Line(ctx, LT.error_copy(base, k)) for k in picks]
+    grids = [LT.da_grid(*sizes[k]) for k in picks]
+    off = np.zeros(len(picks) + 1, dtype=np.int64)
+    off[1:] = np.cumsum([g.shape[0] for g in grids])
+    soa = np.ascontiguousarray(np.concatenate(grids).T)
+    lt = np.empty(int(off[-1]), dtype=np.int32)
+    A.track_batched(lines, off, soa, 1000, loss=lt, mode=MODES[mode])
+    r = soa.T.copy()
+    for j, k in enumerate(picks):
+        s = slice(off[j], off[j + 1])
+        c = case(CG, f"c3_{k}")
+        check_case(c, r[s], lt[s], f"{mode} copy {k}")
+        check_area(c, lt[s])
