@@ -118,6 +118,9 @@ def lib() -> C.CDLL:
         "accel_get_tile": (I, [P, C.POINTER(I)]),
         "accel_m66": (I, [P, I, I, D, D, I, C.POINTER(D)]),
         "accel_m66_at": (I, [P, I, I, C.POINTER(D), I, D, C.POINTER(D)]),
+        "accel_m66_knob": (I, [P, I, I, C.POINTER(D), I, P, P, P, C.POINTER(D), C.POINTER(D)]),
+        "accel_correct_tune": (I, [P, P, I, P, I, C.POINTER(D), C.POINTER(D), I, I, C.POINTER(I)]),
+        "accel_correct_chrom": (I, [P, P, I, P, I, C.POINTER(D), C.POINTER(D), I, I, C.POINTER(I)]),
         "accel_adjoint_create": (I, [P, I, I, I, P, P, P, I, C.POINTER(P)]),
         "accel_adjoint_destroy": (I, [P]),
         "accel_adjoint_forward": (I, [P, P, P]),
@@ -125,6 +128,8 @@ def lib() -> C.CDLL:
         "accel_beam_stat": (I, [P, P, I, I, C.POINTER(D), C.POINTER(D), C.POINTER(D), C.POINTER(I)]),
         "accel_beam_stat_noalloc": (I, [P, I, C.c_int64, P, P]),
         "accel_naff": (I, [P, I, D, D, C.POINTER(D)]),
+        "accel_track_diffusion": (I, [P, I, I, P, P, P, P, P, D, D, D, D, I, C.POINTER(D)]),
+        "accel_track_tune": (I, [P, I, D, D, D, D, D, D, I, C.POINTER(D), C.POINTER(D)]),
         "accel_fp64_peak": (I, [P, C.POINTER(D)]),
         "accel_set_device_memory_limit": (I, [C.c_int64]),
         "accel_set_adjoint_tape_budget": (I, [C.c_int64]),
@@ -508,11 +513,61 @@ class Line:
                "accel_track")
         return r
 
+    def track_diffusion(self, nturn, x0, y0, xlow=0.0, xhi=0.5, ylow=0.0, yhi=0.5, mode=MODE_FUSED):
+        """ALine::trackDiffusion (accel_track_diffusion): (nux, nuy, dif, total) of the points."""
+        x0 = np.ascontiguousarray(x0, dtype=np.float64)
+        y0 = np.ascontiguousarray(y0, dtype=np.float64)
+        n = len(x0)
+        nux, nuy, dif = np.zeros(n), np.zeros(n), np.zeros(n)
+        tot = C.c_double()
+        _check(lib().accel_track_diffusion(self.h, nturn, n, C.c_void_p(x0.ctypes.data), C.c_void_p(y0.ctypes.data),
+                                           C.c_void_p(nux.ctypes.data), C.c_void_p(nuy.ctypes.data),
+                                           C.c_void_p(dif.ctypes.data), xlow, xhi, ylow, yhi, mode,
+                                           C.byref(tot)), "accel_track_diffusion")
+        return nux, nuy, dif, tot.value
+
+    def track_tune(self, nturn, x0, y0, xlow=0.0, xhi=0.5, ylow=0.0, yhi=0.5, mode=MODE_FUSED):
+        """ALine::tracktune (accel_track_tune): (tunex, tuney) of one starting point."""
+        a, b = C.c_double(), C.c_double()
+        _check(lib().accel_track_tune(self.h, nturn, x0, y0, xlow, xhi, ylow, yhi, mode, C.byref(a), C.byref(b)),
+               "accel_track_tune")
+        return a.value, b.value
+
     def m66(self, dpp=0.0, delta=1e-8, method=0, st=0, ed=None) -> np.ndarray:
         m = (C.c_double * 36)()
         ed = len(self) if ed is None else ed
         _check(lib().accel_m66(self.h, st, ed, dpp, delta, method, m), "accel_m66")
         return np.array(m).reshape(6, 6)
+
+    def m66_knob(self, knob, r0=(0, 0, 0, 0, 0, 0), st=0, ed=None):
+        """(m66, dm66/dknob) for a knob moving the (element, field, index) coefficients in `knob`
+        together (accel_m66_knob): exact, from hyper-dual numbers."""
+        knob = list(knob)
+        e = np.array([k[0] for k in knob], dtype=np.int32)
+        f = np.array([k[1] for k in knob], dtype=np.int32)
+        i = np.array([k[2] for k in knob], dtype=np.int32)
+        m, dm = (C.c_double * 36)(), (C.c_double * 36)()
+        p = (C.c_double * 6)(*[float(x) for x in r0])
+        ed = len(self) if ed is None else ed
+        _check(lib().accel_m66_knob(self.h, st, ed, p, len(knob), C.c_void_p(e.ctypes.data), C.c_void_p(f.ctypes.data),
+                                    C.c_void_p(i.ctypes.data), m, dm), "accel_m66_knob")
+        return np.array(m).reshape(6, 6), np.array(dm).reshape(6, 6)
+
+    def _correct(self, fn, fam1, fam2, a, b, method, maxit):
+        f1 = np.ascontiguousarray(fam1, dtype=np.int32)
+        f2 = np.ascontiguousarray(fam2, dtype=np.int32)
+        x, y, it = C.c_double(a), C.c_double(b), C.c_int(0)
+        _check(fn(self.h, C.c_void_p(f1.ctypes.data), len(f1), C.c_void_p(f2.ctypes.data), len(f2),
+                  C.byref(x), C.byref(y), method, maxit, C.byref(it)), fn.__name__)
+        return x.value, y.value, it.value
+
+    def correct_tune(self, fam1, fam2, tunex, tuney, method=0, maxit=8):
+        """accel_correct_tune: (achieved x, y, iterations); method 0 exact Newton, 1 the reference's fit."""
+        return self._correct(lib().accel_correct_tune, fam1, fam2, tunex, tuney, method, maxit)
+
+    def correct_chrom(self, fam1, fam2, chromx, chromy, method=0, maxit=8):
+        """accel_correct_chrom: (achieved x, y, iterations); method 0 exact Newton, 1 the reference's fit."""
+        return self._correct(lib().accel_correct_chrom, fam1, fam2, chromx, chromy, method, maxit)
 
     def m66_at(self, r0, method=0, delta=1e-8, st=0, ed=None) -> np.ndarray:
         m = (C.c_double * 36)()

@@ -1170,6 +1170,57 @@ int accel_m66(accel_line* L, int st, int ed, double dpp, double delta, int metho
     return accel_m66_at(L, st, ed, r0, method, delta, m);
 }
 
+int accel_m66_knob(accel_line* L, int st, int ed, const double* r0, int nk, const int32_t* elem,
+                   const int32_t* field, const int32_t* index, double* m, double* dm) {
+    if (!L || !r0 || !m || !dm || nk <= 0 || !elem || !field || !index) return fail(ACCEL_E_INVALID, "bad argument");
+    const int ne = (int)L->desc.size();
+    if (st < 0 || ed > ne || st > ed) return fail(ACCEL_E_INVALID, "element range out of bounds");
+    // per-element knob codes: kind * 16 + coefficient index (kind 1 PolynomB, 2 PolynomA, 3 Quad K)
+    std::vector<int32_t> code((size_t)ne, 0);
+    for (int j = 0; j < nk; j++) {
+        const int e = elem[j];
+        if (e < 0 || e >= ne) return fail(ACCEL_E_INVALID, "knob element out of range");
+        const accel_elem_desc& d = L->desc[(size_t)e];
+        int c = 0;
+        if (d.type == ACCEL_STRMPOLE && (field[j] == ACCEL_F_POLYNOMB || field[j] == ACCEL_F_POLYNOMA)) {
+            if (index[j] < 0 || index[j] >= ACCEL_MAX_MPOLE) return fail(ACCEL_E_INVALID, "multipole index outside 0..9");
+            c = (field[j] == ACCEL_F_POLYNOMB ? 1 : 2) * 16 + index[j];
+        } else if (d.type == ACCEL_STRMPOLE && field[j] == ACCEL_F_K) {
+            c = 1 * 16 + 1;
+        } else if (d.type == ACCEL_QUAD && field[j] == ACCEL_F_K) {
+            c = 3 * 16;
+        } else {
+            return fail(ACCEL_E_UNSUPPORTED, std::string("no knob derivative for this field of ") + d.famname);
+        }
+        if (code[(size_t)e] != 0 && code[(size_t)e] != c)
+            return fail(ACCEL_E_UNSUPPORTED, "one knob moves two coefficients of one element");
+        code[(size_t)e] = c;
+    }
+    accel_ctx* C = L->ctx;
+    std::lock_guard<std::mutex> lk(C->mu);
+    CK(cudaSetDevice(C->device));
+    int s = line_sync(L);
+    if (s) return s;
+    if ((s = check_supported(L, st, ed))) return s;
+    for (int k = st; k < ed; k++)
+        if (is_collective(L->desc[k].type) && L->desc[k].flags)
+            return fail(ACCEL_E_UNSUPPORTED, "a transfer matrix through an active wake is not defined");
+    // scratch: r0 at 0, m at 8, dm at 48, the knob codes from double 128 on
+    if ((size_t)ne > (kScratchDoubles - 128) * 2) return fail(ACCEL_E_TOO_LARGE, "too many elements for a knob derivative");
+    if ((s = C->scratch.ensure(sizeof(double) * kScratchDoubles))) return s;
+    double* d = (double*)C->scratch.p;
+    int32_t* dk = (int32_t*)(d + 128);
+    CK(cudaMemcpyAsync(d, r0, 6 * sizeof(double), cudaMemcpyHostToDevice, C->stream));
+    CK(cudaMemcpyAsync(dk, code.data(), sizeof(int32_t) * code.size(), cudaMemcpyHostToDevice, C->stream));
+    launch_m66_knob((const DevElem*)L->d_tbl.p, st, ed, d, dk, d + 8, d + 48, C->stream);
+    C->launches += 1;
+    CK(cudaMemcpyAsync(m, d + 8, 36 * sizeof(double), cudaMemcpyDeviceToHost, C->stream));
+    CK(cudaMemcpyAsync(dm, d + 48, 36 * sizeof(double), cudaMemcpyDeviceToHost, C->stream));
+    CK(cudaStreamSynchronize(C->stream));
+    CK(cudaGetLastError());
+    return ACCEL_OK;
+}
+
 // ALine::setrfphase() (aline.cpp:465-501): cavities off, radiation on, one turn of a zero
 // particle, phi_s = asin(U0/V_tot), radiation off.  Cavities are left off, as the reference does.
 int accel_line_setrfphase(accel_line* L, double* phis_out) {

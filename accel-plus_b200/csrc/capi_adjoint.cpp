@@ -1,14 +1,20 @@
 // capi_adjoint.cpp — the forward/backward C-ABI pair of the adjoint.
 //
 // accel_adjoint_forward tracks N particles for nturn turns (literal maps, effective Horner order),
-// keeping the state at every ckpt_every-th turn.  accel_adjoint_backward then walks the segments
-// last to first: recompute the segment's turn-start states from its checkpoint, then reverse its
-// turns in chunks, last to first.  For each chunk, one wide kernel tapes every turn's unit
+// keeping the state at every ckpt_every-th turn.  The reverse pass needs, per turn, the unit
 // Jacobians (the 6x6 maps from one parameter element's output to the next one's) and the
-// parameter sensitivities, with dual numbers, and one kernel per particle sweeps them backwards
-// (kern_adjoint.cu).  The chunk is
-// as many turns of a segment as fit a 4 GB tape; when not even one turn fits, each turn is
-// reversed element by element instead (one launch per turn, an element-input tape of ne x 6 x N).
+// parameter sensitivities, taped by one wide kernel over (turn, particle), and one kernel per
+// 32-particle tile sweeps them backwards (kern_adjoint.cu).  How they are scheduled depends on
+// the tape budget (accel_set_adjoint_tape_budget; by default half of the free device memory):
+//   whole run   every turn's Jacobians fit: the forward runs in launches of 32 turns and each
+//               chunk is taped on a second stream as soon as the forward has written its turn
+//               starts, so the taping (wide, FP64-bound) runs behind the forward (one particle
+//               per thread, latency-bound); the backward is a single sweep over the run;
+//   chunks      accel_adjoint_backward walks the segments last to first: the segment's turn
+//               starts (kept by the forward when they fit, else recomputed from its checkpoint),
+//               then, chunk by chunk, last to first, the tape and its sweep;
+//   per turn    when not even one turn's tape fits, each turn is reversed element by element
+//               (one launch per turn, an element-input tape of ne x 6 x N).
 // Memory on the device: (nseg + K + 3) x 6 x N doubles for checkpoints, turn-start states, state,
 // adjoint and scratch, plus the tape.
 //
@@ -41,8 +47,22 @@ using namespace accel;
 
 namespace {
 constexpr int kMaxAdjParams = 2048;
-constexpr double kTapeBudgetDefault = 4.0e9;  // each tape: the turn starts; one chunk of Jacobians
-std::atomic<double> g_tape_budget{kTapeBudgetDefault};  // accel_set_adjoint_tape_budget
+// Device memory each tape may take (the turn starts; the Jacobians): accel_set_adjoint_tape_budget,
+// or by default half of the device memory free when the adjoint is created, at least 4e9 bytes.
+constexpr double kTapeBudgetFloor = 4.0e9;
+std::atomic<double> g_tape_budget{-1.0};  // <= 0: the default
+constexpr int kForwardChunk = 32;  // turns per forward launch when the tapes follow it chunk by chunk
+
+double tape_budget() {
+    const double b = g_tape_budget.load();
+    if (b > 0) return b;
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+        cudaGetLastError();
+        fr = 0;
+    }
+    return std::max(kTapeBudgetFloor, 0.5 * (double)fr);
+}
 
 bool dev_ptr(const void* p) {
     cudaPointerAttributes a;
@@ -64,9 +84,20 @@ struct accel_adjoint {
     int chunk = 0;               // turns per block-Jacobian tape; 0: per-turn element reversal
     bool general = true;         // the tape needs the dual-number fallback (jtape_needs_general)
     bool all_turns = false;      // turn_tape holds every turn of the run, written by the forward
+    // the Jacobian tape of every turn of the run fits the budget: the forward runs in chunks of
+    // kForwardChunk turns and each chunk's tape is written on the second stream as soon as its
+    // turn starts are out, behind the forward; the backward is then one sweep
+    bool whole = false;
+    cudaStream_t tape_stream = nullptr;
+    std::vector<cudaEvent_t> chunk_ev;  // the forward has written chunk c's turn starts
+    cudaEvent_t tape_done = nullptr;    // every tape of the last forward is written
     DevBuf st, lam, aos, tape, ckpt, turn_tape, part, meta, final_x, grad, jt, rt, pel, grow, uzd;
     bool have_forward = false;
     ~accel_adjoint() {
+        if (tape_stream) cudaStreamSynchronize(tape_stream);
+        for (cudaEvent_t e : chunk_ev) cudaEventDestroy(e);
+        if (tape_done) cudaEventDestroy(tape_done);
+        if (tape_stream) cudaStreamDestroy(tape_stream);
         for (DevBuf* b : {&st, &lam, &aos, &tape, &ckpt, &turn_tape, &part, &meta, &final_x, &grad, &jt, &rt, &pel,
                           &grow, &uzd})
             b->release();
@@ -96,7 +127,7 @@ static AdjParams params_of(accel_adjoint* J) {
 extern "C" {
 
 int accel_set_adjoint_tape_budget(int64_t bytes) {
-    g_tape_budget = bytes <= 0 ? kTapeBudgetDefault : (double)bytes;
+    g_tape_budget = bytes <= 0 ? -1.0 : (double)bytes;
     return ACCEL_OK;
 }
 
@@ -186,13 +217,14 @@ int accel_adjoint_create(accel_line* L, int N, int nturn, int every, const int32
     J->general = jtape_needs_general(L->host_tbl.data(), ne, J->pcount.data(), J->pfirst.data(), J->pkind.data());
     // every turn-start state kept by the forward when that fits the tape budget: the reverse
     // pass then recomputes nothing (otherwise each segment is recomputed from its checkpoint)
-    const double budget = g_tape_budget.load();
+    const double budget = tape_budget();
     J->all_turns = (double)s6 * nturn <= budget;
     const size_t span = (size_t)adj_tile_span(N);  // tiled tapes: 32-particle tiles
     const double per_turn = 8.0 * (double)span * (36.0 * (J->npe + 1) + 6.0 * nparam);
     J->chunk = (int)std::min<double>(std::min(every, nturn), std::floor(budget / per_turn));
+    J->whole = J->all_turns && per_turn * nturn <= budget;
     if (J->chunk >= 1) {
-        const size_t c = (size_t)J->chunk, nn = span;
+        const size_t c = (size_t)(J->whole ? nturn : J->chunk), nn = span;
         if ((s = J->jt.ensure(sizeof(double) * c * (size_t)(J->npe + 1) * 36 * nn)) ||
             (s = J->rt.ensure(sizeof(double) * std::max<size_t>(1, c * (size_t)nparam * 6 * nn))) ||
             (nparam > 384 && (s = J->grow.ensure(sizeof(double) * nn * (size_t)nparam))) ||
@@ -204,6 +236,12 @@ int accel_adjoint_create(accel_line* L, int N, int nturn, int every, const int32
         std::vector<int32_t> uz((size_t)J->npe + 1);
         jtape_unit_zd(L->host_tbl.data(), ne, J->pelem.data(), J->npe, uz.data());
         CK(cudaMemcpy(J->uzd.p, uz.data(), sizeof(int32_t) * uz.size(), cudaMemcpyHostToDevice));
+        if (J->whole) {
+            CK(cudaStreamCreateWithFlags(&J->tape_stream, cudaStreamNonBlocking));
+            J->chunk_ev.assign((size_t)((nturn + kForwardChunk - 1) / kForwardChunk), nullptr);
+            for (cudaEvent_t& e : J->chunk_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+            CK(cudaEventCreateWithFlags(&J->tape_done, cudaEventDisableTiming));
+        }
     } else {
         J->chunk = 0;
         if ((s = J->tape.ensure(s6 * (size_t)ne))) return s;
@@ -256,11 +294,33 @@ int accel_adjoint_forward(accel_adjoint* J, const double* r0, double* r_final) {
     }
     launch_aos_to_soa(in, (double*)J->st.p, J->n, s);
     AdjParams a = params_of(J);
-    launch_adj_forward(a, (double*)J->ckpt.p, J->nturn, J->every, J->all_turns ? (double*)J->turn_tape.p : nullptr,
-                       s);
+    if (J->whole) {
+        // forward in chunks; each chunk's Jacobian tape on the second stream as soon as the
+        // chunk's turn starts are written, so the taping runs behind the forward
+        const size_t span = (size_t)adj_tile_span(J->n);
+        double* jt = (double*)J->jt.p;
+        double* rt = (double*)J->rt.p;
+        int c = 0;
+        for (int t0 = 0; t0 < J->nturn; t0 += kForwardChunk, c++) {
+            const int nt = std::min(kForwardChunk, J->nturn - t0);
+            launch_adj_forward(a, (double*)J->ckpt.p, t0, nt, J->every, (double*)J->turn_tape.p, s);
+            CK(cudaEventRecord(J->chunk_ev[(size_t)c], s));
+            CK(cudaStreamWaitEvent(J->tape_stream, J->chunk_ev[(size_t)c], 0));
+            launch_adj_jtape(a, (const double*)J->turn_tape.p, t0, nt, nullptr, J->npe,
+                             jt + (size_t)t0 * (J->npe + 1) * 36 * span, rt + (size_t)t0 * J->nparam * 6 * span,
+                             J->general, J->tape_stream);
+        }
+        CK(cudaEventRecord(J->tape_done, J->tape_stream));
+        CK(cudaStreamWaitEvent(s, J->tape_done, 0));  // the call returns with the tapes written
+        C->launches += 2 * c;
+    } else {
+        launch_adj_forward(a, (double*)J->ckpt.p, 0, J->nturn, J->every,
+                           J->all_turns ? (double*)J->turn_tape.p : nullptr, s);
+        C->launches += 1;
+    }
     CK(cudaMemcpyAsync(J->final_x.p, J->st.p, sizeof(double) * (size_t)J->n, cudaMemcpyDeviceToDevice, s));
     launch_soa_to_aos((const double*)J->st.p, (double*)J->aos.p, J->n, s);
-    C->launches += 3;
+    C->launches += 2;
     if (dev_ptr(r_final)) CK(cudaMemcpyAsync(r_final, J->aos.p, s6, cudaMemcpyDeviceToDevice, s));
     else CK(cudaMemcpyAsync(r_final, J->aos.p, s6, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
@@ -287,8 +347,14 @@ int accel_adjoint_backward(accel_adjoint* J, const double* g, double* dr0, doubl
     if (J->nparam > 0) CK(cudaMemsetAsync(J->part.p, 0, sizeof(double) * (size_t)nblk * J->nparam, s));
     AdjParams a = params_of(J);
     int64_t launches = 1;
+    // the forward wrote every turn's tape: one sweep over the whole run, last turn to first
+    if (J->whole) {
+        launch_adj_jsweep(a, J->nturn, (const double*)J->final_x.p, J->npe, (const int32_t*)J->pel.p,
+                          (const double*)J->jt.p, (const double*)J->rt.p, (double*)J->grow.p, s);
+        launches++;
+    }
     // with all_turns the forward kept every turn's starting state: nothing to recompute
-    for (int seg = J->nseg - 1; seg >= 0; seg--) {
+    for (int seg = J->whole ? -1 : J->nseg - 1; seg >= 0; seg--) {
         const int t0 = seg * J->every;
         const int nt = std::min(J->every, J->nturn - t0);
         const double* tt = (const double*)J->turn_tape.p;  // this segment's turn-start states

@@ -759,9 +759,11 @@ void ALine::correctchrom(double& chromx, double& chromy, unsigned nfam1, unsigne
     calcchrom(chromx, chromy);
 }
 
-// Newton on exact one-turn matrices: tunes from the tangent map (no delta-difference noise),
-// the 2x2 response by central differences of those exact tunes, iterated until the residual
-// stops shrinking.  Returns the iterations used.
+// Newton on exact one-turn matrices: the tunes from the tangent map about (0, 0, 0, 0, 0, dp),
+// the point the reference's calctune expands about (no delta-difference noise), and their 2 x 2
+// response to the two families from the exact knob derivative of that matrix (accel_m66_knob:
+// hyper-dual numbers through every element, no difference in the knobs), iterated until the
+// residual stops shrinking.  Returns the iterations used.
 static void exact_tunes(ALine& L, double& tx, double& ty, double dp) {
     double m[36];
     L.getm66(m, 0, L.getnumber(), dp, 1e-8, true);
@@ -769,28 +771,54 @@ static void exact_tunes(ALine& L, double& tx, double& ty, double dp) {
     ty = tune_of(m, 2);
 }
 
+// The coefficients knob_add moves for a family at multipole `order`: Quad K (order 1) or
+// StrMPole PolynomB[order].
+static void family_coeffs(const ALine& L, unsigned nfam, const unsigned* lfam, int order, std::vector<int32_t>& e,
+                          std::vector<int32_t>& f, std::vector<int32_t>& i) {
+    e.clear(); f.clear(); i.clear();
+    for (unsigned j = 0; j < nfam; j++) {
+        const accel_elem_desc& d = L.element(lfam[j]);
+        if (d.type == ACCEL_QUAD && order == 1) { e.push_back((int32_t)lfam[j]); f.push_back(ACCEL_F_K); i.push_back(0); }
+        else if (d.type == ACCEL_STRMPOLE) { e.push_back((int32_t)lfam[j]); f.push_back(ACCEL_F_POLYNOMB); i.push_back(order); }
+    }
+}
+
+// Exact tunes at dp and J[k][i] = d tune_k / d family_i: tune = acos(c) / 2 pi with
+// c = (m_kk + m_k+1,k+1) / 2, so d tune = -dc / (2 pi sqrt(1 - c^2)).
+static int tune_response(ALine& L, double dp, int order, const unsigned* nf, const unsigned* const* lf,
+                         double t[2], double J[2][2]) {
+    const double r0[6] = {0, 0, 0, 0, 0, dp};
+    accel_line* line = L.device_line();
+    if (!line) return L.last_status() ? L.last_status() : ACCEL_E_INVALID;
+    for (int i = 0; i < 2; i++) {
+        std::vector<int32_t> e, f, x;
+        family_coeffs(L, nf[i], lf[i], order, e, f, x);
+        if (e.empty()) return accel::fail(ACCEL_E_INVALID, "a correction family has no magnet the knob can move");
+        double m[36], dm[36];
+        int s = accel_m66_knob(line, 0, (int)L.getnumber(), r0, (int)e.size(), e.data(), f.data(), x.data(), m, dm);
+        if (s) return s;
+        for (int k = 0; k < 2; k++) {
+            const int p = 2 * k;
+            const double c = 0.5 * (m[6 * p + p] + m[6 * (p + 1) + p + 1]);
+            const double dc = 0.5 * (dm[6 * p + p] + dm[6 * (p + 1) + p + 1]);
+            t[k] = tune_of(m, p);
+            J[k][i] = -dc / (2.0 * kPi * std::sqrt(1.0 - c * c));
+        }
+    }
+    return ACCEL_OK;
+}
+
 int ALine::correct_tune_exact(double& tunex, double& tuney, unsigned nfam1, unsigned nfam2,
                               const unsigned* lfam1, const unsigned* lfam2, int maxit) {
-    const double tgt[2] = {tunex, tuney}, h = 1e-6;
+    const double tgt[2] = {tunex, tuney};
     const unsigned* lf[2] = {lfam1, lfam2};
     unsigned nf[2] = {nfam1, nfam2};
     int it = 0;
     for (; it < maxit; it++) {
-        double t0[2];
-        exact_tunes(*this, t0[0], t0[1], 0);
+        double t0[2], J[2][2];
+        if ((status_ = tune_response(*this, 0.0, 1, nf, lf, t0, J))) return it;
         double res = std::hypot(t0[0] - tgt[0], t0[1] - tgt[1]);
         if (res < 1e-12) break;
-        double J[2][2];
-        for (int i = 0; i < 2; i++) {
-            double a[2], b[2];
-            knob_add(nf[i], lf[i], 1, h);
-            exact_tunes(*this, a[0], a[1], 0);
-            knob_add(nf[i], lf[i], 1, -2 * h);
-            exact_tunes(*this, b[0], b[1], 0);
-            knob_add(nf[i], lf[i], 1, h);
-            J[0][i] = (a[0] - b[0]) / (2 * h);
-            J[1][i] = (a[1] - b[1]) / (2 * h);
-        }
         double det = J[0][0] * J[1][1] - J[0][1] * J[1][0];
         double r0 = tgt[0] - t0[0], r1 = tgt[1] - t0[1];
         knob_add(nfam1, lfam1, 1, (J[1][1] * r0 - J[0][1] * r1) / det);
@@ -800,39 +828,38 @@ int ALine::correct_tune_exact(double& tunex, double& tuney, unsigned nfam1, unsi
     return it;
 }
 
+// Chromaticity as the reference's calcchrom defines it, the tune change over dpp = +-1e-5
+// (aline.cpp:1108-1158), here from exact tunes; its knob response from the exact knob
+// derivatives of those tunes.
+static const double kChromDpp = 1.0e-5;
+
 static void exact_chrom(ALine& L, double& cx, double& cy) {
-    const double dpp = 1.0e-5;
     double a0, a1, b0, b1;
-    exact_tunes(L, a0, a1, -dpp);
-    exact_tunes(L, b0, b1, dpp);
-    cx = (b0 - a0) / dpp / 2.0;
-    cy = (b1 - a1) / dpp / 2.0;
+    exact_tunes(L, a0, a1, -kChromDpp);
+    exact_tunes(L, b0, b1, kChromDpp);
+    cx = (b0 - a0) / kChromDpp / 2.0;
+    cy = (b1 - a1) / kChromDpp / 2.0;
 }
 
 int ALine::correct_chrom_exact(double& chromx, double& chromy, unsigned nfam1, unsigned nfam2,
                                const unsigned* lfam1, const unsigned* lfam2, int maxit) {
-    const double tgt[2] = {chromx, chromy}, h = 1e-4;
+    const double tgt[2] = {chromx, chromy};
     const unsigned* lf[2] = {lfam1, lfam2};
     unsigned nf[2] = {nfam1, nfam2};
     int it = 0;
     double prev = 1e300;
     for (; it < maxit; it++) {
-        double c0[2];
-        exact_chrom(*this, c0[0], c0[1]);
+        double tm[2], tp[2], Jm[2][2], Jp[2][2];
+        if ((status_ = tune_response(*this, -kChromDpp, 2, nf, lf, tm, Jm))) return it;
+        if ((status_ = tune_response(*this, kChromDpp, 2, nf, lf, tp, Jp))) return it;
+        double c0[2], J[2][2];
+        for (int k = 0; k < 2; k++) {
+            c0[k] = (tp[k] - tm[k]) / kChromDpp / 2.0;
+            for (int i = 0; i < 2; i++) J[k][i] = (Jp[k][i] - Jm[k][i]) / kChromDpp / 2.0;
+        }
         double res = std::hypot(c0[0] - tgt[0], c0[1] - tgt[1]);
         if (res < 1e-9 || res >= prev) break;
         prev = res;
-        double J[2][2];
-        for (int i = 0; i < 2; i++) {
-            double a[2], b[2];
-            knob_add(nf[i], lf[i], 2, h);
-            exact_chrom(*this, a[0], a[1]);
-            knob_add(nf[i], lf[i], 2, -2 * h);
-            exact_chrom(*this, b[0], b[1]);
-            knob_add(nf[i], lf[i], 2, h);
-            J[0][i] = (a[0] - b[0]) / (2 * h);
-            J[1][i] = (a[1] - b[1]) / (2 * h);
-        }
         double det = J[0][0] * J[1][1] - J[0][1] * J[1][0];
         double r0 = tgt[0] - c0[0], r1 = tgt[1] - c0[1];
         knob_add(nfam1, lfam1, 2, (J[1][1] * r0 - J[0][1] * r1) / det);
@@ -848,4 +875,80 @@ extern "C" int accel_naff(const double* data, int n, double xlow, double xhi, do
     if (!data || !nu || n < 4) return accel::fail(ACCEL_E_INVALID, "accel_naff: need data, nu and n >= 4");
     *nu = accelgpu::naff(n, data, xlow, xhi);
     return ACCEL_OK;
+}
+
+// ALine::trackDiffusion and ALine::tracktune (aline.cpp:716-779, 1159-1186) on a line of the C
+// ABI: the points are tracked together on the device one turn per call (the line's descriptors in
+// a host ALine on the same context), the NAFF analysis runs on the host.
+extern "C" int accel_track_diffusion(accel_line* L, int nturn, int np, const double* x0, const double* y0,
+                                     double* nux, double* nuy, double* dif, double xlow, double xhi,
+                                     double ylow, double yhi, int mode, double* total) {
+    if (!L || np <= 0 || nturn < 2 || !x0 || !y0 || !nux || !nuy || !dif)
+        return accel::fail(ACCEL_E_INVALID, "accel_track_diffusion: need a line, np > 0, nturn >= 2 and every array");
+    if (mode != ACCEL_MODE_FUSED && mode != ACCEL_MODE_PLAIN && mode != ACCEL_MODE_EXACT)
+        return accel::fail(ACCEL_E_INVALID, "accel_track_diffusion: bad mode");
+    accelgpu::ALine a(L->ctx, L->desc);
+    a.mode = mode;
+    const double t = a.trackDiffusion(nturn, (unsigned)np, x0, y0, nux, nuy, dif, xlow, xhi, ylow, yhi);
+    if (a.last_status()) return a.last_status();
+    if (total) *total = t;
+    return ACCEL_OK;
+}
+
+extern "C" int accel_track_tune(accel_line* L, int nturn, double x0, double y0, double xlow, double xhi,
+                                double ylow, double yhi, int mode, double* tunex, double* tuney) {
+    if (!L || nturn < 4 || !tunex || !tuney)
+        return accel::fail(ACCEL_E_INVALID, "accel_track_tune: need a line, nturn >= 4, tunex and tuney");
+    if (mode != ACCEL_MODE_FUSED && mode != ACCEL_MODE_PLAIN && mode != ACCEL_MODE_EXACT)
+        return accel::fail(ACCEL_E_INVALID, "accel_track_tune: bad mode");
+    accelgpu::ALine a(L->ctx, L->desc);
+    a.mode = mode;
+    a.tracktune(*tunex, *tuney, (unsigned)nturn, x0, y0, xlow, xhi, ylow, yhi);
+    return a.last_status();
+}
+
+// ALine::correcttune / correctchrom (aline.cpp:1243-1418) on a line of the C ABI.  method 0: Newton
+// iterations driven by exact knob derivatives (accel_m66_knob) until the residual is below 1e-12
+// (tunes) or 1e-9 (chromaticities) or stops shrinking, at most maxit; method 1: the reference's
+// fit, one step of a response built by stepping each family by 1e-5.  The families' coefficients
+// are written back to the line.
+static int correct_on_line(accel_line* L, const int32_t* fam1, int n1, const int32_t* fam2, int n2,
+                           double* a, double* b, int method, int maxit, int* iterations, bool chrom) {
+    if (!L || !fam1 || !fam2 || n1 <= 0 || n2 <= 0 || !a || !b || (method != 0 && method != 1) || maxit < 1)
+        return accel::fail(ACCEL_E_INVALID, "bad argument");
+    const int ne = (int)L->desc.size();
+    std::vector<unsigned> l1((size_t)n1), l2((size_t)n2);
+    for (int j = 0; j < n1; j++) {
+        if (fam1[j] < 0 || fam1[j] >= ne) return accel::fail(ACCEL_E_INVALID, "family element out of range");
+        l1[(size_t)j] = (unsigned)fam1[j];
+    }
+    for (int j = 0; j < n2; j++) {
+        if (fam2[j] < 0 || fam2[j] >= ne) return accel::fail(ACCEL_E_INVALID, "family element out of range");
+        l2[(size_t)j] = (unsigned)fam2[j];
+    }
+    accelgpu::ALine line(L->ctx, L->desc);
+    int it = 1;
+    if (method == 0) {
+        it = chrom ? line.correct_chrom_exact(*a, *b, (unsigned)n1, (unsigned)n2, l1.data(), l2.data(), maxit)
+                   : line.correct_tune_exact(*a, *b, (unsigned)n1, (unsigned)n2, l1.data(), l2.data(), maxit);
+    } else if (chrom) {
+        line.correctchrom(*a, *b, (unsigned)n1, (unsigned)n2, l1.data(), l2.data());
+    } else {
+        line.correcttune(*a, *b, (unsigned)n1, (unsigned)n2, l1.data(), l2.data());
+    }
+    if (line.last_status()) return line.last_status();
+    L->desc = line.descs();
+    L->dirty = true;
+    if (iterations) *iterations = it;
+    return ACCEL_OK;
+}
+
+extern "C" int accel_correct_tune(accel_line* L, const int32_t* fam1, int n1, const int32_t* fam2, int n2,
+                                  double* tunex, double* tuney, int method, int maxit, int* iterations) {
+    return correct_on_line(L, fam1, n1, fam2, n2, tunex, tuney, method, maxit, iterations, false);
+}
+
+extern "C" int accel_correct_chrom(accel_line* L, const int32_t* fam1, int n1, const int32_t* fam2, int n2,
+                                   double* chromx, double* chromy, int method, int maxit, int* iterations) {
+    return correct_on_line(L, fam1, n1, fam2, n2, chromx, chromy, method, maxit, iterations, true);
 }

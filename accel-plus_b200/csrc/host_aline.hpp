@@ -115,6 +115,7 @@ public:
                             const unsigned* lfam1, const unsigned* lfam2, int maxit = 8);
 
     accel_line* device_line();  // synced accel_line (rebuilt after host edits)
+    const std::vector<accel_elem_desc>& descs() const { return desc_; }
     accel_ctx* ctx() const { return ctx_; }
     int last_status() const { return status_; }
     int mode = ACCEL_MODE_FUSED;

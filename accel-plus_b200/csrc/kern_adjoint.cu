@@ -110,13 +110,15 @@ __device__ __forceinline__ void store6(double* s, int64_t n, int64_t p, const do
 // Forward: nturn turns from st, checkpoint every `every` turns; st ends at the final state.  With
 // turn_tape (the run's turn starts fit the tape budget) every turn's starting state is kept too,
 // so the reverse pass needs no recomputation; the states are the ones recomputing would give.
-__global__ void __launch_bounds__(kAdjThreads) k_adj_fwd(const AdjParams a, double* ckpt, int nturn, int every,
-                                                         double* turn_tape) {
+// Turns [t0, t0 + nturn) of the run: a long run may be issued as several launches in a row (st
+// carries the state from one to the next), checkpoints and turn starts indexed by the run's turn.
+__global__ void __launch_bounds__(kAdjThreads) k_adj_fwd(const AdjParams a, double* ckpt, int t0, int nturn,
+                                                         int every, double* turn_tape) {
     const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= a.n) return;
     double r[6];
     load6(a.st, a.n, p, r);
-    for (int t = 0; t < nturn; t++) {
+    for (int t = t0; t < t0 + nturn; t++) {
         if (t % every == 0) store6(ckpt + (int64_t)(t / every) * 6 * a.n, a.n, p, r);
         if (turn_tape) store6(turn_tape + (int64_t)t * 6 * a.n, a.n, p, r);
         if (!(r[0] != r[0])) fast_turn(a, r);
@@ -346,7 +348,9 @@ __global__ void __launch_bounds__(128, GENERAL ? 1 : 3) k_adj_jtape(const AdjPar
     if (gid >= n * nt) return;
     const int t = (int)(gid / n);
     const int64_t p = gid - (int64_t)t * n;
-    if (final_x[p] != final_x[p]) return;
+    // a particle lost by the end is skipped when that is known (final_x given); a tape written
+    // while the forward still runs covers every particle, and the sweep ignores the lost ones
+    if (final_x && final_x[p] != final_x[p]) return;
     const int64_t ntile = (n + kTile - 1) / kTile, b = p / kTile;
     const int l = (int)(p % kTile);
     const double* s0 = turn_tape + (int64_t)(j0 + t) * 6 * n;
@@ -482,9 +486,9 @@ __global__ void k_adj_reduce(const double* part, int nblk, int nparam, double* o
     }
 }
 
-void launch_adj_forward(const AdjParams& a, double* ckpt, int nturn, int every, double* turn_tape,
+void launch_adj_forward(const AdjParams& a, double* ckpt, int t0, int nturn, int every, double* turn_tape,
                         cudaStream_t s) {
-    k_adj_fwd<<<adj_blocks(a.n), kAdjThreads, 0, s>>>(a, ckpt, nturn, every, turn_tape);
+    k_adj_fwd<<<adj_blocks(a.n), kAdjThreads, 0, s>>>(a, ckpt, t0, nturn, every, turn_tape);
 }
 void launch_adj_recompute(const AdjParams& a, const double* ckpt, double* turn_tape, int nturn, int every,
                           int seg0, int nseg, cudaStream_t s) {

@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include "kernels.h"
+#include "hdual.cuh"
 #include "elem_literal.cuh"
 
 namespace accel {
@@ -124,6 +125,69 @@ __global__ void k_m66_fd(const DevElem* __restrict__ tbl, int e0, int e1, const 
         int row = j / 6, col = j % 6;
         m[j] = (rr[col][row] - rr[col + 6][row]) / 2.0 / delta;
     }
+}
+
+// A knob element on hyper-dual numbers: its coefficient `idx` (kind 1: StrMPole PolynomB, kind 2:
+// StrMPole PolynomA, kind 3: Quad K) carries a unit knob derivative; otherwise the literal map of
+// lit::pass, slice for slice (accel.cpp:800-847, 824-827, 193-209).
+__device__ void pass_knob(const DevElem& e, HDual* r, int kind, int idx) {
+    if (lit::is_lost(r[0])) return;
+    if (e.op == OP_QUAD) {
+        HDual K(e.v[V_QK]);
+        K.k = 1.0;
+        lit::quad6(r, e.v[V_LEN], K);
+        return;
+    }
+    HDual A[ACCEL_MAX_MPOLE], B[ACCEL_MAX_MPOLE];
+    for (int i = 0; i < ACCEL_MAX_MPOLE; i++) { A[i] = HDual(e.v[V_A + i]); B[i] = HDual(e.v[V_B + i]); }
+    if (kind == 1) B[idx].k = 1.0;
+    else A[idx].k = 1.0;
+    if (e.op == OP_STRKICK) {
+        lit::strthinkick(r, A, B, 1.0, ACCEL_MAX_MPOLE - 1);
+        return;
+    }
+    const double L1 = e.v[V_L1], L2 = e.v[V_L2], K1 = e.v[V_K1], K2 = e.v[V_K2];
+    for (int m = 0; m < e.nslice; m++) {
+        HDual norm = 1 / (1 + r[5]);
+        HDual NormL1 = L1 * norm, NormL2 = L2 * norm;
+        lit::fastdrift(r, NormL1);
+        lit::strthinkick(r, A, B, K1, ACCEL_MAX_MPOLE - 1);
+        lit::fastdrift(r, NormL2);
+        lit::strthinkick(r, A, B, K2, ACCEL_MAX_MPOLE - 1);
+        lit::fastdrift(r, NormL2);
+        lit::strthinkick(r, A, B, K1, ACCEL_MAX_MPOLE - 1);
+        lit::fastdrift(r, NormL1);
+    }
+}
+
+// Transfer matrix of [e0, e1) about r0 and its exact derivative with respect to one knob that
+// moves every coefficient knob[] names by the same amount: the literal maps on hyper-dual numbers
+// (hdual.cuh), m_ij = r_i.d[j], dm_ij = r_i.m[j].  knob[e] for element e: 0 when the knob does
+// not move it, else kind * 16 + coefficient index.
+__global__ void k_m66_knob(const DevElem* __restrict__ tbl, int e0, int e1, const double* r0,
+                           const int32_t* __restrict__ knob, double* m, double* dm) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    HDual r[6];
+    for (int i = 0; i < 6; i++) {
+        r[i] = HDual(r0[i]);
+        r[i].d[i] = 1.0;
+    }
+    lit::QeSource q{0, 0, 0, 0, 0};
+    for (int e = e0; e < e1; e++) {
+        const int kc = knob[e];
+        if (kc == 0) lit::pass<HDual>(tbl[e], r, q);
+        else pass_knob(tbl[e], r, kc >> 4, kc & 15);
+    }
+    for (int i = 0; i < 6; i++)
+        for (int j = 0; j < 6; j++) {
+            m[6 * i + j] = r[i].d[j];
+            dm[6 * i + j] = r[i].m[j];
+        }
+}
+
+void launch_m66_knob(const DevElem* tbl, int e0, int e1, const double* r0_dev, const int32_t* knob_dev,
+                     double* m_dev, double* dm_dev, cudaStream_t s) {
+    k_m66_knob<<<1, 32, 0, s>>>(tbl, e0, e1, r0_dev, knob_dev, m_dev, dm_dev);
 }
 
 void launch_m66(const DevElem* tbl, int e0, int e1, const double* r0_dev, double delta, int method,

@@ -101,6 +101,9 @@ void launch_plain_turn_end(const TrackParams& p, int32_t* turn_ctr, cudaStream_t
 void launch_exact(const TrackParams& p, int e0, int e1, int nturn, int32_t* turn_ctr, bool record,
                   cudaStream_t s);
 // exact tangent map (Dual<6>) / central differences through [e0, e1) of one table
+// transfer matrix and its exact derivative in one knob (knob codes per element: kind * 16 + index)
+void launch_m66_knob(const DevElem* tbl, int e0, int e1, const double* r0_dev, const int32_t* knob_dev,
+                     double* m_dev, double* dm_dev, cudaStream_t s);
 void launch_m66(const DevElem* tbl, int e0, int e1, const double* r0_dev, double delta, int method,
                 double* m_dev, cudaStream_t s);
 
@@ -123,7 +126,8 @@ struct AdjParams {
 };
 int adj_blocks(int64_t n);
 // turn_tape: null, or room for every turn's starting state (nturn x 6 x n doubles)
-void launch_adj_forward(const AdjParams& a, double* ckpt, int nturn, int every, double* turn_tape,
+// turns [t0, t0 + nturn) of the run; st carries the state between consecutive launches
+void launch_adj_forward(const AdjParams& a, double* ckpt, int t0, int nturn, int every, double* turn_tape,
                         cudaStream_t s);
 // turn-start states of checkpoint segments seg0 .. seg0+nseg-1 into turn_tape, from turn seg0 * every on
 void launch_adj_recompute(const AdjParams& a, const double* ckpt, double* turn_tape, int nturn, int every,

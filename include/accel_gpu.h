@@ -17,6 +17,8 @@
  *   ALine::trackDA                              accel.h:628       -> accel_track (loss turns) + host
  *   ALine::trackMA                              accel.h:630       -> accel_track_batched (start offsets)
  *   ALine::getm66                               accel.h:635-637   -> accel_m66
+ *   ALine::trackDiffusion / tracktune           accel.h:629,649   -> accel_track_diffusion / _tune
+ *   ALine::correcttune / correctchrom           accel.h:644-645   -> accel_correct_tune / _chrom
  *   ALine::deserialize / AccelElement::create   accel.h:68,607    -> accel_lattice_read
  *   ALine::serialize                            accel.h:606       -> accel_lattice_write
  *   AccelElement::setfield / getfield           accel.h:71-72     -> accel_line_set_field / get_field
@@ -277,6 +279,36 @@ int  accel_m66_at(accel_line* line, int st, int ed, const double* r0, int method
                   double* m66);
 
 /*
+ * The exact tangent-map matrix about r0 (as accel_m66_at, method 0) and its exact derivative with
+ * respect to one knob: a knob moves the nk coefficients (elem[j], field[j], index[j]) together by
+ * the same amount (StrMPole ACCEL_F_POLYNOMB / ACCEL_F_POLYNOMA with index = order, StrMPole
+ * ACCEL_F_K = PolynomB[1], Quad ACCEL_F_K), as a magnet family on one power supply does.
+ * dm66[6i+j] = d m66[6i+j] / d knob, from hyper-dual numbers through every element pass (second
+ * mixed derivatives of the map, no difference in the knob).  It replaces the difference-based
+ * knob responses of ALine::calctuneresp / calcchromresp (aline.cpp:1187-1355), which step each
+ * family by 1e-5; the tune and chromaticity corrections below are driven by it.
+ */
+int  accel_m66_knob(accel_line* line, int st, int ed, const double* r0, int nk, const int32_t* elem,
+                    const int32_t* field, const int32_t* index, double* m66, double* dm66);
+
+/*
+ * Tune and chromaticity correction with two magnet families (ALine::correcttune / correctchrom,
+ * accel.h:644-645, aline.cpp:1243-1418): fam1[n1], fam2[n2] are element indices; tune knobs move
+ * Quad K or StrMPole PolynomB[1], chromaticity knobs StrMPole PolynomB[2].  *x, *y: the targets
+ * in, the achieved values out (tunes from the one-turn matrix about (0,0,0,0,0,dpp) as calctune
+ * takes it; chromaticity as the tune change over dpp = +-1e-5, as calcchrom).
+ *   method 0: Newton iterations whose 2 x 2 response is the exact knob derivative of the tunes
+ *             (accel_m66_knob), until the residual is below 1e-12 (tunes) / 1e-9 (chromaticities)
+ *             or stops shrinking, at most maxit; *iterations gets the steps taken;
+ *   method 1: the reference's fit: one step of a response built by stepping each family by 1e-5.
+ * The families' new coefficients are written into the line.
+ */
+int  accel_correct_tune(accel_line* line, const int32_t* fam1, int n1, const int32_t* fam2, int n2,
+                        double* tunex, double* tuney, int method, int maxit, int* iterations);
+int  accel_correct_chrom(accel_line* line, const int32_t* fam1, int n1, const int32_t* fam2, int n2,
+                         double* chromx, double* chromy, int method, int maxit, int* iterations);
+
+/*
  * Reverse-mode (adjoint) pair.  Parameters are (element index, field, index) triples
  * (ACCEL_F_POLYNOMB/A of StrMPole, ACCEL_F_K of Quad).
  * accel_adjoint_forward tracks r0 (host or device, AoS, N particles) for nturn turns, keeping a
@@ -284,9 +316,11 @@ int  accel_m66_at(accel_line* line, int st, int ed, const double* r0, int method
  * accel_adjoint_backward takes dL/dr_final (AoS, 6N) and returns dL/dr0 (AoS, 6N) and
  * dL/dparams (nparam).  The reverse pass needs every turn's starting state: the forward keeps
  * them all when they fit the tape budget, else each segment is recomputed from its checkpoint.
- * It then tapes the Jacobians of a chunk of turns at once, as many as fit the budget, or, when not
- * even one turn fits, reverses turn by turn.  The three ways give the same gradient (the last to
- * round-off).
+ * When the Jacobian tape of every turn fits the budget too, the forward writes it as it goes, on
+ * a second stream behind the forward's own launches, and returns once it is written; the backward
+ * is then one sweep.  Otherwise the backward tapes the Jacobians of a chunk of turns at once, as
+ * many as fit the budget, or, when not even one turn fits, reverses turn by turn.  The ways give
+ * the same gradient (the last to round-off).
  */
 typedef struct accel_adjoint accel_adjoint;  /* holds its line (and context) until destroyed */
 int  accel_adjoint_create(accel_line* line, int N, int nturn, int ckpt_every,
@@ -296,9 +330,10 @@ int  accel_adjoint_destroy(accel_adjoint* adj);
 int  accel_adjoint_forward(accel_adjoint* adj, const double* r0, double* r_final);
 int  accel_adjoint_backward(accel_adjoint* adj, const double* dl_drfinal, double* dl_dr0,
                             double* dl_dparams);
-/* Device memory an adjoint created afterwards may give to each of its tapes (the turn starts,
- * and one chunk of Jacobians); bytes <= 0 restores the default of 4e9.  A smaller budget trades
- * speed for memory.  No counterpart in the reference (which has no reverse mode). */
+/* Device memory an adjoint created afterwards may give to each of its tapes (the turn starts;
+ * the Jacobians, of the whole run or of one chunk of turns); bytes <= 0 restores the default:
+ * half of the device memory free when the adjoint is created, at least 4e9.  A smaller budget
+ * trades speed for memory.  No counterpart in the reference (which has no reverse mode). */
 int  accel_set_adjoint_tape_budget(int64_t bytes);
 
 /* Beam moments of live particles (calc_beam_stat, utility.cpp:387-438): mean[6], sigma[6],
@@ -332,6 +367,20 @@ int  accel_beam_stat_noalloc(const double* r, int layout, int64_t N, double* out
  * line in [xlow, xhi], refined by golden-section search on the sin^4-windowed projection
  * (the reference's naff, utility.cpp:21-97). */
 int  accel_naff(const double* data, int n, double xlow, double xhi, double* nu);
+
+/* Tune diffusion of np starting points (x0[i], y0[i], the other coordinates 0), as
+ * ALine::trackDiffusion (accel.h:629, aline.cpp:716-779): each point is tracked for nt - 1 turns,
+ * nt the power of two at or above nturn (the points together on the device, in `mode`); NAFF
+ * gives the tunes of the first and second halves of the x and y records; nux, nuy receive the
+ * first half's, dif = max(-4 ln nt, ln(2 |dnu| / nt)).  A point lost by the end gives NaN in all
+ * three and counts -3 in *total (optional), the sum of dif. */
+int  accel_track_diffusion(accel_line* line, int nturn, int np, const double* x0, const double* y0,
+                           double* nux, double* nuy, double* dif, double xlow, double xhi,
+                           double ylow, double yhi, int mode, double* total);
+/* Tunes of one starting point (x0, y0) from NAFF over nt turns (nt the power of two at or above
+ * nturn), as ALine::tracktune (accel.h:649, aline.cpp:1159-1186). */
+int  accel_track_tune(accel_line* line, int nturn, double x0, double y0, double xlow, double xhi,
+                      double ylow, double yhi, int mode, double* tunex, double* tuney);
 
 /* Device FP64 FMA throughput micro-benchmark (TFLOP/s, FMA = 2 flops). */
 int  accel_fp64_peak(accel_ctx* ctx, double* tflops);

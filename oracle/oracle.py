@@ -145,6 +145,8 @@ def ref():
             "ref_trackDA": (D, [P, D, D, D, I, I, I, P, P]),
             "ref_trackMA": (D, [P, D, D, I, I, P, P, I, P]),
             "ref_beam_stat": (I, [P, I, P, P, P]), "ref_getco4": (None, [P, D, P]),
+            "ref_trackDiffusion": (D, [P, I, I, P, P, P, P, P, D, D, D, D]),
+            "ref_tracktune": (None, [P, I, D, D, D, D, D, D, pd, pd]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -254,6 +256,21 @@ class RefLine:
         area = ref().ref_trackDA(self.h, xmax, xmin, ymax, nturn, nray, nstep, rx.ctypes.data,
                                  ry.ctypes.data)
         return area, rx, ry
+
+    def trackDiffusion(self, nturn, x0, y0, xlow=0.0, xhi=0.5, ylow=0.0, yhi=0.5):
+        """ALine::trackDiffusion: (nux, nuy, dif, total) of the points (x0[i], y0[i])."""
+        x0 = np.ascontiguousarray(x0, dtype=np.float64)
+        y0 = np.ascontiguousarray(y0, dtype=np.float64)
+        n = len(x0)
+        nux, nuy, dif = np.zeros(n), np.zeros(n), np.zeros(n)
+        tot = ref().ref_trackDiffusion(self.h, nturn, n, x0.ctypes.data, y0.ctypes.data, nux.ctypes.data,
+                                       nuy.ctypes.data, dif.ctypes.data, xlow, xhi, ylow, yhi)
+        return nux, nuy, dif, tot
+
+    def tracktune(self, nturn, x0, y0, xlow=0.0, xhi=0.5, ylow=0.0, yhi=0.5):
+        a, b = C.c_double(), C.c_double()
+        ref().ref_tracktune(self.h, nturn, x0, y0, xlow, xhi, ylow, yhi, C.byref(a), C.byref(b))
+        return a.value, b.value
 
     def trackMA(self, dppmax, dppmin, nturn, nstep, lfam, threads=1):
         ref().ref_set_threads(threads)

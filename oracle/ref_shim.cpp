@@ -9,7 +9,8 @@
 //   ALine::deserialize (aline.cpp:202), ALine::pass (aline.cpp:313-363), ALine::getm66
 //   (aline.cpp:900-927), calctune/calcchrom/correctchrom (aline.cpp:1032,1108,1356),
 //   setrfphase (aline.cpp:465), trackDA (aline.cpp:607), trackMA (aline.cpp:781),
-//   set_*_onoff (aline.cpp:258,429,453), AStrMPole/ABendMPole setfield (accel.cpp:574-798).
+//   set_*_onoff (aline.cpp:258,429,453), AStrMPole/ABendMPole setfield (accel.cpp:574-798),
+//   trackDiffusion (aline.cpp:716), tracktune (aline.cpp:1159).
 #include <fstream>
 #include <string>
 #include <cmath>
@@ -164,6 +165,17 @@ double ref_trackMA(void* h, double dppmax, double dppmin, int nturn, int nstep,
                              (unsigned)nfam, l);
     delete[] l;
     return v;
+}
+
+// Tune diffusion (aline.cpp:716-779) and tracked tunes (aline.cpp:1159-1186).
+double ref_trackDiffusion(void* h, int nturn, int np, double* x0, double* y0, double* nux, double* nuy,
+                          double* dif, double xlow, double xhi, double ylow, double yhi) {
+    return L(h)->trackDiffusion(nturn, (unsigned)np, x0, y0, nux, nuy, dif, xlow, xhi, ylow, yhi);
+}
+
+void ref_tracktune(void* h, int nturn, double x0, double y0, double xlow, double xhi, double ylow,
+                   double yhi, double* tunex, double* tuney) {
+    L(h)->tracktune(*tunex, *tuney, (unsigned)nturn, x0, y0, xlow, xhi, ylow, yhi);
 }
 
 // Beam moments (utility.cpp:387-438).

@@ -77,3 +77,101 @@ def test_two_gloo_ranks():
     assert r0["sizes"] != r1["sizes"]          # each rank draws its own grids ...
     assert r0["k1"] != r1["k1"]                # ... and its own error seeds
     assert r1["ref_arm_output"] == ""          # only rank 0 runs and prints the reference arm
+
+
+WAKE_CHILD = r"""
+import json, os, sys, importlib
+from datetime import timedelta
+sys.path.insert(0, os.environ["ROOT"])
+sys.path.insert(0, os.path.join(os.environ["ROOT"], "oracle"))
+import numpy as np
+import torch
+import torch.distributed as dist
+import oracle as O
+LT = importlib.import_module("accel-plus_b200.lattices")
+
+dist.init_process_group("gloo", timeout=timedelta(seconds=60))
+rank, world = dist.get_rank(), dist.get_world_size()
+el = LT.longwake_elem(energy_mev=3000.0, charge_nc=2.0, rs=1e3, fr=10e9, q=1.0, nbins=256)
+E, charge, Rs, fr, Q, nbins = (el.f[k] for k in range(6))
+nbins = int(min(max(nbins, 1), 4096))
+
+
+def staged_wake(mine):
+    # the engine's exchange for a bunch spread over ranks: local z range and live count, their
+    # min / max / sum over ranks, the bin geometry from those, local bin counts, their sum over
+    # ranks, then the oracle's wake voltage (orc_longwake_voltage) and the kick of local particles
+    live = ~np.isnan(mine[:, 0])
+    z = mine[live, 4]
+    zmin = torch.tensor([z.min() if len(z) else np.inf], dtype=torch.float64)
+    zmax = torch.tensor([z.max() if len(z) else -np.inf], dtype=torch.float64)
+    n = torch.tensor([int(live.sum())], dtype=torch.int64)
+    dist.all_reduce(zmin, op=dist.ReduceOp.MIN)
+    dist.all_reduce(zmax, op=dist.ReduceOp.MAX)
+    dist.all_reduce(n, op=dist.ReduceOp.SUM)
+    zmin, zmax, nlive = float(zmin.item()), float(zmax.item()), int(n.item())
+    if nlive == 0:
+        return mine
+    dz = (zmax - zmin) / nbins
+    if not dz > 0:
+        dz = 1e-12
+    inv_dz = 1.0 / dz
+    b = np.clip(((z - zmin) * inv_dz).astype(np.int64), 0, nbins - 1)
+    counts = torch.tensor(np.bincount(b, minlength=nbins), dtype=torch.int64)
+    dist.all_reduce(counts, op=dist.ReduceOp.SUM)
+    qper = charge * 1e-9 / nlive
+    V = np.zeros(nbins)
+    c = np.ascontiguousarray(counts.numpy().astype(np.float64))
+    O.port().orc_longwake_voltage(nbins, dz, c.ctypes.data, qper, Rs, fr, Q, V.ctypes.data)
+    inv_e = 1.0 / (E * 1e6)
+    out = mine.copy()
+    out[np.nonzero(live)[0], 5] = mine[live, 5] - V[b] * inv_e
+    return out
+
+
+rng = np.random.default_rng(17)
+N = 20011
+r = np.zeros((N, 6))
+r[:, 0] = rng.normal(0, 1e-4, N)
+r[:, 4] = rng.normal(0, 3e-3, N)
+r[:, 5] = rng.normal(0, 1e-3, N)
+r[::97, 0] = np.nan          # lost before the wake: skipped
+r[5, 4] = r[6, 4]            # equal z on two ranks
+ref = r.copy()
+O.port_track([el], ref, 1, loss=False)   # the one-rank wake over the whole bunch
+res = {"rank": rank}
+# interleaved shards
+mine = staged_wake(r[rank::world].copy())
+res["interleaved_bit_exact"] = bool(np.array_equal(mine.view(np.int64), ref[rank::world].view(np.int64)))
+res["kicked"] = bool(np.any(mine[:, 5] != r[rank::world, 5]))
+# contiguous shards, the second holding the bunch head (largest z) and every lost particle
+order = np.argsort(np.where(np.isnan(r[:, 0]), np.inf, r[:, 4]), kind="stable")
+half = order[: N // 2] if rank == 0 else order[N // 2:]
+mine = staged_wake(r[half].copy())
+res["contiguous_bit_exact"] = bool(np.array_equal(mine.view(np.int64), ref[half].view(np.int64)))
+dist.barrier()
+dist.destroy_process_group()
+print("RESULT " + json.dumps(res))
+"""
+
+
+def test_two_gloo_ranks_split_bunch_wake():
+    """The longitudinal wake of a bunch split over two ranks, exchanged as the engine does it
+    (z range and live count by min / max / sum, then bin counts by sum): each rank's kicked
+    particles equal, bit for bit, the one-rank wake of the whole bunch (integer counts and exact
+    min / max make the exchange exact)."""
+    pytest.importorskip("torch")
+    port = free_port()
+    procs = []
+    for rank in range(2):
+        env = dict(os.environ, ROOT=ROOT, RANK=str(rank), LOCAL_RANK=str(rank), WORLD_SIZE="2",
+                   MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), CUDA_VISIBLE_DEVICES="")
+        procs.append(subprocess.Popen([sys.executable, "-c", WAKE_CHILD], env=env, cwd=ROOT,
+                                      stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True))
+    res = []
+    for p in procs:
+        out, err = p.communicate(timeout=240)
+        assert p.returncode == 0, err[-3000:]
+        res.append(json.loads([l for l in out.splitlines() if l.startswith("RESULT ")][-1][7:]))
+    for r in res:
+        assert r["interleaved_bit_exact"] and r["contiguous_bit_exact"] and r["kicked"], r
