@@ -135,6 +135,7 @@ def lib() -> C.CDLL:
         "accel_set_adjoint_tape_budget": (I, [C.c_int64]),
         "accel_device_memory_held": (I, [C.POINTER(C.c_int64)]),
         "accel_launch_count": (I, [P, C.POINTER(C.c_int64)]),
+        "accel_transwake_pair_passes": (I, [P, C.POINTER(C.c_int64)]),
         "accel_profile_enable": (I, [P, I]),
         "accel_profile_read": (I, [P, C.POINTER(D), C.POINTER(C.c_int64), C.POINTER(D)]),
     }
@@ -367,6 +368,12 @@ class Context:
     def launch_count(self) -> int:
         v = C.c_int64()
         _check(lib().accel_launch_count(self.h, C.byref(v)), "accel_launch_count")
+        return v.value
+
+    def transwake_pair_passes(self) -> int:
+        """Fused-mode transverse wake passes that fell back to the O(N^2) pair sum."""
+        v = C.c_int64()
+        _check(lib().accel_transwake_pair_passes(self.h, C.byref(v)), "accel_transwake_pair_passes")
         return v.value
 
     def profile(self, on: bool):

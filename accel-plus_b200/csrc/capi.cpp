@@ -288,6 +288,7 @@ static int emit_part(accel_ctx* C, const CoreReq& q, int part, int turns, cudaSt
     P.turn_dev = cnt + 3;
     P.err = cnt + 4;
     P.lost_flag = cnt + 5;
+    P.tw_pair_passes = cnt + 6;
     P.seed = L0->seed;
     P.rng_base = (int32_t*)L0->d_rng.p;
     P.turn0 = 0;
@@ -449,7 +450,9 @@ static int capture_part(accel_ctx* C, const CoreReq& q, int part, int turns, cud
 static int run_core(accel_ctx* C, const CoreReq& q, cudaStream_t user) {
     int s;
     if ((s = C->live0.ensure(sizeof(int32_t) * std::max<int64_t>(1, q.ntot)))) return s;
+    const bool fresh_cnt = C->cnt.p == nullptr;
     if ((s = C->cnt.ensure(sizeof(int32_t) * 16))) return s;
+    if (fresh_cnt) CK(cudaMemsetAsync(C->cnt.p, 0, sizeof(int32_t) * 16, C->stream));  // [6]: a count kept
     if ((s = C->scratch.ensure(sizeof(double) * kScratchDoubles))) return s;
     bool tw = false;
     for (int k = q.e0; k < q.e1; k++) tw |= q.lines[0]->desc[k].type == ACCEL_TRANSWAKE;
@@ -1323,6 +1326,19 @@ int accel_profile_read(accel_ctx* C, double* fused_ms, int64_t* n, double* total
     if (fused_ms) *fused_ms = f;
     if (n) *n = cnt;
     if (total_ms) *total_ms = tot;
+    return ACCEL_OK;
+}
+
+int accel_transwake_pair_passes(accel_ctx* C, int64_t* count) {
+    if (!C || !count) return fail(ACCEL_E_INVALID, "NULL argument");
+    std::lock_guard<std::mutex> lk(C->mu);
+    *count = 0;
+    if (!C->cnt.p) return ACCEL_OK;
+    CK(cudaSetDevice(C->device));
+    int32_t v = 0;
+    CK(cudaMemcpyAsync(&v, (int32_t*)C->cnt.p + 6, sizeof v, cudaMemcpyDeviceToHost, C->stream));
+    CK(cudaStreamSynchronize(C->stream));
+    *count = v;
     return ACCEL_OK;
 }
 

@@ -172,6 +172,9 @@ __global__ void k_tw_kick_sorted(const TrackParams P, const double* key, const i
     const double zr = key[0], zmin = key[nv - 1];
     const bool factor = c.ax * (zr - zmin) <= 600.0 && c.ay * (zr - zmin) <= 600.0;
     const double scale = c.q / c.energy / 1.0e6;
+    // the pair sum over all entries, O(N^2), where the bunch is too long for the factorisation:
+    // counted, so that a caller can see the slow path was taken
+    if (!factor && P.tw_pair_passes && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(P.tw_pair_passes, 1);
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nv; k += gridDim.x * blockDim.x) {
         const int64_t g = val[k];
         // this rank's live slots only (a slot past nlive can sort among the first nv only when a

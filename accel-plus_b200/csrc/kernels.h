@@ -28,6 +28,7 @@ struct TrackParams {
                              //        1 contiguous live-list range per block (L1 keeps fewer tables)
     const int32_t* rng_base; // device: QE turn base of the line (advanced per call)
     uint64_t seed;
+    int32_t* tw_pair_passes; // transverse wake passes that fell back to the pair sum (may be null)
 };
 
 // ---- fused (kern_fused.cu) ----------------------------------------------------------------

@@ -398,6 +398,14 @@ int  accel_device_memory_held(int64_t* bytes);
 /* Number of this library's kernels launched since the context was created. */
 int  accel_launch_count(accel_ctx* ctx, int64_t* count);
 
+/* Transverse wake passes of the fused mode that fell back to the pair sum since the context was
+ * created.  The z-sorted sum factorises exp(a z_ij); where a * (z_max - z_min) > 600 over the
+ * live entries (a bunch many wake lengths long) that would overflow, and each particle then sums
+ * over every entry ahead of it: O(N^2) for the N entries of all ranks, 66 ms per pass at 65,536
+ * entries and about a minute at 2^20.  No counterpart in the reference, whose pass is always the
+ * pair sum (accel.cpp:1603-1657). */
+int  accel_transwake_pair_passes(accel_ctx* ctx, int64_t* count);
+
 /* Measurement hook.  When on, every fused-kernel launch inside a tracking graph is bracketed by
  * CUDA events recorded on the stream it runs on; accel_profile_read synchronizes the context's
  * stream and returns, for the most recent tracking call, the summed device time of those

@@ -261,9 +261,10 @@ def test_config4_gradient_full_size(A, ctx, LT):
     4D DBA, checkpoints every 64 turns, with respect to every particle's initial coordinates and
     the 36 sextupole knobs (the 72 sextupoles in mirror pairs).  Checked against central
     differences taken on the GPU's exact mode (the reference's operation order), every difference
-    of the job tracked in one batched call: all 36 knobs, Richardson-extrapolated at steps 1e-3
-    and 1e-3/3 (which must agree to 3e-7), and dL/dr0 of all 4,096 particles in x, x', y, y' and
-    delta.  Tolerance 1e-6 relative."""
+    of the job tracked in one batched call: all 36 knobs, Richardson-extrapolated at steps 3e-6
+    and 1e-6 (which must agree to 3e-7; over 512 turns the loss is far from linear at larger
+    steps), and dL/dr0 of all 4,096 particles in x, x', y, y' and delta.  Tolerance 1e-6
+    relative."""
     import bench
     ring = LT.config4_ring()
     line = A.Line(ctx, ring)
@@ -282,4 +283,4 @@ def test_config4_gradient_full_size(A, ctx, LT):
     adj.close()
     assert res["knob_richardson_agreement"] < 3e-7, res
     assert res["knob_max_rel_err"] < 1e-6, res
-    assert res["coord_max_rel_err"] < 1e-6, res
+    assert res["coord_max_rel_err"] < 1e-6, res["coord"]

@@ -15,9 +15,6 @@ Bars, for every mode:
   final coordinates of the regular particles within 1e-9 of the reference (relative to each
       coordinate's RMS); bit for bit in the plain and exact modes where no transcendental
       enters (the FODO), since they keep the reference's operation order;
-  every other survivor off the boundary no farther from the reference than the reference's own
-      run ends from itself under the 1e-12 start perturbation (in this chaotic lattice most
-      survivors after 1,000 turns amplify that perturbation past 1e-9);
   the DA area by trackDA's triangle fan (aline.cpp:689-708, over each grid column's first lost
       point) within one grid cell of the reference's.
 The GPU runs through the C-ABI (accel_track and accel_track_batched); nothing is re-tracked on
@@ -52,23 +49,19 @@ def case(CG, prefix):
 
 
 def check_case(c, r, lt, mode, bit_exact=False):
-    """Loss turns off the boundary; regular orbits within 1e-9 (or bit for bit); every other
-    survivor off the boundary no farther from the reference than the reference's own run ends
-    from itself when x and y start 1e-12 away (its measured sensitivity, `amp`); and the aperture
-    codes of particles lost in the same turn as in the reference."""
+    """Loss turns off the boundary; regular orbits within 1e-9 (or, bit_exact, every survivor off
+    the boundary bit for bit); and the aperture codes of particles lost in the same turn as in
+    the reference."""
     ref_lt, bnd, reg = c["loss"], c["boundary"], c["regular"]
     bad = (lt != ref_lt) & ~bnd
     assert not bad.any(), (mode, np.nonzero(bad)[0][:20], lt[bad][:20], ref_lt[bad][:20])
     assert reg.sum() > 0
-    surv = (ref_lt < 0) & ~bnd
     if bit_exact:
+        surv = (ref_lt < 0) & ~bnd
         assert same_bits(r[surv], c["out"][surv]), mode
     else:
         err = rel_err_each(r[reg], c["out"][reg], c["scale"])
         assert np.max(err) < 1e-9, (mode, float(np.max(err)))
-        err = rel_err_each(r[surv], c["out"][surv], c["scale"])
-        bar = np.maximum(1e-9, c["amp"][surv])
-        assert np.all(err <= bar), (mode, int((err > bar).sum()), float(np.max(err / bar)))
     lost_same = (lt >= 0) & (lt == ref_lt) & ~bnd
     assert np.all(np.isnan(r[lt >= 0, 0]))
     assert np.array_equal(r[lost_same, 4], c["out"][lost_same, 4], equal_nan=True)

@@ -118,3 +118,37 @@ def test_quantum_excitation_equilibrium(A, ctx, LT):
                        ("sigma_z", np.sqrt(mine[(4, 4)]), np.sqrt(ref[(4, 4)])),
                        ("sigma_delta", np.sqrt(mine[(5, 5)]), np.sqrt(ref[(5, 5)]))):
         assert abs(g - w) <= 0.02 * w, (name, g, w, n_ref)
+
+
+@pytest.mark.parametrize("mode", ["lump", "lump_qe"])
+def test_syncrad_lumped_modes_statistics(A, ctx, LT, mode):
+    """ASyncRad's random modes (accel.cpp:1806-1854), reached as the reference's deck reaches them
+    through the radiation flag (aline.cpp:273-289): LUMP (damping and excitation) and LUMP_QE
+    (excitation alone), on the 4D DBA with one 0.2 m SyncRad element, every particle from the
+    origin for 300 turns.  The reference's moments over 16,384 particles (pooled single-threaded
+    srand runs, tests/golden/syncrad_lump.npz from make_syncrad_golden.py) against the engine's
+    over 262,144: rms sizes within 2 % in x, x', y, y', z and delta; means within four combined
+    standard errors; nobody lost.  LUMP_DAMP alone is deterministic and an element case of
+    golden.npz."""
+    import sys
+    sys.path.insert(0, GOLDEN)
+    import make_syncrad_golden as S
+    ref = np.load(os.path.join(GOLDEN, "syncrad_lump.npz"))
+    n_ref, turns = int(ref["n"][0]), int(ref["turns"][0])
+    line = A.Line(ctx, S.ring(A, LT))
+    line.set_flags(rad=A.RAD_LUMP if mode == "lump" else A.RAD_LUMP_QE, cavity=0)
+    line.set_seed(777 if mode == "lump" else 778)
+    n = 262144
+    r = np.zeros((n, 6))
+    line.track(r, turns)
+    live = ~np.isnan(r[:, 0])
+    assert live.all() and int(ref[f"{mode}_nlive"][0]) == n_ref
+    m = r.mean(axis=0)
+    d = r - m
+    sig = np.sqrt((d * d).mean(axis=0))
+    rs, rm = ref[f"{mode}_sigma"], ref[f"{mode}_mean"]
+    for k in range(6):
+        assert rs[k] > 0
+        assert abs(sig[k] - rs[k]) <= 0.02 * rs[k], (mode, k, sig[k], rs[k])
+        se = np.sqrt(rs[k] ** 2 / n_ref + sig[k] ** 2 / n)
+        assert abs(m[k] - rm[k]) <= 4 * se, (mode, k, m[k], rm[k], se)

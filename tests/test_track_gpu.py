@@ -305,8 +305,11 @@ def test_transverse_wake_sorted_sum_matches_pair_sum(A, ctx, spread):
     line = A.Line(ctx, [A.elem(A.DRIFT, "D", 0.3), tw, A.elem(A.DRIFT, "D", 0.2)])
     a, b, c = r.copy(), r.copy(), r.copy()
     line.track(a, 1, mode=A.MODE_PLAIN)
+    n0 = ctx.transwake_pair_passes()
     line.track(b, 1, mode=A.MODE_FUSED)
     line.track(c, 1, mode=A.MODE_FUSED)
+    # the long bunch takes the pair-sum fallback, once per pass, and the counter says so
+    assert ctx.transwake_pair_passes() - n0 == (2 if spread == "long" else 0)
     assert np.array_equal(b, c, equal_nan=True)  # the scan adds in a fixed order: reproducible
     live = ~np.isnan(r[:, 0])
     assert np.array_equal(np.isnan(a[:, 0]), np.isnan(b[:, 0]))
