@@ -131,6 +131,7 @@ def ref():
             "ref_set_crab": (None, [P, I]),
             "ref_pass": (None, [P, P, I, I]), "ref_pass_range": (None, [P, P, I, I, I]),
             "ref_track_loss": (None, [P, P, I, I, P]),
+            "ref_track_loss_last": (None, [P, P, I, I, P, P]),
             "ref_m66": (None, [P, I, I, D, D, P]),
             "ref_calc_tune": (None, [P, pd, pd]), "ref_calc_chrom": (None, [P, pd, pd]),
             "ref_correct_chrom": (None, [P, S, S, S, pd, pd]),
@@ -184,10 +185,16 @@ class RefLine:
         ref().ref_pass_range(self.h, r.ctypes.data, r.size // 6, st, ed)
         return r
 
-    def track_loss(self, r: np.ndarray, nturn: int, threads: int = 1) -> np.ndarray:
+    def track_loss(self, r: np.ndarray, nturn: int, threads: int = 1, last=None) -> np.ndarray:
+        """Loss turns (-1: survived) by a per-turn NaN scan; with `last` (N x 6), each particle's
+        state at the end of the last turn it survived."""
         ref().ref_set_threads(threads)
         lt = np.empty(r.size // 6, dtype=np.int32)
-        ref().ref_track_loss(self.h, r.ctypes.data, r.size // 6, nturn, lt.ctypes.data)
+        if last is None:
+            ref().ref_track_loss(self.h, r.ctypes.data, r.size // 6, nturn, lt.ctypes.data)
+        else:
+            ref().ref_track_loss_last(self.h, r.ctypes.data, r.size // 6, nturn, lt.ctypes.data,
+                                      last.ctypes.data)
         return lt
 
     def m66(self, dpp=0.0, delta=1e-8, st=0, ed=None) -> np.ndarray:

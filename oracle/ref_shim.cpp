@@ -65,6 +65,22 @@ void ref_track_loss(void* h, double* r, int N, int nturn, int* loss_turn) {
     }
 }
 
+// The same scan, also keeping in last[6N] each particle's state at the end of the last turn it
+// survived (the final state for survivors): how far perturbed runs are apart just before a loss.
+void ref_track_loss_last(void* h, double* r, int N, int nturn, int* loss_turn, double* last) {
+    for (int i = 0; i < N; i++) loss_turn[i] = -1;
+    for (int i = 0; i < 6 * N; i++) last[i] = r[i];
+    for (int t = 0; t < nturn; t++) {
+        L(h)->pass(r, N);
+        for (int i = 0; i < N; i++) {
+            if (loss_turn[i] >= 0) continue;
+            if (std::isnan(r[6 * i])) loss_turn[i] = t;
+            else
+                for (int k = 0; k < 6; k++) last[6 * i + k] = r[6 * i + k];
+        }
+    }
+}
+
 void ref_m66(void* h, int st, int ed, double dpp, double delta, double* m36) {
     Mat m(6, 6);
     L(h)->getm66(m, (unsigned)st, (unsigned)ed, dpp, delta);

@@ -23,9 +23,11 @@ plus 1e-15 m absolute).  Stored per case:
   <case>_loss      loss turn per particle (-1 = survived)
   <case>_boundary  fate changes under the perturbation, or (grids) a grid neighbour's fate
                    differs: the chaotic aperture boundary, where either fate is accepted
-  <case>_amp       how far the perturbed runs end from the unperturbed one: the largest over
-                   both signs and the six coordinates of |difference| / RMS (inf when a
-                   perturbed run loses the particle)
+  <case>_amp       how far the perturbed runs are from the unperturbed one at the end of the
+                   last turn the particle survives (the final turn for survivors): the largest
+                   over both signs and the six coordinates of |difference| / RMS (inf when a
+                   perturbed run loses the particle in another turn).  A lost particle with a
+                   large amp was on a chaotic orbit before its loss, and its loss turn is fragile
   <case>_regular   survives, off the boundary, and amp < 1e-9
   <case>_scale     that RMS per coordinate over the surviving particles
   <case>_pert_area (grids) the DA area of the two perturbed runs, for the area tolerance
@@ -106,18 +108,20 @@ def grid_area(loss: np.ndarray, nx: int, ny: int, x0=-0.025, x1=0.025, y0=0.0, y
 def classify(line, r0: np.ndarray, nturn: int, threads: int, shape=None) -> dict:
     t0 = time.perf_counter()
     out = r0.copy()
-    lt = line.track_loss(out, nturn, threads=threads)
+    last = np.empty_like(r0)
+    lt = line.track_loss(out, nturn, threads=threads, last=last)
     sc = rms_scale(out)
     sens = np.zeros(len(r0), dtype=bool)
     amp = np.zeros(len(r0))
     areas = []
     for sgn in (1.0, -1.0):
         g = perturbed(r0, sgn)
-        lg = line.track_loss(g, nturn, threads=threads)
+        gl = np.empty_like(r0)
+        lg = line.track_loss(g, nturn, threads=threads, last=gl)
         sens |= lg != lt
         with np.errstate(invalid="ignore"):
-            d = np.max(np.abs(g - out) / sc, axis=1)
-        d[np.isnan(d)] = np.inf
+            d = np.max(np.abs(gl - last) / sc, axis=1)
+        d[np.isnan(d) | (lg != lt)] = np.inf
         amp = np.maximum(amp, d)
         if shape:
             areas.append(grid_area(lg, *shape))
