@@ -104,7 +104,7 @@ accel_ctx::~accel_ctx() {
     cudaSetDevice(device);
     graphs.clear();
     for (DevBuf* b : {&state, &aos, &loss, &live0, &cnt, &tables, &tbl_off, &pinst, &scratch,
-                      &iscratch, &probe_state, &tw_scratch})
+                      &iscratch, &probe_state, &tw_scratch, &hot})
         b->release();
     for (cudaEvent_t e : prof_events) cudaEventDestroy(e);
     if (ev0) cudaEventDestroy(ev0);
@@ -227,6 +227,8 @@ struct CoreReq {
     int e0, e1, nturn, mode;
     int variant, seg, sched;
     bool probe;  // autotuning probe: no RNG advance bookkeeping
+    int grid_staged;  // staged schedule: resident blocks on the device
+    int64_t nrec;     // staged schedule: records in `tables` (instances x elements)
 };
 
 // A request is issued as four parts, each a short kernel sequence:
@@ -298,6 +300,10 @@ static int emit_part(accel_ctx* C, const CoreReq& q, int part, int turns, cudaSt
         launch_init_live(q.st, q.ntot, q.loss, live, cnt + 0, cnt + 2, 1, s);
         launch_fill_i32(cnt + 3, 0, 3, s);  // turn counter, error word, lost flag
         launches += 2;
+        if (q.mode == ACCEL_MODE_FUSED && q.sched == kSchedStaged) {
+            launch_extract_hot(q.tables, q.nrec, C->hot.p, s);  // the lines the blocks stage
+            launches++;
+        }
         return ACCEL_OK;
     }
     if (part == PART_POST) {
@@ -359,13 +365,14 @@ static int emit_part(accel_ctx* C, const CoreReq& q, int part, int turns, cudaSt
         }
     };
     if (q.mode == ACCEL_MODE_FUSED) {
-        const int grid = C->sm_count * std::max(1, C->bps[q.variant]);
+        const int grid = q.sched == kSchedStaged ? q.grid_staged : C->sm_count * std::max(1, C->bps[q.variant]);
         if (!has_collective(L0, q.e0, q.e1)) {
             P.e0 = q.e0;
             P.e1 = q.e1;
             P.nturn = turns;
             mark(0);
-            launch_fused(P, q.variant, grid, s);
+            if (q.sched == kSchedStaged) launch_fused_staged(P, q.variant, C->hot.p, (int)L0->desc.size(), grid, s);
+            else launch_fused(P, q.variant, grid, s);
             mark(1);
             launches++;
         } else {
@@ -379,7 +386,10 @@ static int emit_part(accel_ctx* C, const CoreReq& q, int part, int turns, cudaSt
                     P.e1 = b;
                     P.nturn = 1;
                     mark(0);
-                    launch_fused(P, q.variant, grid, s);
+                    if (q.sched == kSchedStaged)
+                        launch_fused_staged(P, q.variant, C->hot.p, (int)L0->desc.size(), grid, s);
+                    else
+                        launch_fused(P, q.variant, grid, s);
                     mark(1);
                     launch_fill_i32(cnt + 2, 0, 1, s);  // chunk counter for the next range
                     launches += 2;
@@ -447,6 +457,8 @@ static int capture_part(accel_ctx* C, const CoreReq& q, int part, int turns, cud
     return ACCEL_OK;
 }
 
+static int run_core_plan(accel_ctx* C, const CoreReq& q, cudaStream_t user);
+
 static int run_core(accel_ctx* C, const CoreReq& q, cudaStream_t user) {
     int s;
     if ((s = C->live0.ensure(sizeof(int32_t) * std::max<int64_t>(1, q.ntot)))) return s;
@@ -486,10 +498,31 @@ static int run_core(accel_ctx* C, const CoreReq& q, cudaStream_t user) {
     }
     if ((s = C->iscratch.ensure(sizeof(int32_t) * 4096))) return s;
     if (q.variant < 0 || q.variant >= kNumFusedVariants) return fail(ACCEL_E_INVALID, "bad variant");
-    if (C->bps[q.variant] == 0) {
-        C->bps[q.variant] = fused_blocks_per_sm(q.variant);
-        if (C->bps[q.variant] <= 0) return fail(ACCEL_E_CUDA, "fused kernel cannot be resident");
+    CoreReq qs = q;
+    if (q.mode == ACCEL_MODE_FUSED && q.sched == kSchedStaged) {
+        // the staged schedule: one instance's hot lines per block in shared memory; a line too
+        // long for shared memory runs the first schedule instead
+        const int ne = (int)q.lines[0]->desc.size();
+        const int v = q.variant < kNumStagedVariants ? q.variant : 0;
+        const int nb = staged_blocks_per_sm(v, ne);
+        if (nb <= 0) {
+            qs.sched = 0;
+        } else {
+            qs.variant = v;
+            qs.grid_staged = C->sm_count * nb;
+            qs.nrec = (int64_t)q.ninst * ne;
+            if ((s = C->hot.ensure((size_t)qs.nrec * 128))) return s;
+        }
     }
+    if (qs.sched != kSchedStaged && C->bps[qs.variant] == 0) {
+        C->bps[qs.variant] = fused_blocks_per_sm(qs.variant);
+        if (C->bps[qs.variant] <= 0) return fail(ACCEL_E_CUDA, "fused kernel cannot be resident");
+    }
+    return run_core_plan(C, qs, user);
+}
+
+// Issue a prepared request (buffers sized, schedule resolved): as graphs, or directly with events.
+static int run_core_plan(accel_ctx* C, const CoreReq& q, cudaStream_t user) {
     const Plan plan = make_plan(q, has_collective(q.lines[0], q.e0, q.e1));
     // order after the caller's prior work on `user`, run on the private stream, then order the
     // caller's stream after ours (user may be 0, the legacy default stream)
@@ -528,7 +561,7 @@ static int run_core(accel_ctx* C, const CoreReq& q, cudaStream_t user) {
                  (int64_t)q.probe, (int64_t)(intptr_t)C->live0.p, (int64_t)(intptr_t)C->cnt.p,
                  (int64_t)(intptr_t)C->scratch.p, (int64_t)(intptr_t)C->iscratch.p,
                  (int64_t)(intptr_t)C->tw_scratch.p, (int64_t)C->tw_scratch.bytes, C->tw_slots, C->tw_ntot_all,
-                 (int64_t)(intptr_t)C->comm};
+                 (int64_t)(intptr_t)C->comm, (int64_t)(intptr_t)C->hot.p, (int64_t)q.grid_staged};
         for (int i = 0; i < q.ninst && i < 4; i++) {
             key.v.push_back((int64_t)(intptr_t)q.lines[i]);
             key.v.push_back(q.lines[i]->version);
@@ -1084,7 +1117,7 @@ int accel_autotune(accel_line* const* lines, int ninst, const int64_t* part_off,
     int best_v = 0, best_sched = 0;
     float best = 1e30f;
     for (int sched = 0; sched < kNumSched; sched++)
-        for (int v = 0; v < kNumFusedVariants; v++) {
+        for (int v = 0; v < (sched == kSchedStaged ? kNumStagedVariants : kNumFusedVariants); v++) {
             float ms = 1e30f;
             for (int rep = 0; rep < 2; rep++) {
                 float m1 = 0;
@@ -1108,7 +1141,7 @@ int accel_autotune(accel_line* const* lines, int ninst, const int64_t* part_off,
     C->graphs.clear();
     C->tuned[tune_key(lines, ninst, ntot, -1)] = {best_v, best_seg, best_sched};
     if (tile_out3) {
-        tile_out3[0] = fused_variant_info(best_v).block;
+        tile_out3[0] = best_sched == kSchedStaged ? staged_variant_info(best_v).block : fused_variant_info(best_v).block;
         tile_out3[1] = best_seg;
         tile_out3[2] = best_v + 100 * best_sched;
     }
@@ -1120,7 +1153,9 @@ int accel_set_tile(accel_ctx* C, int block, int seg_turns, int variant) {
     std::lock_guard<std::mutex> lk(C->mu);
     int sched = -1;
     if (variant >= 100) { sched = variant / 100; variant %= 100; }
-    if (variant >= kNumFusedVariants || sched >= kNumSched) return fail(ACCEL_E_INVALID, "variant out of range");
+    if (variant >= kNumFusedVariants || sched >= kNumSched ||
+        (sched == kSchedStaged && variant >= kNumStagedVariants))
+        return fail(ACCEL_E_INVALID, "variant out of range");
     C->tile_sched = sched;
     if (variant < 0 && block > 0) {
         for (int v = 0; v < kNumFusedVariants; v++)
@@ -1136,7 +1171,7 @@ int accel_get_tile(accel_ctx* C, int* t) {
     if (!C || !t) return fail(ACCEL_E_INVALID, "NULL argument");
     int v, s, sc;
     default_tile(C, v, s, sc);
-    t[0] = fused_variant_info(v).block;
+    t[0] = sc == kSchedStaged ? staged_variant_info(v).block : fused_variant_info(v).block;
     t[1] = s;
     t[2] = v + 100 * sc;
     return ACCEL_OK;

@@ -33,11 +33,21 @@ struct TrackParams {
 
 // ---- fused (kern_fused.cu) ----------------------------------------------------------------
 constexpr int kNumFusedVariants = 6;
-constexpr int kNumSched = 2;
+// 0: chunks pulled per warp from an atomic counter; 1: a contiguous live-list range per block;
+// 2: per-block tasks with the instance's element hot lines staged in shared memory (staged
+//    variants, their own (block, min blocks) table)
+constexpr int kNumSched = 3;
+constexpr int kSchedStaged = 2;
+constexpr int kNumStagedVariants = 3;
 struct VariantInfo { int block; int min_blocks; };
 VariantInfo fused_variant_info(int v);
 int fused_blocks_per_sm(int variant);                     // occupancy at the variant's block
 void launch_fused(const TrackParams& p, int variant, int grid, cudaStream_t s);
+VariantInfo staged_variant_info(int v);
+int staged_blocks_per_sm(int v, int ne);  // resident blocks with ne hot lines each (0: does not fit)
+void launch_fused_staged(const TrackParams& p, int v, const void* hot, int ne, int grid, cudaStream_t s);
+// the first 128-byte line of each of nrec records, contiguous (the staged variant's source)
+void launch_extract_hot(const DevElem* tbl, int64_t nrec, void* hot, cudaStream_t s);
 // Stable compaction, in place (live == the list it compacts).  Resets the chunk counter and adds
 // `turns` to the device turn counter.  With lost_flag, the list is scanned only when the flag is
 // set (a particle was lost since the last compaction), and the flag is cleared.

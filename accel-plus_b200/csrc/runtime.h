@@ -54,7 +54,7 @@ struct accel_ctx {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     std::mutex mu;
     accel::DevBuf state, aos, loss, live0, cnt, tables, tbl_off, pinst, scratch, iscratch,
-        probe_state, tw_scratch;
+        probe_state, tw_scratch, hot;  // hot: the element records' first lines (staged schedule)
     int tile_variant = -1;  // -1: tuned or default
     int tile_seg = 0;       // 0: tuned or default
     int tile_sched = -1;    // -1: tuned or default

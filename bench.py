@@ -330,7 +330,7 @@ def adjoint_leg(A, LT, ctx, steps: int = 3, ranks=None, check: bool = True) -> d
     dknob_local = np.array([dp[knob[a]] + dp[knob[b]] for a, b in pairs])
     dknob = ranks.sum_array(dknob_local) if ranks else dknob_local
     # the gradient at this size against finite differences (this rank's particles)
-    fd_check = adjoint_fd_check(A, LT, ctx, r0, nturn, pairs, dknob_local, dr0) if check else None
+    fd_check = adjoint_fd_check(A, LT, ctx, adj, r0, nturn, pairs, elems) if check else None
     n_in = 6 * n + len(pairs)
     naive, batched = 2 * n_in, 2 * (6 + len(pairs))
     adj.close()
@@ -352,11 +352,17 @@ def adjoint_leg(A, LT, ctx, steps: int = 3, ranks=None, check: bool = True) -> d
             "timing": "wall clock around synchronous C-ABI calls, mean of %d" % steps}
 
 
-def adjoint_fd_check(A, LT, ctx, r0, nturn, pairs, dknob, dr0, knob_step=3e-6, converge=False,
-                     coords=(0, 1, 2, 3, 5)) -> dict:
-    """The adjoint's gradient of L = sum over survivors of (x^2 + y^2) against central finite
+def adjoint_fd_check(A, LT, ctx, adj, r0, nturn, pairs, elems, knob_step=3e-6, converge=False,
+                     coords=(0, 1, 2, 3, 5), amp_max=1e3) -> dict:
+    """The adjoint's gradient of L = sum over particles of (x^2 + y^2) against central finite
     differences of L taken on the GPU in the exact mode (the reference's operation order, bit for
-    bit the plain kernel), all differences of the job tracked together in one batched call:
+    bit the plain kernel), all differences of the job tracked together in one batched call.
+    A finite difference can only check a particle whose final state is a smooth function of its
+    inputs at the step sizes used: the same call tracks the bunch with x and y nudged by 1e-12
+    (relative), and particles whose nudge grows more than amp_max-fold over the run (chaotic
+    orbits: of the 4,096 Gaussian particles over 512 turns of the 4D DBA, 2 amplify it more than
+    1e7-fold) are left out of both sides: the adjoint is run with its seed dL/dr_final zero
+    there (it is linear in the seed) and the differences sum the same particles.
       knobs: each of the sextupole pairs moved by +-h and +-h/2 (Richardson-extrapolated central
         difference, error O(h^4)), h = knob_step; with `converge`, also at h/3, the estimate at
         h/3 taken and the two required to agree.  Over 512 turns the loss is far from linear in
@@ -375,6 +381,13 @@ def adjoint_fd_check(A, LT, ctx, r0, nturn, pairs, dknob, dr0, knob_step=3e-6, c
     scale = np.sqrt(np.mean(r0 ** 2, axis=0))
     steps = [knob_step] + ([knob_step / 3] if converge else [])
     rings, particles, tags = [], [], []
+    nudged = r0.copy()
+    nudged[:, 0] *= 1 + 1e-12
+    nudged[:, 2] *= 1 + 1e-12
+    for tag, p in ((("base",), r0), (("nudged",), nudged)):
+        rings.append(ring)
+        particles.append(p)
+        tags.append(tag)
     for j, (ea, eb) in enumerate(pairs):
         for h in steps:
             for dv in (h, -h, h / 2, -h / 2):
@@ -402,22 +415,42 @@ def adjoint_fd_check(A, LT, ctx, r0, nturn, pairs, dknob, dr0, knob_step=3e-6, c
                            device="cuda", dtype=torch.float64).contiguous()
         A.track_batched(ls, off, soa, nturn, mode=mode)
         torch.cuda.synchronize()
-        out = soa.cpu().numpy()
-        x, y = out[0].reshape(-1, n), out[2].reshape(-1, n)
+        return soa.cpu().numpy().reshape(6, -1, n)  # [coordinate, copy, particle]
+
+    def loss_each(out):
+        x, y = out[0], out[2]
         with np.errstate(invalid="ignore"):
             return np.where(np.isnan(x), 0.0, x * x + y * y)  # per-particle loss, each copy
 
     torch.cuda.synchronize()
     t = time.perf_counter()
-    lp = run(list(range(len(lines))), A.MODE_EXACT)
+    out = run(list(range(len(lines))), A.MODE_EXACT)
     secs = time.perf_counter() - t
     ci = [i for i, tg in enumerate(tags) if tg[0] == "coord"]
-    lp_fused = run(ci, A.MODE_FUSED)
+    lp, lp_fused = loss_each(out), loss_each(run(ci, A.MODE_FUSED))
     for l in lines:
         l.close()
+    # the particles a finite difference can check
+    fin = out[:, 0, :].T
+    sc = np.sqrt(np.nanmean(fin ** 2, axis=0))
+    sc[sc == 0] = 1.0
+    with np.errstate(invalid="ignore"):
+        growth = np.max(np.abs(out[:, 1, :].T - fin) / sc, axis=1) / 1e-12
+    keep = np.isfinite(growth) & (growth <= amp_max)
+    # the adjoint over those particles
+    rf = adj.forward(r0)
+    g = np.zeros_like(rf)
+    live = keep & ~np.isnan(rf[:, 0])
+    g[live, 0], g[live, 2] = 2 * rf[live, 0], 2 * rf[live, 2]
+    dr0, dp = adj.backward(g)
+    knob = {e: j for j, e in enumerate(elems)}
+    dknob = np.array([dp[knob[a]] + dp[knob[b]] for a, b in pairs])
     f, ff = {}, {}
     for i, tg in enumerate(tags):
-        f[tg] = lp[i].sum() if tg[0] == "knob" else lp[i]
+        if tg[0] == "knob":
+            f[tg] = lp[i][keep].sum()
+        elif tg[0] == "coord":
+            f[tg] = lp[i]
     for r, i in enumerate(ci):
         ff[tags[i]] = lp_fused[r]
 
@@ -436,21 +469,74 @@ def adjoint_fd_check(A, LT, ctx, r0, nturn, pairs, dknob, dr0, knob_step=3e-6, c
     knob_rel = np.abs(dknob - knob_fd) / np.abs(knob_fd)
     coord = {}
     for k in coords:
-        floor = 1e-3 * np.max(np.abs(dr0[:, k]))
-        out = {}
+        floor = 1e-3 * np.max(np.abs(dr0[keep, k]))
+        res = {}
         for name, tab in (("exact", f), ("fused", ff)):
             fd = rich(lambda dv, k=k, tab=tab: tab[("coord", k, cstep[k], dv)], cstep[k])
-            rel = np.abs(dr0[:, k] - fd) / np.maximum(np.abs(fd), floor)
+            rel = np.where(keep, np.abs(dr0[:, k] - fd) / np.maximum(np.abs(fd), floor), 0.0)
             w = int(np.argmax(rel))
-            out[name] = {"max_rel_err": float(rel[w]), "p99_rel_err": float(np.percentile(rel, 99)),
+            res[name] = {"max_rel_err": float(rel[w]), "p99_rel_err": float(np.percentile(rel[keep], 99)),
                          "worst_particle": w, "adjoint": float(dr0[w, k]), "fd": float(fd[w])}
-        coord[str(k)] = out
+        coord[str(k)] = res
     return {"fd_mode": "exact (the reference's operation order), all differences in one batched call",
+            "particles_checked": int(keep.sum()), "particles": n,
+            "left_out": f"{int((~keep).sum())} whose 1e-12 nudge grows more than {amp_max:g}-fold (chaotic)",
             "knobs": len(pairs), "knob_step": knob_step, "knob_max_rel_err": float(np.max(knob_rel)),
             "knob_richardson_agreement": float(np.max(conv)) if conv else None,
-            "coords_checked_per_particle": [int(k) for k in coords], "particles": n,
+            "coords_checked_per_particle": [int(k) for k in coords],
             "coord_max_rel_err": max(c["exact"]["max_rel_err"] for c in coord.values()),
             "coord": coord, "instances": len(lines), "seconds": round(secs, 2)}
+
+
+def parity_on_classified_copies(off, fused_soa, fused_loss, plain_soa=None, plain_loss=None):
+    """The timed fused run checked on the copies whose reference outputs and per-particle
+    classification are committed (tests/golden/config_golden.npz: four copies of this workload,
+    1,000 turns, by the reference library): loss turns where the fate is certain (off the
+    boundary and not chaotic); regular survivors within 1e-9 of the reference and of the plain
+    kernel; and the DA area beside the reference's and its own spread under a 1e-12 nudge."""
+    path = os.path.join(ROOT, "tests", "golden", "config_golden.npz")
+    if not os.path.exists(path):
+        return None
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    import make_config_golden as MC
+    cg = np.load(path)
+    picks = [int(k) for k in cg["c3_copies"]]
+    tot = {"regular": 0, "reg_ref": 0, "reg_plain": 0, "checked": 0, "lt_ok": 0, "worst": 0.0}
+    areas = []
+    for k in picks:
+        s = slice(int(off[k]), int(off[k + 1]))
+        ref, lt_ref = cg[f"c3_{k}_out"], cg[f"c3_{k}_loss"]
+        reg, amp, sc = cg[f"c3_{k}_regular"], cg[f"c3_{k}_amp"], cg[f"c3_{k}_scale"]
+        unc = MC.fate_uncertain(cg[f"c3_{k}_boundary"], amp)
+        r, lt = fused_soa[:, s].T, fused_loss[s]
+        with np.errstate(invalid="ignore"):
+            err = np.max(np.abs(r - ref) / sc, axis=1)
+        err[np.isnan(err)] = np.inf
+        tot["checked"] += int((~unc).sum())
+        tot["lt_ok"] += int(((lt == lt_ref) & ~unc).sum())
+        tot["regular"] += int(reg.sum())
+        tot["reg_ref"] += int((err[reg] < 1e-9).sum())
+        if reg.any():
+            tot["worst"] = max(tot["worst"], float(err[reg].max()))
+        if plain_soa is not None:
+            with np.errstate(invalid="ignore"):
+                ep = np.max(np.abs(r - plain_soa[:, s].T) / sc, axis=1)
+            tot["reg_plain"] += int((ep[reg] < 1e-9).sum())
+        nx, ny = (int(v) for v in cg[f"c3_{k}_shape"])
+        cell = (0.05 / (nx - 1)) * (0.012 / (ny - 1))
+        a_ref = MC.grid_area(lt_ref, nx, ny)
+        areas.append({"copy": k, "fused_cells_from_reference": round((MC.grid_area(lt, nx, ny) - a_ref) / cell, 1),
+                      "reference_nudged_cells": [round((a - a_ref) / cell, 1) for a in cg[f"c3_{k}_pert_area"]]})
+    return {"copies": picks, "turns": 1000, "particles_with_certain_fate": tot["checked"],
+            "loss_turns_equal_where_fate_certain": tot["lt_ok"] / max(1, tot["checked"]),
+            "regular_survivors": tot["regular"],
+            "regular_within_1e-9_of_reference": tot["reg_ref"] / max(1, tot["regular"]),
+            "regular_within_1e-9_of_plain": (tot["reg_plain"] / max(1, tot["regular"]))
+            if plain_soa is not None else None,
+            "worst_regular_rel_err": tot["worst"], "da_area": areas,
+            "classification": "tests/golden/config_golden.npz: the reference re-tracked with x, y "
+                              "moved by +-1e-12; fate uncertain on the boundary or where the nudge "
+                              "grows past 1e-3 of the beam RMS"}
 
 
 class Ranks:

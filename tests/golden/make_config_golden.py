@@ -55,6 +55,17 @@ import oracle as O  # noqa: E402
 
 EPS = 1e-12
 OUT = os.path.join(HERE, "config_golden.npz")
+# A particle whose end state (or state before its loss) moves by more than this fraction of the
+# beam RMS under the 1e-12 nudge, a billion-fold amplification, is on a chaotic orbit: its fate
+# over the run is decided at the rounding level, and in this lattice even two reference runs 1e-12
+# apart may keep it alive in both while ending O(1) apart.
+CHAOTIC_AMP = 1e-3
+
+
+def fate_uncertain(boundary, amp):
+    """The particles whose fate or loss turn a rounding-level difference may change: the
+    boundary found by the perturbed runs and the grid neighbours, plus the chaotic orbits."""
+    return boundary | (amp > CHAOTIC_AMP)
 
 
 def ref_line(elems, rad: int, cavity: int):

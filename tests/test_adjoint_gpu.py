@@ -263,8 +263,10 @@ def test_config4_gradient_full_size(A, ctx, LT):
     differences taken on the GPU's exact mode (the reference's operation order), every difference
     of the job tracked in one batched call: all 36 knobs, Richardson-extrapolated at steps 3e-6
     and 1e-6 (which must agree to 3e-7; over 512 turns the loss is far from linear at larger
-    steps), and dL/dr0 of all 4,096 particles in x, x', y, y' and delta.  Tolerance 1e-6
-    relative."""
+    steps), and dL/dr0 of every particle in x, x', y, y' and delta.  Particles whose 1e-12 nudge
+    grows more than 1,000-fold over the run (chaotic orbits, a few in the Gaussian's tails) cannot
+    be checked by any finite difference and are left out of both sides; at least 99 % remain.
+    Tolerance 1e-6 relative."""
     import bench
     ring = LT.config4_ring()
     line = A.Line(ctx, ring)
@@ -276,11 +278,9 @@ def test_config4_gradient_full_size(A, ctx, LT):
     adj = A.Adjoint(line, 4096, 512, 64, params)
     rf = adj.forward(r0)
     assert not np.isnan(rf[:, 0]).any()
-    dr0, dp = adj.backward(grad_final(rf))
-    knob = {e: j for j, e in enumerate(elems)}
-    dknob = np.array([dp[knob[a]] + dp[knob[b]] for a, b in pairs])
-    res = bench.adjoint_fd_check(A, LT, ctx, r0, 512, pairs, dknob, dr0, converge=True)
+    res = bench.adjoint_fd_check(A, LT, ctx, adj, r0, 512, pairs, elems, converge=True)
     adj.close()
+    assert res["particles_checked"] >= 0.99 * 4096, res
     assert res["knob_richardson_agreement"] < 3e-7, res
     assert res["knob_max_rel_err"] < 1e-6, res
     assert res["coord_max_rel_err"] < 1e-6, res["coord"]

@@ -6,17 +6,20 @@ library, all host threads) holds the reference's final states and loss turns for
   c2      the 18-cell DBA with radiation and RF, the full 101 x 51 grid, 1,024 turns;
   c3_<k>  four error-seeded copies of that DBA on their full grids (the smallest, the largest and
           two from the middle of the batched workload's grid sizes), 1,000 turns;
-with every particle classified by re-tracking it with x and y moved by +-1e-12: `boundary`
-(either fate is acceptable there: the fate changes under the perturbation, or a grid neighbour's
-fate differs) and `regular` (survives off the boundary with the perturbation grown to < 1e-9).
+with every particle classified by re-tracking it with x and y moved by +-1e-12.  A particle's
+fate is uncertain (make_config_golden.fate_uncertain) where the perturbation changes its loss turn,
+where a grid neighbour's fate differs, or where its orbit is chaotic (the nudge grows past 1e-3 of
+the beam RMS by the end, or by the turn before its loss); `regular` particles survive with the
+nudge grown to less than 1e-9.
 
 Bars, for every mode:
-  loss turns equal to the reference's bit for bit at every particle off the boundary;
+  loss turns equal to the reference's bit for bit at every particle whose fate is certain;
   final coordinates of the regular particles within 1e-9 of the reference (relative to each
       coordinate's RMS); bit for bit in the plain and exact modes where no transcendental
-      enters (the FODO), since they keep the reference's operation order;
-  the DA area by trackDA's triangle fan (aline.cpp:689-708, over each grid column's first lost
-      point) within one grid cell of the reference's.
+      enters (the FODO), since they keep the reference's operation order.
+The DA area (trackDA's triangle fan, aline.cpp:689-708, over each grid column's first lost point)
+is not held to a bar: at 1,000 turns it rests on chaotic points, and the reference's own runs
+1e-12 apart differ by up to 31 grid cells (pert_area in the fixture).
 The GPU runs through the C-ABI (accel_track and accel_track_batched); nothing is re-tracked on
 the CPU.
 """
@@ -52,7 +55,7 @@ def check_case(c, r, lt, mode, bit_exact=False):
     """Loss turns off the boundary; regular orbits within 1e-9 (or, bit_exact, every survivor off
     the boundary bit for bit); and the aperture codes of particles lost in the same turn as in
     the reference."""
-    ref_lt, bnd, reg = c["loss"], c["boundary"], c["regular"]
+    ref_lt, bnd, reg = c["loss"], MC.fate_uncertain(c["boundary"], c["amp"]), c["regular"]
     bad = (lt != ref_lt) & ~bnd
     assert not bad.any(), (mode, np.nonzero(bad)[0][:20], lt[bad][:20], ref_lt[bad][:20])
     assert reg.sum() > 0
@@ -66,14 +69,6 @@ def check_case(c, r, lt, mode, bit_exact=False):
     assert np.all(np.isnan(r[lt >= 0, 0]))
     assert np.array_equal(r[lost_same, 4], c["out"][lost_same, 4], equal_nan=True)
     return int(reg.sum()), int((lt != ref_lt).sum())
-
-
-def check_area(c, lt):
-    nx, ny = (int(v) for v in c["shape"])
-    cell = (0.05 / (nx - 1)) * (0.012 / (ny - 1))
-    a_ref = MC.grid_area(c["loss"], nx, ny)
-    a = MC.grid_area(lt, nx, ny)
-    assert abs(a - a_ref) <= cell, (a, a_ref, cell)
 
 
 @pytest.mark.parametrize("mode", ["fused", "plain", "exact"])
@@ -97,7 +92,6 @@ def test_config2_full_grid(A, ctx, LT, CG, mode):
     lt = np.empty(len(r), dtype=np.int32)
     line.track(r, 1024, loss=lt, mode=MODES[mode])
     check_case(c, r, lt, mode)
-    check_area(c, lt)
 
 
 @pytest.mark.parametrize("mode", ["fused", "plain", "exact"])
@@ -119,4 +113,3 @@ def test_config3_copies_full_grids(A, ctx, LT, CG, mode):
         s = slice(off[j], off[j + 1])
         c = case(CG, f"c3_{k}")
         check_case(c, r[s], lt[s], f"{mode} copy {k}")
-        check_area(c, lt[s])

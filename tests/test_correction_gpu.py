@@ -7,11 +7,11 @@ Richardson-extrapolated central differences of the exact matrix in the knob (1e-
 
 The corrections (method 0) iterate Newton with that exact 2 x 2 response; the reference's fit
 (method 1, and the reference library itself) steps each family by 1e-5 to build a response from
-difference-based tunes, whose delta = 1e-8 central differences leave tunes about 1e-8 and
-chromaticities about 1e-4 off.  Every result is judged by the same yardstick, the exact tunes
-and chromaticities of the corrected ring: the Newton iterations land within 1e-12 (tunes) and
-1e-9 (chromaticities) in a few steps, where the reference's fit, repeated as many times, stays
-orders of magnitude away.
+difference-based tunes and chromaticities.  Every result is judged by the same yardstick, the
+exact tunes and chromaticities of the corrected ring.  The Newton iterations land within 1e-12
+(tunes) and 1e-9 (chromaticities); the reference's fit, repeated as many times, ends farther
+from the target (measured here: tunes 8e-6, 2e-11, 3e-12 after one, two, three fits;
+chromaticities 1e-3, 2e-6, 2e-8), its floor set by the noise of its difference-based quantities.
 """
 from __future__ import annotations
 
@@ -95,12 +95,13 @@ def test_tune_correction_newton_against_reference_fit(A, ctx, LT, O):
     line = A.Line(ctx, ring)
     tx, ty, it = line.correct_tune(family(ring, A, "QF1"), family(ring, A, "QD1"), *target, method=0)
     got = exact_tunes(line)
-    assert np.max(np.abs(got - target)) < 1e-12 and abs(tx - target[0]) < 1e-12 and abs(ty - target[1]) < 1e-12
+    ours = np.max(np.abs(got - target))
+    assert ours < 1e-12 and abs(tx - target[0]) < 1e-12 and abs(ty - target[1]) < 1e-12
     assert 1 <= it <= 5
     # the reference's fit, repeated as many times, judged by the exact tunes of its ring
     fits = _reference_after_fits(O, A, ring, "tune", ("QF1", "QD1"), target, max(it, 3))
     res = [np.max(np.abs(exact_tunes(A.Line(ctx, _with_coeffs(ring, A, c, 1))) - target)) for c in fits]
-    assert min(res) > 100 * max(1e-14, np.max(np.abs(got - target))), res
+    assert res[it - 1] > ours and res[0] > 1e-7, (it, ours, res)
     # the engine's own restatement of the reference fit (method 1) agrees with the reference's step
     l1 = A.Line(ctx, ring)
     l1.correct_tune(family(ring, A, "QF1"), family(ring, A, "QD1"), *target, method=1)
@@ -114,8 +115,9 @@ def test_chrom_correction_newton_against_reference_fit(A, ctx, LT, O):
     line = A.Line(ctx, ring)
     cx, cy, it = line.correct_chrom(family(ring, A, "SF"), family(ring, A, "SD"), *target, method=0)
     got = exact_chrom(line)
-    assert np.max(np.abs(got - target)) < 1e-9, got
+    ours = np.max(np.abs(got - target))
+    assert ours < 1e-9, got
     assert 1 <= it <= 5
     fits = _reference_after_fits(O, A, ring, "chrom", ("SF", "SD"), target, max(it, 3))
     res = [np.max(np.abs(exact_chrom(A.Line(ctx, _with_coeffs(ring, A, c, 2))) - target)) for c in fits]
-    assert min(res) > 100 * 1e-9, res
+    assert res[it - 1] > ours and res[0] > 1e-5, (it, ours, res)
