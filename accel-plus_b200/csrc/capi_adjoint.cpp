@@ -89,15 +89,21 @@ struct accel_adjoint {
     // turn starts are out, behind the forward; the backward is then one sweep
     bool whole = false;
     cudaStream_t tape_stream = nullptr;
+    cudaStream_t fwd_stream = nullptr;  // the forward's launches, at the device's highest priority
+    cudaEvent_t fwd_ready = nullptr;    // the forward may start (after the caller's input copy)
+    cudaEvent_t fwd_done = nullptr;
     std::vector<cudaEvent_t> chunk_ev;  // the forward has written chunk c's turn starts
     cudaEvent_t tape_done = nullptr;    // every tape of the last forward is written
     DevBuf st, lam, aos, tape, ckpt, turn_tape, part, meta, final_x, grad, jt, rt, pel, grow, uzd;
     bool have_forward = false;
     ~accel_adjoint() {
         if (tape_stream) cudaStreamSynchronize(tape_stream);
+        if (fwd_stream) cudaStreamSynchronize(fwd_stream);
         for (cudaEvent_t e : chunk_ev) cudaEventDestroy(e);
-        if (tape_done) cudaEventDestroy(tape_done);
+        for (cudaEvent_t e : {tape_done, fwd_ready, fwd_done})
+            if (e) cudaEventDestroy(e);
         if (tape_stream) cudaStreamDestroy(tape_stream);
+        if (fwd_stream) cudaStreamDestroy(fwd_stream);
         for (DevBuf* b : {&st, &lam, &aos, &tape, &ckpt, &turn_tape, &part, &meta, &final_x, &grad, &jt, &rt, &pel,
                           &grow, &uzd})
             b->release();
@@ -237,7 +243,14 @@ int accel_adjoint_create(accel_line* L, int N, int nturn, int every, const int32
         jtape_unit_zd(L->host_tbl.data(), ne, J->pelem.data(), J->npe, uz.data());
         CK(cudaMemcpy(J->uzd.p, uz.data(), sizeof(int32_t) * uz.size(), cudaMemcpyHostToDevice));
         if (J->whole) {
-            CK(cudaStreamCreateWithFlags(&J->tape_stream, cudaStreamNonBlocking));
+            // the forward on the highest-priority stream: a chunk's blocks are placed ahead of
+            // the tape blocks waiting for room, so the latency-bound forward is not held back
+            int least = 0, greatest = 0;
+            CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+            CK(cudaStreamCreateWithPriority(&J->fwd_stream, cudaStreamNonBlocking, greatest));
+            CK(cudaStreamCreateWithPriority(&J->tape_stream, cudaStreamNonBlocking, least));
+            CK(cudaEventCreateWithFlags(&J->fwd_ready, cudaEventDisableTiming));
+            CK(cudaEventCreateWithFlags(&J->fwd_done, cudaEventDisableTiming));
             J->chunk_ev.assign((size_t)((nturn + kForwardChunk - 1) / kForwardChunk), nullptr);
             for (cudaEvent_t& e : J->chunk_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
             CK(cudaEventCreateWithFlags(&J->tape_done, cudaEventDisableTiming));
@@ -301,16 +314,20 @@ int accel_adjoint_forward(accel_adjoint* J, const double* r0, double* r_final) {
         double* jt = (double*)J->jt.p;
         double* rt = (double*)J->rt.p;
         int c = 0;
+        CK(cudaEventRecord(J->fwd_ready, s));
+        CK(cudaStreamWaitEvent(J->fwd_stream, J->fwd_ready, 0));
         for (int t0 = 0; t0 < J->nturn; t0 += kForwardChunk, c++) {
             const int nt = std::min(kForwardChunk, J->nturn - t0);
-            launch_adj_forward(a, (double*)J->ckpt.p, t0, nt, J->every, (double*)J->turn_tape.p, s);
-            CK(cudaEventRecord(J->chunk_ev[(size_t)c], s));
+            launch_adj_forward(a, (double*)J->ckpt.p, t0, nt, J->every, (double*)J->turn_tape.p, J->fwd_stream);
+            CK(cudaEventRecord(J->chunk_ev[(size_t)c], J->fwd_stream));
             CK(cudaStreamWaitEvent(J->tape_stream, J->chunk_ev[(size_t)c], 0));
             launch_adj_jtape(a, (const double*)J->turn_tape.p, t0, nt, nullptr, J->npe,
                              jt + (size_t)t0 * (J->npe + 1) * 36 * span, rt + (size_t)t0 * J->nparam * 6 * span,
                              J->general, J->tape_stream);
         }
+        CK(cudaEventRecord(J->fwd_done, J->fwd_stream));
         CK(cudaEventRecord(J->tape_done, J->tape_stream));
+        CK(cudaStreamWaitEvent(s, J->fwd_done, 0));
         CK(cudaStreamWaitEvent(s, J->tape_done, 0));  // the call returns with the tapes written
         C->launches += 2 * c;
     } else {
