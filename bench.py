@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint (gradient) leg")
     ap.add_argument("--adjoint-only", action="store_true",
                     help="only the adjoint leg, printed as its own JSON line (profiling runs)")
+    ap.add_argument("--no-fd-check", action="store_true",
+                    help="skip the adjoint's finite-difference check (profiling runs)")
     ap.add_argument("--wake-only", action="store_true",
                     help="time the bunch workload with its per-turn wake (2^20 particles) and exit")
     ap.add_argument("--wake-turns", type=int, default=200)
@@ -737,7 +739,7 @@ def engine_arm(args):
 
     adjoint = None
     if not args.no_adjoint:
-        adjoint = adjoint_leg(A, LT, ctx, ranks=ranks)
+        adjoint = adjoint_leg(A, LT, ctx, ranks=ranks, check=not args.no_fd_check)
 
     # the collective workloads: a 2^20-particle bunch with its per-turn longitudinal wake, and the
     # transverse wake's sorted sum against the pair sum (each rank on its own GPU)
@@ -871,18 +873,18 @@ def wake_only(turns: int, variant: int = -1):
     ctx.close()
 
 
-def adjoint_only():
+def adjoint_only(check: bool = True):
     A = importlib.import_module("accel-plus_b200")
     LT = importlib.import_module("accel-plus_b200.lattices")
     ctx = A.Context(0)
-    print(json.dumps({"adjoint": adjoint_leg(A, LT, ctx)}), flush=True)
+    print(json.dumps({"adjoint": adjoint_leg(A, LT, ctx, check=check)}), flush=True)
     ctx.close()
 
 
 def main():
     args = parse()
     if args.adjoint_only:
-        adjoint_only()
+        adjoint_only(check=not args.no_fd_check)
         return
     if args.wake_only:
         wake_only(args.wake_turns, args.variant)
