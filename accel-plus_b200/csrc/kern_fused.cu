@@ -116,7 +116,8 @@ __global__ void __launch_bounds__(BS, MINB) k_fused(const TrackParams P) {
 
 // Variant table: (block, min blocks per SM) pairs the autotuner chooses from; the launch bound
 // caps registers per thread at 65536 / (block * min_blocks).
-#define FUSED_VARIANTS(X) X(0, 128, 4) X(1, 128, 3) X(2, 256, 2) X(3, 64, 8) X(4, 128, 5) X(5, 128, 2)
+#define FUSED_VARIANTS(X) X(0, 128, 4) X(1, 128, 3) X(2, 256, 2) X(3, 64, 8) X(4, 128, 5) X(5, 128, 2) \
+    X(6, 128, 6) X(7, 128, 7)
 
 VariantInfo fused_variant_info(int v) {
     switch (v) {

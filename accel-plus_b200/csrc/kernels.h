@@ -32,7 +32,7 @@ struct TrackParams {
 };
 
 // ---- fused (kern_fused.cu) ----------------------------------------------------------------
-constexpr int kNumFusedVariants = 6;
+constexpr int kNumFusedVariants = 8;
 // 0: chunks pulled per warp from an atomic counter; 1: a contiguous live-list range per block;
 // 2: per-block tasks with the instance's element hot lines staged in shared memory (staged
 //    variants, their own (block, min blocks) table)

@@ -332,7 +332,14 @@ def adjoint_leg(A, LT, ctx, steps: int = 3, ranks=None, check: bool = True) -> d
     dknob_local = np.array([dp[knob[a]] + dp[knob[b]] for a, b in pairs])
     dknob = ranks.sum_array(dknob_local) if ranks else dknob_local
     # the gradient at this size against finite differences (this rank's particles)
-    fd_check = adjoint_fd_check(A, LT, ctx, adj, r0, nturn, pairs, elems) if check else None
+    fd_check = tangent = None
+    if check:
+        fd_check = adjoint_fd_check(A, LT, ctx, adj, r0, nturn, pairs, elems)
+        growth = fd_check.pop("growth")
+        # checked without differences over the run: the most sensitive orbits short of chaos and
+        # quiet ones
+        tangent = adjoint_tangent_check(A, LT, ctx, adj, r0, nturn, tangent_picks(growth, 4, 4),
+                                        pairs, elems, growth=growth)
     n_in = 6 * n + len(pairs)
     naive, batched = 2 * n_in, 2 * (6 + len(pairs))
     adj.close()
@@ -350,34 +357,42 @@ def adjoint_leg(A, LT, ctx, steps: int = 3, ranks=None, check: bool = True) -> d
             "fd_cost_ratio_batched": batched * t_fd / t_adj,
             "survivors": int((~np.isnan(rf[:, 0])).sum()),
             "knob_gradient_norm": float(np.linalg.norm(dknob)),
-            "fd_check": fd_check,
+            "fd_check": fd_check, "tangent_check": tangent,
             "timing": "wall clock around synchronous C-ABI calls, mean of %d" % steps}
 
 
 def adjoint_fd_check(A, LT, ctx, adj, r0, nturn, pairs, elems, knob_steps=(3e-6, 1e-6),
-                     coord_step=1e-7, coords=(0, 1, 2, 3, 5), tol_conv=1e-7) -> dict:
+                     coord_step=1e-7, coords=(0, 1, 2, 3, 5), quiet=10.0, tol_conv=1e-7) -> dict:
     """The adjoint's gradient of L = sum over particles of (x^2 + y^2) against central finite
     differences taken on the GPU in the exact mode (the reference's operation order, bit for bit
     the plain kernel), every difference of the job tracked together in one batched call.
 
-    Particles are independent, so every finite difference is taken per particle: each copy of
-    the bunch moves one knob (a sextupole pair) or one coordinate of every particle, and each
-    particle's own loss l = x^2 + y^2 gives its derivative.  Each derivative is a Richardson-
-    extrapolated central difference (steps +-h, +-h/2; error O(h^4)) at two step sizes (knobs
-    3e-6 and 1e-6; coordinates h = 1e-7 of the coordinate's spread relative to x's (1e-7 for
-    delta, whose spread is 0) and h/2).  Over 512 turns a particle's final state is smooth enough
-    at these steps only where its orbit is not too sensitive: a few particles of the Gaussian's
-    tails amplify a 1e-12 nudge more than 1e7-fold.  The check therefore covers the particles whose
-    differences have converged, i.e. whose two estimates agree to tol_conv relative for every knob
-    and coordinate, and the adjoint is run with its seed dL/dr_final restricted to them (it is
-    linear in the seed): knob gradients of their summed loss, and their dL/dr0.
+    Particles are independent, so every difference is taken per particle: each copy of the bunch
+    moves one knob (a sextupole pair) or one coordinate of every particle, and each particle's own
+    loss l = x^2 + y^2 gives its derivative, Richardson-extrapolated (steps +-h, +-h/2; error
+    O(h^4)) at two step sizes (knobs 3e-6 and 1e-6; coordinates h = 1e-7 of the spread relative to
+    x's, 1e-7 for delta, and h/2).  Over 512 turns a difference is trustworthy only on an orbit
+    that does not amplify small changes much: the same call tracks the bunch with x and y nudged
+    by 1e-12 (relative), and the check covers the quiet particles, whose nudge grows at most
+    `quiet`-fold (half of the Gaussian bunch; a few particles of its tails amplify it more than
+    1e7-fold) and whose two estimates agree to tol_conv for every knob and coordinate; the adjoint
+    is run with its seed dL/dr_final restricted to them (it is linear in the seed).
     Relative error of a knob: |adjoint - fd| / |fd|; of a coordinate entry: |adjoint - fd| /
-    max(|fd|, 1e-3 x the largest |adjoint| of that coordinate), the bar of the smaller tests."""
+    max(|fd|, 1e-3 x the largest |adjoint| of that coordinate), the bar of the smaller tests.
+    Differences over 512 turns are themselves good to about 1e-5 relative at best (steps small
+    enough to stay linear meet the rounding of the run): against the exact forward-mode
+    derivatives of adjoint_tangent_check, the exact mode's and the fused mode's differences are
+    off by 1e-6 to 1e-4 on the same particles where the adjoint agrees to 1e-7 or better.  The
+    tight check of the gradient is adjoint_tangent_check; this one shows it at the full size
+    against the only derivative the reference itself can give, its own tracking differenced."""
     import torch
     n = len(r0)
     ring = LT.config4_ring()
     scale = np.sqrt(np.mean(r0 ** 2, axis=0))
-    rings, particles, tags = [], [], []
+    nudged = r0.copy()
+    nudged[:, 0] *= 1 + 1e-12
+    nudged[:, 2] *= 1 + 1e-12
+    rings, particles, tags = [ring, ring], [r0, nudged], [("base",), ("nudged",)]
     for j, (ea, eb) in enumerate(pairs):
         for h in knob_steps:
             for dv in (h, -h, h / 2, -h / 2):
@@ -411,6 +426,7 @@ def adjoint_fd_check(A, LT, ctx, adj, r0, nturn, pairs, elems, knob_steps=(3e-6,
     out = soa.cpu().numpy().reshape(6, -1, n)
     with np.errstate(invalid="ignore"):
         lp = np.where(np.isnan(out[0]), 0.0, out[0] ** 2 + out[2] ** 2)  # [copy, particle]
+    growth = nudge_growth(out[:, 0, :].T, out[:, 1, :].T)
     f = {tg: lp[i] for i, tg in enumerate(tags)}
 
     def rich(key, h):
@@ -422,7 +438,7 @@ def adjoint_fd_check(A, LT, ctx, adj, r0, nturn, pairs, elems, knob_steps=(3e-6,
         ref = np.abs(e2) + 1e-3 * np.max(np.abs(e2))
         return np.abs(e1 - e2) <= tol_conv * ref
 
-    ok = np.ones(n, dtype=bool)
+    ok = np.isfinite(growth) & (growth <= quiet)
     kfd = np.zeros((len(pairs), n))
     for j in range(len(pairs)):
         e = [rich(lambda dv, j=j, h=h: ("knob", j, h, dv), h) for h in knob_steps]
@@ -433,14 +449,7 @@ def adjoint_fd_check(A, LT, ctx, adj, r0, nturn, pairs, elems, knob_steps=(3e-6,
         e = [rich(lambda dv, k=k, h=h: ("coord", k, h, dv), h) for h in (cstep[k], cstep[k] / 2)]
         cfd[k] = e[-1]
         ok &= converged(e[0], e[1])
-    # the adjoint over the particles whose differences converged
-    rf = adj.forward(r0)
-    g = np.zeros_like(rf)
-    live = ok & ~np.isnan(rf[:, 0])
-    g[live, 0], g[live, 2] = 2 * rf[live, 0], 2 * rf[live, 2]
-    dr0, dp = adj.backward(g)
-    knob = {e: j for j, e in enumerate(elems)}
-    dknob = np.array([dp[knob[a]] + dp[knob[b]] for a, b in pairs])
+    dr0, dknob = masked_gradient(adj, r0, ok, pairs, elems)
     knob_fd = kfd[:, ok].sum(axis=1)
     knob_rel = np.abs(dknob - knob_fd) / np.abs(knob_fd)
     coord = {}
@@ -452,21 +461,123 @@ def adjoint_fd_check(A, LT, ctx, adj, r0, nturn, pairs, elems, knob_steps=(3e-6,
                          "adjoint": float(dr0[w, k]), "fd": float(cfd[k][w])}
     return {"fd_mode": "exact (the reference's operation order), all differences in one batched call",
             "particles_checked": int(ok.sum()), "particles": n,
-            "left_out": f"{int((~ok).sum())} whose differences did not converge to {tol_conv:g} "
-                        f"(orbits too sensitive over {nturn} turns for these steps)",
+            "checked": f"the quiet particles: a 1e-12 nudge grows at most {quiet:g}-fold over {nturn} turns "
+                       f"and the differences at two steps agree to {tol_conv:g}",
             "knobs": len(pairs), "knob_steps": list(knob_steps), "knob_max_rel_err": float(np.max(knob_rel)),
             "coord_steps": "1e-7 and 5e-8 of each coordinate's spread relative to x's",
             "coords_checked_per_particle": [int(k) for k in coords],
             "coord_max_rel_err": max(c["max_rel_err"] for c in coord.values()),
-            "coord": coord, "instances": len(lines), "seconds": round(secs, 2)}
+            "coord": coord, "growth": growth, "instances": len(lines), "seconds": round(secs, 2)}
+
+
+def nudge_growth(base: np.ndarray, nudged: np.ndarray) -> np.ndarray:
+    """How many times a 1e-12 relative nudge of x and y has grown by the end: the largest over the
+    coordinates of |difference| / RMS, over 1e-12 (inf for a particle lost in either run)."""
+    sc = np.sqrt(np.nanmean(base ** 2, axis=0))
+    sc[sc == 0] = 1.0
+    with np.errstate(invalid="ignore"):
+        g = np.max(np.abs(nudged - base) / sc, axis=1) / 1e-12
+    g[~np.isfinite(g)] = np.inf
+    return g
+
+
+def masked_gradient(adj, r0, mask, pairs, elems):
+    """dL/dr0 and the knob gradients of L summed over the particles in `mask` (the adjoint's seed
+    dL/dr_final is 2x, 2y there and zero elsewhere)."""
+    rf = adj.forward(r0)
+    g = np.zeros_like(rf)
+    live = mask & ~np.isnan(rf[:, 0])
+    g[live, 0], g[live, 2] = 2 * rf[live, 0], 2 * rf[live, 2]
+    dr0, dp = adj.backward(g)
+    knob = {e: j for j, e in enumerate(elems)}
+    return dr0, np.array([dp[knob[a]] + dp[knob[b]] for a, b in pairs])
+
+
+def tangent_picks(growth: np.ndarray, n_sensitive: int, n_quiet: int, seed: int = 0) -> np.ndarray:
+    """Particles for adjoint_tangent_check: the n_sensitive whose 1e-12 nudge grows most while
+    staying at most 1e4-fold (the most sensitive orbits short of chaos), and n_quiet drawn (seeded)
+    from those whose nudge grows at most 10-fold."""
+    order = np.argsort(np.where(growth <= 1e4, growth, -1.0))
+    sens = order[-n_sensitive:]
+    quiet = np.setdiff1d(np.nonzero(growth <= 10)[0], sens)
+    q = np.random.default_rng(seed).choice(quiet, min(n_quiet, len(quiet)), replace=False)
+    return np.sort(np.concatenate([sens, q]))
+
+
+def adjoint_tangent_check(A, LT, ctx, adj, r0, nturn, pick, pairs, elems, hk=1e-3,
+                          growth=None, detail=False) -> dict:
+    """The gradient for the particles `pick` by forward-mode accumulation along each particle's
+    own exact-mode trajectory, with no difference taken across more than one turn:
+      coordinates: J = product over the turns of the exact one-turn tangent map about r_t
+        (accel_m66_at, method 0: dual numbers through the literal element maps), dL/dr0 = J^T g;
+      knobs: v_k <- M_t v_k + b_{t,k}, where b_{t,k} is the one-turn map's derivative with respect
+        to knob k at r_t (central differences of one turn at +-hk, +-hk/2, Richardson-extrapolated;
+        one turn amplifies nothing), dL/dk = g . v_k;
+    with g = dl/dr_final = (2x, 0, 2y, 0, 0, 0).  Against the adjoint (reverse mode through the
+    fused maps) this holds for particles of any sensitivity short of chaos, where differences over
+    the whole run no longer converge.  Relative errors: dL/dr0 per particle, the largest
+    |adjoint - tangent| over the coordinates over the largest |tangent|; the knobs, over the
+    particles together, the largest |adjoint - tangent| over the largest |tangent|."""
+    ring = LT.config4_ring()
+    line = A.Line(ctx, ring)
+    kr = []
+    for ea, eb in pairs:
+        for dv in (hk, -hk, hk / 2, -hk / 2):
+            rr = [d.copy() for d in ring]
+            rr[ea].poly_b[2] += dv
+            rr[eb].poly_b[2] += dv
+            kr.append(rr)
+    klines = [A.Line(ctx, rr) for rr in kr]
+    m, nk = len(pick), len(pairs)
+    off = np.arange(len(klines) + 1, dtype=np.int64) * m
+    r = np.ascontiguousarray(r0[pick])
+    J = np.tile(np.eye(6), (m, 1, 1))
+    V = np.zeros((m, nk, 6))
+    for _ in range(nturn):
+        soa = np.ascontiguousarray(np.tile(r, (len(klines), 1)).T)
+        A.track_batched(klines, off, soa, 1, mode=A.MODE_EXACT)
+        out = soa.T.reshape(nk, 4, m, 6)
+        d1 = (out[:, 0] - out[:, 1]) / (2 * hk)
+        d2 = (out[:, 2] - out[:, 3]) / hk
+        b = (4 * d2 - d1) / 3
+        for q in range(m):
+            M = line.m66_at(r[q], method=0)
+            J[q] = M @ J[q]
+            V[q] = V[q] @ M.T + b[:, q, :]
+        line.track(r, 1, mode=A.MODE_EXACT)
+    for l in klines:
+        l.close()
+    line.close()
+    g = np.zeros((m, 6))
+    g[:, 0], g[:, 2] = 2 * r[:, 0], 2 * r[:, 2]
+    tangent = np.einsum("qij,qi->qj", J, g)
+    tknob = np.einsum("qkj,qj->k", V, g)
+    mask = np.zeros(len(r0), dtype=bool)
+    mask[pick] = True
+    dr0, dknob = masked_gradient(adj, r0, mask, pairs, elems)
+    err = np.max(np.abs(dr0[pick] - tangent), axis=1) / np.max(np.abs(tangent), axis=1)
+    kerr = np.max(np.abs(dknob - tknob)) / np.max(np.abs(tknob))
+    res = {} if not detail else {"dr0": tangent.tolist(),
+                                 "knob_each": np.einsum("qkj,qj->qk", V, g).tolist()}
+    if growth is not None:
+        gp = np.maximum(growth[pick], 10.0)
+        res |= {"growth": [float(x) for x in growth[pick]],
+                "coord_err_per_growth_max": float(np.max(err / gp))}
+    return res | {"particles": [int(p) for p in pick], "coord_max_rel_err": float(np.max(err)),
+            "coord_rel_err": [float(e) for e in err], "knob_max_rel_err": float(kerr),
+            "method": "forward mode along each particle's exact-mode trajectory: exact one-turn "
+                      f"tangent maps; knob terms from one-turn differences (+-{hk:g}, Richardson)"}
 
 
 def parity_on_classified_copies(off, fused_soa, fused_loss, plain_soa=None, plain_loss=None):
     """The timed fused run checked on the copies whose reference outputs and per-particle
     classification are committed (tests/golden/config_golden.npz: four copies of this workload,
     1,000 turns, by the reference library): loss turns where the fate is certain (off the
-    boundary and not chaotic); regular survivors within 1e-9 of the reference and of the plain
-    kernel; and the DA area beside the reference's and its own spread under a 1e-12 nudge."""
+    boundary and not chaotic); every survivor of certain fate against its own spread (its error
+    over `amp`, what a 1e-12 nudge of its start grows to in the reference; the parity tests bar
+    50 for the fused mode); regular survivors (amp < 1e-10) within 1e-9 of the reference and of
+    the plain kernel; and the DA area beside the reference's and its own spread under a 1e-12
+    nudge."""
     path = os.path.join(ROOT, "tests", "golden", "config_golden.npz")
     if not os.path.exists(path):
         return None
@@ -474,19 +585,25 @@ def parity_on_classified_copies(off, fused_soa, fused_loss, plain_soa=None, plai
     import make_config_golden as MC
     cg = np.load(path)
     picks = [int(k) for k in cg["c3_copies"]]
-    tot = {"regular": 0, "reg_ref": 0, "reg_plain": 0, "checked": 0, "lt_ok": 0, "worst": 0.0}
+    tot = {"regular": 0, "reg_ref": 0, "reg_plain": 0, "checked": 0, "lt_ok": 0, "worst": 0.0,
+           "surv": 0, "spread": 0.0}
     areas = []
     for k in picks:
         s = slice(int(off[k]), int(off[k + 1]))
         ref, lt_ref = cg[f"c3_{k}_out"], cg[f"c3_{k}_loss"]
-        reg, amp, sc = cg[f"c3_{k}_regular"], cg[f"c3_{k}_amp"], cg[f"c3_{k}_scale"]
+        amp, sc = cg[f"c3_{k}_amp"], cg[f"c3_{k}_scale"]
         unc = MC.fate_uncertain(cg[f"c3_{k}_boundary"], amp)
+        surv = (lt_ref < 0) & ~unc
+        reg = surv & (amp < MC.REGULAR_AMP)
         r, lt = fused_soa[:, s].T, fused_loss[s]
         with np.errstate(invalid="ignore"):
             err = np.max(np.abs(r - ref) / sc, axis=1)
         err[np.isnan(err)] = np.inf
         tot["checked"] += int((~unc).sum())
         tot["lt_ok"] += int(((lt == lt_ref) & ~unc).sum())
+        tot["surv"] += int(surv.sum())
+        if surv.any():
+            tot["spread"] = max(tot["spread"], float(np.max(err[surv] / np.maximum(amp[surv], 1e-12))))
         tot["regular"] += int(reg.sum())
         tot["reg_ref"] += int((err[reg] < 1e-9).sum())
         if reg.any():
@@ -502,6 +619,8 @@ def parity_on_classified_copies(off, fused_soa, fused_loss, plain_soa=None, plai
                       "reference_nudged_cells": [round((a - a_ref) / cell, 1) for a in cg[f"c3_{k}_pert_area"]]})
     return {"copies": picks, "turns": 1000, "particles_with_certain_fate": tot["checked"],
             "loss_turns_equal_where_fate_certain": tot["lt_ok"] / max(1, tot["checked"]),
+            "survivors_with_certain_fate": tot["surv"],
+            "max_error_over_reference_spread": tot["spread"],
             "regular_survivors": tot["regular"],
             "regular_within_1e-9_of_reference": tot["reg_ref"] / max(1, tot["regular"]),
             "regular_within_1e-9_of_plain": (tot["reg_plain"] / max(1, tot["regular"]))
@@ -509,7 +628,7 @@ def parity_on_classified_copies(off, fused_soa, fused_loss, plain_soa=None, plai
             "worst_regular_rel_err": tot["worst"], "da_area": areas,
             "classification": "tests/golden/config_golden.npz: the reference re-tracked with x, y "
                               "moved by +-1e-12; fate uncertain on the boundary or where the nudge "
-                              "grows past 1e-3 of the beam RMS"}
+                              "grows past 1e-3 of the beam RMS; regular: the nudge grows below 1e-10"}
 
 
 class Ranks:

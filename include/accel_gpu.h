@@ -261,7 +261,9 @@ int  accel_track_batched(accel_line* const* lines, int ninst, const int64_t* par
 
 /* Autotuner control: tile = {block, turns per segment (compaction cadence), variant}, where
  * variant = register-cap variant + 100 x scheduling mode (0: chunks of 32 particles pulled per
- * warp from an atomic counter; 1: a contiguous live-list range per block). */
+ * warp from an atomic counter; 1: a contiguous live-list range per block; 2: blocks of live
+ * particles with their instance's element hot lines staged in shared memory).  Register-cap
+ * variants 0-7 for modes 0 and 1, 0-2 for mode 2. */
 int  accel_autotune(accel_line* const* lines, int ninst, const int64_t* part_off,
                     const double* r_soa, int64_t ntot, int* tile_out3);
 int  accel_set_tile(accel_ctx* ctx, int block, int seg_turns, int variant);  /* 0s = auto */

@@ -28,7 +28,8 @@ plus 1e-15 m absolute).  Stored per case:
                    over both signs and the six coordinates of |difference| / RMS (inf when a
                    perturbed run loses the particle in another turn).  A lost particle with a
                    large amp was on a chaotic orbit before its loss, and its loss turn is fragile
-  <case>_regular   survives, off the boundary, and amp < 1e-9
+  <case>_regular   survives, off the boundary, and amp < REGULAR_AMP (1e-10: the nudge grows at
+                   most 100-fold)
   <case>_scale     that RMS per coordinate over the surviving particles
   <case>_pert_area (grids) the DA area of the two perturbed runs, for the area tolerance
   c3_copies        the copy indices; <case>_shape (nx, ny) for grids
@@ -60,6 +61,8 @@ OUT = os.path.join(HERE, "config_golden.npz")
 # over the run is decided at the rounding level, and in this lattice even two reference runs 1e-12
 # apart may keep it alive in both while ending O(1) apart.
 CHAOTIC_AMP = 1e-3
+# a regular orbit: the 1e-12 nudge grows at most 100-fold by the end
+REGULAR_AMP = 1e-10
 
 
 def fate_uncertain(boundary, amp):
@@ -149,7 +152,7 @@ def classify(line, r0: np.ndarray, nturn: int, threads: int, shape=None) -> dict
                 xd = slice(max(0, -dx), nx + min(0, -dx))
                 near[yd, xd] |= fate[ys, xs] != fate[yd, xd]
         boundary |= near.ravel()
-    regular = (lt < 0) & ~boundary & (amp < 1e-9)
+    regular = (lt < 0) & ~boundary & (amp < REGULAR_AMP)
     res = {"out": out, "loss": lt.astype(np.int32), "boundary": boundary, "regular": regular,
            "scale": sc, "amp": amp}
     if shape:

@@ -9,14 +9,21 @@ library, all host threads) holds the reference's final states and loss turns for
 with every particle classified by re-tracking it with x and y moved by +-1e-12.  A particle's
 fate is uncertain (make_config_golden.fate_uncertain) where the perturbation changes its loss turn,
 where a grid neighbour's fate differs, or where its orbit is chaotic (the nudge grows past 1e-3 of
-the beam RMS by the end, or by the turn before its loss); `regular` particles survive with the
-nudge grown to less than 1e-9.
+the beam RMS by the end, or by the turn before its loss).  `amp` is what the nudge has grown to at
+the end (relative to each coordinate's RMS): the reference's own spread for that particle.
 
 Bars, for every mode:
   loss turns equal to the reference's bit for bit at every particle whose fate is certain;
-  final coordinates of the regular particles within 1e-9 of the reference (relative to each
-      coordinate's RMS); bit for bit in the plain and exact modes where no transcendental
-      enters (the FODO), since they keep the reference's operation order.
+  every survivor of certain fate within SPREAD[mode] x max(amp, 1e-12) of the reference: as close
+      as a nudge of 1e-11 (plain, exact: the reference's arithmetic, CUDA's transcendentals) or
+      5e-11 (fused: FMA contraction and the fused maps' operation order) would move the
+      reference's own particle -- a rounding difference of each turn grows with the orbit's
+      sensitivity, so the error of a sensitive orbit is measured in its own spread;
+  regular survivors (the nudge grown at most 100-fold, amp < 1e-10) within 1e-9;
+  bit for bit in the plain and exact modes where no transcendental enters (the FODO), since they
+      keep the reference's operation order.
+Measured on the full config-2 grid: the largest error / amp is 17 (fused) and 3.8 (plain,
+exact) over 2,056 survivors of certain fate, and the regular survivors are within 3.3e-10.
 The DA area (trackDA's triangle fan, aline.cpp:689-708, over each grid column's first lost point)
 is not held to a bar: at 1,000 turns it rests on chaotic points, and the reference's own runs
 1e-12 apart differ by up to 31 grid cells (pert_area in the fixture).
@@ -39,6 +46,7 @@ import make_config_golden as MC  # noqa: E402
 pytestmark = pytest.mark.gpu
 
 MODES = {"fused": 0, "plain": 1, "exact": 2}
+SPREAD = {"fused": 50.0, "plain": 10.0, "exact": 10.0}
 
 
 @pytest.fixture(scope="module")
@@ -52,19 +60,25 @@ def case(CG, prefix):
 
 
 def check_case(c, r, lt, mode, bit_exact=False):
-    """Loss turns off the boundary; regular orbits within 1e-9 (or, bit_exact, every survivor off
-    the boundary bit for bit); and the aperture codes of particles lost in the same turn as in
-    the reference."""
-    ref_lt, bnd, reg = c["loss"], MC.fate_uncertain(c["boundary"], c["amp"]), c["regular"]
+    """Loss turns where the fate is certain; survivors of certain fate within their spread, the
+    regular ones within 1e-9 (or, bit_exact, every survivor of certain fate bit for bit); and the
+    aperture codes of particles lost in the same turn as in the reference."""
+    kind = mode.split()[0]
+    ref_lt, amp = c["loss"], c["amp"]
+    bnd = MC.fate_uncertain(c["boundary"], amp)
     bad = (lt != ref_lt) & ~bnd
     assert not bad.any(), (mode, np.nonzero(bad)[0][:20], lt[bad][:20], ref_lt[bad][:20])
+    surv = (ref_lt < 0) & ~bnd
+    reg = surv & (amp < MC.REGULAR_AMP)
     assert reg.sum() > 0
     if bit_exact:
-        surv = (ref_lt < 0) & ~bnd
         assert same_bits(r[surv], c["out"][surv]), mode
     else:
-        err = rel_err_each(r[reg], c["out"][reg], c["scale"])
-        assert np.max(err) < 1e-9, (mode, float(np.max(err)))
+        err = rel_err_each(r[surv], c["out"][surv], c["scale"])
+        ratio = err / np.maximum(amp[surv], 1e-12)
+        assert np.max(ratio) < SPREAD[kind], (mode, float(np.max(ratio)))
+        err_reg = rel_err_each(r[reg], c["out"][reg], c["scale"])
+        assert np.max(err_reg) < 1e-9, (mode, float(np.max(err_reg)))
     lost_same = (lt >= 0) & (lt == ref_lt) & ~bnd
     assert np.all(np.isnan(r[lt >= 0, 0]))
     assert np.array_equal(r[lost_same, 4], c["out"][lost_same, 4], equal_nan=True)
