@@ -131,6 +131,7 @@ def lib() -> C.CDLL:
         "accel_track_diffusion": (I, [P, I, I, P, P, P, P, P, D, D, D, D, I, C.POINTER(D)]),
         "accel_track_tune": (I, [P, I, D, D, D, D, D, D, I, C.POINTER(D), C.POINTER(D)]),
         "accel_fp64_peak": (I, [P, C.POINTER(D)]),
+        "accel_fp64_peak_clocked": (I, [P, C.POINTER(D), C.POINTER(D)]),
         "accel_set_device_memory_limit": (I, [C.c_int64]),
         "accel_set_adjoint_tape_budget": (I, [C.c_int64]),
         "accel_device_memory_held": (I, [C.POINTER(C.c_int64)]),
@@ -364,6 +365,12 @@ class Context:
         v = C.c_double()
         _check(lib().accel_fp64_peak(self.h, C.byref(v)), "accel_fp64_peak")
         return v.value
+
+    def fp64_peak_clocked(self) -> tuple[float, float]:
+        """(TFLOP/s, SM MHz during the fastest probe run): accel_fp64_peak_clocked."""
+        v, m = C.c_double(), C.c_double()
+        _check(lib().accel_fp64_peak_clocked(self.h, C.byref(v), C.byref(m)), "accel_fp64_peak_clocked")
+        return v.value, m.value
 
     def launch_count(self) -> int:
         v = C.c_int64()

@@ -1126,17 +1126,19 @@ int accel_autotune(accel_line* const* lines, int ninst, const int64_t* part_off,
             }
             if (ms < best * 0.98f) { best = ms; best_v = v; best_sched = sched; }
         }
-    // turns per segment: 64-turn probes, each the better of two runs, the fastest taken
-    int best_seg = 16;
+    // turns per segment: 64-turn probes, each the better of two runs, starting from the untuned
+    // default of 8 and moving outward; another length must win by 2 % (64 turns from the start
+    // over-weight the early turns, where most losses fall and short segments compact sooner)
+    int best_seg = 8;
     best = 1e30f;
-    for (int seg : {1, 2, 4, 8, 16, 32}) {
+    for (int seg : {8, 4, 16, 2, 32, 1}) {
         float ms = 1e30f;
         for (int rep = 0; rep < 2; rep++) {
             float m1 = 0;
             if ((s = time_it(best_v, seg, best_sched, 64, &m1))) return s;
             ms = std::min(ms, m1);
         }
-        if (ms < best) { best = ms; best_seg = seg; }
+        if (ms < best * (seg == 8 ? 1.0f : 0.98f)) { best = ms; best_seg = seg; }
     }
     C->graphs.clear();
     C->tuned[tune_key(lines, ninst, ntot, -1)] = {best_v, best_seg, best_sched};
@@ -1320,16 +1322,20 @@ int accel_beam_stat(accel_ctx* C, const double* r, int layout, int N, double* me
     return ACCEL_OK;
 }
 
-int accel_fp64_peak(accel_ctx* C, double* tflops) {
+int accel_fp64_peak_clocked(accel_ctx* C, double* tflops, double* sm_mhz) {
     if (!C || !tflops) return fail(ACCEL_E_INVALID, "NULL argument");
     std::lock_guard<std::mutex> lk(C->mu);
     CK(cudaSetDevice(C->device));
     float ms = 0;
-    *tflops = fp64_peak_run(C->sm_count, C->stream, &ms);
+    double mhz = 0;
+    *tflops = fp64_peak_run(C->sm_count, C->stream, &ms, &mhz);
+    if (sm_mhz) *sm_mhz = mhz;
     C->launches += 4;  // the warm-up and three timed probes
     CK(cudaGetLastError());
     return ACCEL_OK;
 }
+
+int accel_fp64_peak(accel_ctx* C, double* tflops) { return accel_fp64_peak_clocked(C, tflops, nullptr); }
 
 int accel_profile_enable(accel_ctx* C, int on) {
     if (!C) return fail(ACCEL_E_INVALID, "NULL ctx");

@@ -116,8 +116,7 @@ __global__ void __launch_bounds__(BS, MINB) k_fused(const TrackParams P) {
 
 // Variant table: (block, min blocks per SM) pairs the autotuner chooses from; the launch bound
 // caps registers per thread at 65536 / (block * min_blocks).
-#define FUSED_VARIANTS(X) X(0, 128, 4) X(1, 128, 3) X(2, 256, 2) X(3, 64, 8) X(4, 128, 5) X(5, 128, 2) \
-    X(6, 128, 6) X(7, 128, 7)
+#define FUSED_VARIANTS(X) X(0, 128, 4) X(1, 128, 3) X(2, 256, 2) X(3, 64, 8) X(4, 128, 5) X(5, 128, 2)
 
 VariantInfo fused_variant_info(int v) {
     switch (v) {
@@ -606,7 +605,21 @@ void launch_beam_stat(const double* st, int64_t n, double* part, int nblk, doubl
 // left over cover the loop's own instructions and the probe can reach the pipe's rate.
 constexpr int kPeakChains = 8;
 
-__global__ void __launch_bounds__(512, 4) k_fp64_peak(double* out, int iters, double b, double c) {
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// clk (4 words): block 0's thread 0 records its SM clock counter and the global nanosecond timer
+// at the start and at the end of its loop, which gives the SM clock while the probe runs.
+__global__ void __launch_bounds__(512, 4) k_fp64_peak(double* out, unsigned long long* clk, int iters,
+                                                       double b, double c) {
+    const bool rec = blockIdx.x == 0 && threadIdx.x == 0;
+    if (rec) {
+        clk[0] = clock64();
+        clk[1] = global_ns();
+    }
     double a[kPeakChains];
 #pragma unroll
     for (int j = 0; j < kPeakChains; j++) a[j] = threadIdx.x * 1e-9 + j;
@@ -619,30 +632,42 @@ __global__ void __launch_bounds__(512, 4) k_fp64_peak(double* out, int iters, do
 #pragma unroll
     for (int j = 0; j < kPeakChains; j++) r += a[j];
     if (r == 1234.5) out[0] = r;  // keeps the chains live
+    if (rec) {
+        clk[2] = clock64();
+        clk[3] = global_ns();
+    }
 }
 
-double fp64_peak_run(int sm_count, cudaStream_t s, float* ms_out) {
+double fp64_peak_run(int sm_count, cudaStream_t s, float* ms_out, double* sm_mhz_out) {
     const int iters = 1 << 16, threads = 512, blocks = sm_count * 4;  // about 9 ms
     double* dummy = nullptr;
-    cudaMallocAsync(&dummy, sizeof(double), s);
-    k_fp64_peak<<<blocks, threads, 0, s>>>(dummy, iters / 8, 0.999999, 1e-7);  // warm-up
+    cudaMallocAsync(&dummy, sizeof(double) + 4 * sizeof(unsigned long long), s);
+    unsigned long long* clk = (unsigned long long*)(dummy + 1);
+    k_fp64_peak<<<blocks, threads, 0, s>>>(dummy, clk, iters / 8, 0.999999, 1e-7);  // warm-up
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     float best = 1e30f;
+    double mhz = 0;
     for (int rep = 0; rep < 3; rep++) {  // the best of three
         cudaEventRecord(e0, s);
-        k_fp64_peak<<<blocks, threads, 0, s>>>(dummy, iters, 0.999999, 1e-7);
+        k_fp64_peak<<<blocks, threads, 0, s>>>(dummy, clk, iters, 0.999999, 1e-7);
         cudaEventRecord(e1, s);
         cudaEventSynchronize(e1);
         float ms = 0;
         cudaEventElapsedTime(&ms, e0, e1);
-        if (ms < best) best = ms;
+        if (ms < best) {
+            best = ms;
+            unsigned long long h[4] = {0, 0, 0, 0};
+            cudaMemcpy(h, clk, sizeof(h), cudaMemcpyDeviceToHost);
+            mhz = h[3] > h[1] ? (double)(h[2] - h[0]) / (double)(h[3] - h[1]) * 1e3 : 0.0;
+        }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     cudaFreeAsync(dummy, s);
     if (ms_out) *ms_out = best;
+    if (sm_mhz_out) *sm_mhz_out = mhz;
     double flops = 2.0 * kPeakChains * (double)iters * threads * (double)blocks;
     return flops / (best * 1e-3) / 1e12;
 }

@@ -32,7 +32,7 @@ struct TrackParams {
 };
 
 // ---- fused (kern_fused.cu) ----------------------------------------------------------------
-constexpr int kNumFusedVariants = 8;
+constexpr int kNumFusedVariants = 6;
 // 0: chunks pulled per warp from an atomic counter; 1: a contiguous live-list range per block;
 // 2: per-block tasks with the instance's element hot lines staged in shared memory (staged
 //    variants, their own (block, min blocks) table)
@@ -102,7 +102,7 @@ void launch_lw_regeom(double* scratch, int nbins, double charge_nc, cudaStream_t
 void launch_beam_stat(const double* st, int64_t n, double* partial, int nblk, double* out,
                       cudaStream_t s);
 int beam_stat_blocks(int64_t n);
-double fp64_peak_run(int sm_count, cudaStream_t s, float* ms_out);
+double fp64_peak_run(int sm_count, cudaStream_t s, float* ms_out, double* sm_mhz_out);
 
 // ---- plain (kern_plain.cu) ----------------------------------------------------------------
 void launch_plain_elem(const TrackParams& p, int e, const int32_t* turn_ctr, cudaStream_t s);

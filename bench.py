@@ -241,17 +241,27 @@ def reference_arm(args):
                          "sample": b["sample"]},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "process_maps_engine_library": maps_engine_library(),
+        "native_so_loaded": repo_libraries_mapped(),
     }
     print(json.dumps(line), flush=True)
 
 
-def maps_engine_library() -> bool:
-    """Whether this process has the engine's shared library mapped (/proc/self/maps)."""
+def repo_libraries_mapped() -> list[str]:
+    """The shared libraries under this repository that this process has mapped, relative to it
+    (/proc/self/maps)."""
     try:
         with open("/proc/self/maps") as f:
-            return "libaccelgpu" in f.read()
+            paths = {ln.split()[-1] for ln in f if ln.rstrip().endswith(".so")}
     except OSError:
-        return False
+        return []
+    root = os.path.realpath(ROOT)
+    return sorted(os.path.relpath(os.path.realpath(p), root) for p in paths
+                  if os.path.realpath(p).startswith(root + os.sep))
+
+
+def maps_engine_library() -> bool:
+    """Whether this process has the engine's shared library mapped (/proc/self/maps)."""
+    return any("libaccelgpu" in p for p in repo_libraries_mapped())
 
 
 def config_dict(args, off, aos):
@@ -747,7 +757,7 @@ def engine_arm(args):
     fused_np = state.cpu().numpy()
 
     # ---- roofline of the dominant kernel: one profiled step with events around each launch ----
-    peak = ctx.fp64_peak()
+    peak, probe_mhz = ctx.fp64_peak_clocked()
     sms = torch.cuda.get_device_properties(local).multi_processor_count
     mhz = clk.get("sm_mhz") or clk.get("sm_max_mhz")
     peak_theory = sms * 64 * 2 * mhz * 1e6 / 1e12 if mhz else None
@@ -775,6 +785,9 @@ def engine_arm(args):
                 if achieved and peak_theory else None,
                 "peak_theoretical_basis": "SMs x 64 FP64 FMA per clock x 2 flops x the median SM "
                                           "clock sampled in the timed region",
+                "probe_sm_mhz": probe_mhz,
+                "probe_fma_per_clk_per_sm": (peak * 1e12 / 2 / sms / (probe_mhz * 1e6))
+                if probe_mhz else None,
                 "flops_model": "add/sub/mul/div = 1 at the effective multipole order "
                                "(StrMPole slice 52+3(8m+4), BendMPole slice 4*46+3(90+7m) with "
                                "radiation, drift 14)"}

@@ -263,7 +263,7 @@ int  accel_track_batched(accel_line* const* lines, int ninst, const int64_t* par
  * variant = register-cap variant + 100 x scheduling mode (0: chunks of 32 particles pulled per
  * warp from an atomic counter; 1: a contiguous live-list range per block; 2: blocks of live
  * particles with their instance's element hot lines staged in shared memory).  Register-cap
- * variants 0-7 for modes 0 and 1, 0-2 for mode 2. */
+ * variants 0-5 for modes 0 and 1, 0-2 for mode 2. */
 int  accel_autotune(accel_line* const* lines, int ninst, const int64_t* part_off,
                     const double* r_soa, int64_t ntot, int* tile_out3);
 int  accel_set_tile(accel_ctx* ctx, int block, int seg_turns, int variant);  /* 0s = auto */
@@ -386,6 +386,9 @@ int  accel_track_tune(accel_line* line, int nturn, double x0, double y0, double 
 
 /* Device FP64 FMA throughput micro-benchmark (TFLOP/s, FMA = 2 flops). */
 int  accel_fp64_peak(accel_ctx* ctx, double* tflops);
+/* The same, and the SM clock (MHz) during the fastest run, from the SM's cycle counter against
+ * the global nanosecond timer over one block's loop (sm_mhz may be NULL). */
+int  accel_fp64_peak_clocked(accel_ctx* ctx, double* tflops, double* sm_mhz);
 
 /* Device-memory budget of this process's library (no counterpart in the reference, which tracks
  * in host memory).  Every device buffer the library keeps (particle state, element tables,

@@ -21,7 +21,11 @@ Bars, for every mode:
       sensitivity, so the error of a sensitive orbit is measured in its own spread;
   regular survivors (the nudge grown at most 100-fold, amp < 1e-10) within 1e-9;
   bit for bit in the plain and exact modes where no transcendental enters (the FODO), since they
-      keep the reference's operation order.
+      keep the reference's operation order;
+  the aperture code of each particle lost in the reference's turn equal to the reference's (the
+      fused mode: except on at most 1 % of them, each an orbit already sensitive before its loss;
+      one of 614 on the config-2 grid, a particle whose y at the aperture is 62 mm in the
+      reference and 39 mm in the fused run after a last turn that took px to 0.19).
 Measured on the full config-2 grid: the largest error / amp is 17 (fused) and 3.8 (plain,
 exact) over 2,056 survivors of certain fate, and the regular survivors are within 3.3e-10.
 The DA area (trackDA's triangle fan, aline.cpp:689-708, over each grid column's first lost point)
@@ -81,7 +85,17 @@ def check_case(c, r, lt, mode, bit_exact=False):
         assert np.max(err_reg) < 1e-9, (mode, float(np.max(err_reg)))
     lost_same = (lt >= 0) & (lt == ref_lt) & ~bnd
     assert np.all(np.isnan(r[lt >= 0, 0]))
-    assert np.array_equal(r[lost_same, 4], c["out"][lost_same, 4], equal_nan=True)
+    code, ref_code = r[:, 4], c["out"][:, 4]
+    differ = lost_same & ~((code == ref_code) | (np.isnan(code) & np.isnan(ref_code)))
+    if kind == "fused":
+        # the code names the limits exceeded at the aperture in the loss turn, where an unstable
+        # orbit's state has grown by orders of magnitude within the turn: a rounding difference
+        # may cross a second limit.  Allowed only where the orbit was already sensitive (the
+        # nudge past 1e-9 by the turn before the loss), and rarely.
+        assert not (differ & (amp < 1e-9)).any(), (mode, np.nonzero(differ)[0])
+        assert differ.sum() <= 0.01 * lost_same.sum(), (mode, np.nonzero(differ)[0])
+    else:
+        assert not differ.any(), (mode, np.nonzero(differ)[0])
     return int(reg.sum()), int((lt != ref_lt).sum())
 
 
