@@ -778,9 +778,9 @@ def engine_arm(args):
                 "kernel": "k_fused (persistent FP64 tracker)",
                 "launches": fused_n, "kernel_ms_per_step": fused_ms, "step_ms_profiled": call_ms,
                 "model_flops_per_step": flops,
-                "peak_source": "measured in this run: FP64 FMA-chain probe (accel_fp64_peak, best of "
-                               "three 9 ms runs at full occupancy); MEASURED_PEAKS.json carries "
-                               "no FP64 figure",
+                "peak_source": "measured in this run: FP64 FMA-chain probe (accel_fp64_peak_clocked, "
+                               "best of three 9 ms runs at full occupancy, with the SM clock it "
+                               "ran at); MEASURED_PEAKS.json carries no FP64 figure",
                 "peak_theoretical": peak_theory, "frac_theoretical": (achieved / peak_theory)
                 if achieved and peak_theory else None,
                 "peak_theoretical_basis": "SMs x 64 FP64 FMA per clock x 2 flops x the median SM "
