@@ -9,7 +9,9 @@
 //   whole run   every turn's Jacobians fit: the forward runs in launches of 32 turns and each
 //               chunk is taped on a second stream as soon as the forward has written its turn
 //               starts, so the taping (wide, FP64-bound) runs behind the forward (one particle
-//               per thread, latency-bound); the backward is a single sweep over the run;
+//               per thread, latency-bound); the forward's blocks mark their SMs and the tape
+//               kernel's blocks leave those SMs, so the two share the GPU by SMs rather than
+//               by issue slots; the backward is a single sweep over the run;
 //   chunks      accel_adjoint_backward walks the segments last to first: the segment's turn
 //               starts (kept by the forward when they fit, else recomputed from its checkpoint),
 //               then, chunk by chunk, last to first, the tape and its sweep;
@@ -52,6 +54,12 @@ constexpr int kMaxAdjParams = 2048;
 constexpr double kTapeBudgetFloor = 4.0e9;
 std::atomic<double> g_tape_budget{-1.0};  // <= 0: the default
 constexpr int kForwardChunk = 32;  // turns per forward launch when the tapes follow it chunk by chunk
+// Forward block size in that mode: 4,096 particles take 32 SMs (one warp per scheduler, the
+// forward's latency-bound chain at full speed) and the tape kernel leaves those SMs to it.
+// Measured per gradient (4,096 particles, 512 turns, 36 knobs): 239 ms with 64-thread blocks
+// and tape blocks anywhere; 192-204 ms like this; 16- and 64-turn chunks, 256-thread blocks, or
+// one or two tape blocks left on each forward SM were slower (189-394 ms forward).
+constexpr int kForwardThreads = 128;
 
 double tape_budget() {
     const double b = g_tape_budget.load();
@@ -94,6 +102,9 @@ struct accel_adjoint {
     cudaEvent_t fwd_done = nullptr;
     std::vector<cudaEvent_t> chunk_ev;  // the forward has written chunk c's turn starts
     cudaEvent_t tape_done = nullptr;    // every tape of the last forward is written
+    // whole-run mode: kAdjSmSlots counters of the forward blocks on each SM, then one work
+    // counter per chunk's tape (zeroed at the start of each forward)
+    DevBuf sched;
     DevBuf st, lam, aos, tape, ckpt, turn_tape, part, meta, final_x, grad, jt, rt, pel, grow, uzd;
     bool have_forward = false;
     ~accel_adjoint() {
@@ -105,7 +116,7 @@ struct accel_adjoint {
         if (tape_stream) cudaStreamDestroy(tape_stream);
         if (fwd_stream) cudaStreamDestroy(fwd_stream);
         for (DevBuf* b : {&st, &lam, &aos, &tape, &ckpt, &turn_tape, &part, &meta, &final_x, &grad, &jt, &rt, &pel,
-                          &grow, &uzd})
+                          &grow, &uzd, &sched})
             b->release();
     }
 };
@@ -254,6 +265,7 @@ int accel_adjoint_create(accel_line* L, int N, int nturn, int every, const int32
             J->chunk_ev.assign((size_t)((nturn + kForwardChunk - 1) / kForwardChunk), nullptr);
             for (cudaEvent_t& e : J->chunk_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
             CK(cudaEventCreateWithFlags(&J->tape_done, cudaEventDisableTiming));
+            if ((s = J->sched.ensure(sizeof(int) * (kAdjSmSlots + J->chunk_ev.size())))) return s;
         }
     } else {
         J->chunk = 0;
@@ -314,16 +326,21 @@ int accel_adjoint_forward(accel_adjoint* J, const double* r0, double* r_final) {
         double* jt = (double*)J->jt.p;
         double* rt = (double*)J->rt.p;
         int c = 0;
+        int* sm_fwd = (int*)J->sched.p;
+        int* work = sm_fwd + kAdjSmSlots;
+        CK(cudaMemsetAsync(J->sched.p, 0, sizeof(int) * (kAdjSmSlots + J->chunk_ev.size()), s));
         CK(cudaEventRecord(J->fwd_ready, s));
         CK(cudaStreamWaitEvent(J->fwd_stream, J->fwd_ready, 0));
+        CK(cudaStreamWaitEvent(J->tape_stream, J->fwd_ready, 0));
         for (int t0 = 0; t0 < J->nturn; t0 += kForwardChunk, c++) {
             const int nt = std::min(kForwardChunk, J->nturn - t0);
-            launch_adj_forward(a, (double*)J->ckpt.p, t0, nt, J->every, (double*)J->turn_tape.p, J->fwd_stream);
+            launch_adj_forward(a, (double*)J->ckpt.p, t0, nt, J->every, (double*)J->turn_tape.p, J->fwd_stream,
+                               kForwardThreads, sm_fwd);
             CK(cudaEventRecord(J->chunk_ev[(size_t)c], J->fwd_stream));
             CK(cudaStreamWaitEvent(J->tape_stream, J->chunk_ev[(size_t)c], 0));
             launch_adj_jtape(a, (const double*)J->turn_tape.p, t0, nt, nullptr, J->npe,
                              jt + (size_t)t0 * (J->npe + 1) * 36 * span, rt + (size_t)t0 * J->nparam * 6 * span,
-                             J->general, J->tape_stream);
+                             J->general, J->tape_stream, work + c, sm_fwd, C->sm_count);
         }
         CK(cudaEventRecord(J->fwd_done, J->fwd_stream));
         CK(cudaEventRecord(J->tape_done, J->tape_stream));

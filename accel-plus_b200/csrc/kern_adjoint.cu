@@ -94,6 +94,7 @@ namespace {
 constexpr unsigned FULL = 0xffffffffu;
 constexpr int kAdjThreads = 64;
 constexpr int kTile = 32;  // particles per tile of the tape layouts (one warp of the sweep)
+constexpr unsigned kSmSlots = kAdjSmSlots;
 }  // namespace
 
 int adj_blocks(int64_t n) { return (int)((n + kAdjThreads - 1) / kAdjThreads); }
@@ -112,18 +113,35 @@ __device__ __forceinline__ void store6(double* s, int64_t n, int64_t p, const do
 // so the reverse pass needs no recomputation; the states are the ones recomputing would give.
 // Turns [t0, t0 + nturn) of the run: a long run may be issued as several launches in a row (st
 // carries the state from one to the next), checkpoints and turn starts indexed by the run's turn.
-__global__ void __launch_bounds__(kAdjThreads) k_adj_fwd(const AdjParams a, double* ckpt, int t0, int nturn,
-                                                         int every, double* turn_tape) {
+// sm_fwd (may be null): per SM, the number of forward blocks running on it; each block counts
+// itself in on entry and out when all its threads are done, so that the tape kernel running
+// beside the forward can leave those SMs to it (k_adj_jtape's work loop).
+__device__ __forceinline__ unsigned sm_id() {
+    unsigned id;
+    asm volatile("mov.u32 %0, %%smid;" : "=r"(id));
+    return id;
+}
+
+template <int BS>
+__global__ void __launch_bounds__(BS) k_adj_fwd(const AdjParams a, double* ckpt, int t0, int nturn, int every,
+                                                double* turn_tape, int* sm_fwd) {
+    const unsigned sm = sm_id();
+    if (sm_fwd && threadIdx.x == 0 && sm < kSmSlots) atomicAdd(sm_fwd + sm, 1);
     const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= a.n) return;
-    double r[6];
-    load6(a.st, a.n, p, r);
-    for (int t = t0; t < t0 + nturn; t++) {
-        if (t % every == 0) store6(ckpt + (int64_t)(t / every) * 6 * a.n, a.n, p, r);
-        if (turn_tape) store6(turn_tape + (int64_t)t * 6 * a.n, a.n, p, r);
-        if (!(r[0] != r[0])) fast_turn(a, r);
+    if (p < a.n) {
+        double r[6];
+        load6(a.st, a.n, p, r);
+        for (int t = t0; t < t0 + nturn; t++) {
+            if (t % every == 0) store6(ckpt + (int64_t)(t / every) * 6 * a.n, a.n, p, r);
+            if (turn_tape) store6(turn_tape + (int64_t)t * 6 * a.n, a.n, p, r);
+            if (!(r[0] != r[0])) fast_turn(a, r);
+        }
+        store6(a.st, a.n, p, r);
     }
-    store6(a.st, a.n, p, r);
+    if (sm_fwd) {
+        __syncthreads();
+        if (threadIdx.x == 0 && sm < kSmSlots) atomicSub(sm_fwd + sm, 1);
+    }
 }
 
 // Recompute checkpoint segments seg0 .. seg0+nseg-1 at once, (segment, particle) per thread,
@@ -340,12 +358,9 @@ __device__ __forceinline__ void jtape_unit(const AdjParams& a, double* s, int e0
 }
 
 template <bool GENERAL>
-__global__ void __launch_bounds__(128, GENERAL ? 1 : 3) k_adj_jtape(const AdjParams a, const double* turn_tape, int j0,
-                                                                    int nt, const double* final_x, int npe, double* jt,
-                                                                    double* sens) {
+__device__ __forceinline__ void jtape_one(const AdjParams& a, const double* turn_tape, int j0, int64_t gid,
+                                          const double* final_x, int npe, double* jt, double* sens) {
     const int64_t n = a.n;
-    const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (gid >= n * nt) return;
     const int t = (int)(gid / n);
     const int64_t p = gid - (int64_t)t * n;
     // a particle lost by the end is skipped when that is known (final_x given); a tape written
@@ -371,6 +386,42 @@ __global__ void __launch_bounds__(128, GENERAL ? 1 : 3) k_adj_jtape(const AdjPar
             else jtape_unit<false, false>(a, s, e0, e1, pe, J, S, pstride);
         }
         e0 = e1 + 1;
+    }
+}
+
+// Two ways to cover the n x nt (turn, particle) units, one per thread:
+//   work == null: one unit per thread of the grid;
+//   work != null: a grid sized to the resident blocks takes groups of 128 units from the counter
+//     *work (zeroed before the launch) until none is left.  While the forward runs beside it,
+//     a block whose SM holds a forward block (sm_fwd, see k_adj_fwd) takes no more work and
+//     leaves, so the latency-bound forward keeps its SMs to itself; block 0 never leaves, so
+//     every unit is taped whatever the placement.  Each pass of the loop takes one group or
+//     leaves, and the counter only grows, so the loop ends.
+template <bool GENERAL>
+__global__ void __launch_bounds__(128, GENERAL ? 1 : 3) k_adj_jtape(const AdjParams a, const double* turn_tape, int j0,
+                                                                    int nt, const double* final_x, int npe, double* jt,
+                                                                    double* sens, int* work, const int* sm_fwd) {
+    const int64_t units = a.n * (int64_t)nt;
+    if (!work) {
+        const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+        if (gid < units) jtape_one<GENERAL>(a, turn_tape, j0, gid, final_x, npe, jt, sens);
+        return;
+    }
+    const int64_t groups = (units + 127) / 128;
+    const unsigned sm = sm_id();
+    __shared__ int64_t s_group;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const bool yield = sm_fwd && blockIdx.x != 0 && sm < kSmSlots &&
+                               *(volatile const int*)(sm_fwd + sm) > 0;
+            s_group = yield ? -1 : (int64_t)atomicAdd(work, 1);
+        }
+        __syncthreads();
+        const int64_t g = s_group;
+        __syncthreads();
+        if (g < 0 || g >= groups) return;
+        const int64_t gid = g * 128 + threadIdx.x;
+        if (gid < units) jtape_one<GENERAL>(a, turn_tape, j0, gid, final_x, npe, jt, sens);
     }
 }
 
@@ -487,8 +538,15 @@ __global__ void k_adj_reduce(const double* part, int nblk, int nparam, double* o
 }
 
 void launch_adj_forward(const AdjParams& a, double* ckpt, int t0, int nturn, int every, double* turn_tape,
-                        cudaStream_t s) {
-    k_adj_fwd<<<adj_blocks(a.n), kAdjThreads, 0, s>>>(a, ckpt, t0, nturn, every, turn_tape);
+                        cudaStream_t s, int threads, int* sm_fwd) {
+    const unsigned nb = (unsigned)((a.n + threads - 1) / threads);
+    switch (threads) {
+    case 128: k_adj_fwd<128><<<nb, 128, 0, s>>>(a, ckpt, t0, nturn, every, turn_tape, sm_fwd); break;
+    case 256: k_adj_fwd<256><<<nb, 256, 0, s>>>(a, ckpt, t0, nturn, every, turn_tape, sm_fwd); break;
+    default:
+        k_adj_fwd<kAdjThreads><<<adj_blocks(a.n), kAdjThreads, 0, s>>>(a, ckpt, t0, nturn, every, turn_tape, sm_fwd);
+        break;
+    }
 }
 void launch_adj_recompute(const AdjParams& a, const double* ckpt, double* turn_tape, int nturn, int every,
                           int seg0, int nseg, cudaStream_t s) {
@@ -541,12 +599,20 @@ bool jtape_needs_general(const DevElem* t, int ne, const int32_t* pcount, const 
 }
 
 void launch_adj_jtape(const AdjParams& a, const double* turn_tape, int j0, int nt, const double* final_x,
-                      int npe, double* jt, double* sens, bool general, cudaStream_t s) {
+                      int npe, double* jt, double* sens, bool general, cudaStream_t s, int* work,
+                      const int* sm_fwd, int sm_count) {
     const int64_t threads = a.n * (int64_t)nt;
+    unsigned grid = (unsigned)((threads + 127) / 128);
+    if (work) {
+        int per_sm = 0;
+        if (general) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_adj_jtape<true>, 128, 0);
+        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_adj_jtape<false>, 128, 0);
+        grid = std::min<unsigned>(grid, (unsigned)std::max(1, per_sm * sm_count));
+    }
     if (general)
-        k_adj_jtape<true><<<(unsigned)((threads + 127) / 128), 128, 0, s>>>(a, turn_tape, j0, nt, final_x, npe, jt, sens);
+        k_adj_jtape<true><<<grid, 128, 0, s>>>(a, turn_tape, j0, nt, final_x, npe, jt, sens, work, sm_fwd);
     else
-        k_adj_jtape<false><<<(unsigned)((threads + 127) / 128), 128, 0, s>>>(a, turn_tape, j0, nt, final_x, npe, jt, sens);
+        k_adj_jtape<false><<<grid, 128, 0, s>>>(a, turn_tape, j0, nt, final_x, npe, jt, sens, work, sm_fwd);
 }
 void launch_adj_jsweep(const AdjParams& a, int nt, const double* final_x, int npe, const int32_t* pelem,
                        const double* jt, const double* sens, double* grow, cudaStream_t s) {

@@ -138,8 +138,11 @@ struct AdjParams {
 int adj_blocks(int64_t n);
 // turn_tape: null, or room for every turn's starting state (nturn x 6 x n doubles)
 // turns [t0, t0 + nturn) of the run; st carries the state between consecutive launches
+// threads: block size (64, 128 or 256); sm_fwd: null, or kAdjSmSlots counters of the forward
+// blocks running on each SM (for a tape kernel running beside the forward)
+constexpr int kAdjSmSlots = 256;
 void launch_adj_forward(const AdjParams& a, double* ckpt, int t0, int nturn, int every, double* turn_tape,
-                        cudaStream_t s);
+                        cudaStream_t s, int threads = 64, int* sm_fwd = nullptr);
 // turn-start states of checkpoint segments seg0 .. seg0+nseg-1 into turn_tape, from turn seg0 * every on
 void launch_adj_recompute(const AdjParams& a, const double* ckpt, double* turn_tape, int nturn, int every,
                           int seg0, int nseg, cudaStream_t s);
@@ -149,8 +152,11 @@ void launch_adj_reduce(const double* part, int nblk, int nparam, double* out, cu
 // sweep over it (kern_adjoint.cu)
 // general: the line has elements or parameters outside the explicit-Jacobian maps
 // (jtape_needs_general)
+// work: null (one unit per thread), or a zeroed counter: a grid of the resident blocks takes
+// groups of units from it, leaving the SMs sm_fwd marks (sm_count: the device's SMs)
 void launch_adj_jtape(const AdjParams& a, const double* turn_tape, int j0, int nt, const double* final_x,
-                      int npe, double* jt, double* sens, bool general, cudaStream_t s);
+                      int npe, double* jt, double* sens, bool general, cudaStream_t s, int* work = nullptr,
+                      const int* sm_fwd = nullptr, int sm_count = 0);
 bool jtape_needs_general(const DevElem* host_tbl, int ne, const int32_t* pcount, const int32_t* pfirst,
                          const int32_t* pkind);
 // per tape unit (npe + 1 of them): 1 if any of its elements is not a drift, straight multipole,
