@@ -8,6 +8,9 @@
 //  * 1/(1+delta) is formed once per element where delta cannot change inside it (no radiation),
 //    and the element's per-slice constants are folded with it;
 //  * the adjacent full-length drifts that end one Yoshida slice and begin the next are merged;
+//  * in radiating bends the hx-drift constants are formed once per element and 1/(1+delta)
+//    enters through the angles, and the radiated power of a pure dipole field uses
+//    |B x v|^2 = By^2 ((1+hx)^2 + x'^2);
 //  * a*b+c contracts to FMA.
 // None of these changes the map beyond rounding; the parity tests bound the difference.
 #pragma once
@@ -141,6 +144,29 @@ __device__ __forceinline__ void hxdrift(St& s, double h, const HxCoef& k) {
     s.z = fma(-hx1 * k.dd, q, s.z);
 }
 
+// The same hx drift while delta changes between drifts (radiation): the element constants
+// L, hL/2, L/2 and hL^2/4 are formed once, and 1/(1+delta) enters through the angles
+// P = px/(1+d), Q = py/(1+d): x += (1+hx) L P + (hL^2/4)(P^2 - Q^2), px -= (hL/2)(P px + Q py),
+// y += (1+hx) L Q (1 + (hL/2) px), z -= (1+hx)(L/2)(P^2 + Q^2).
+struct HxConst { double L, c, dd, b; };  // L, hL/2, L/2, hL^2/4
+
+__device__ __forceinline__ HxConst hx_const(double L, double h) {
+    return HxConst{L, 0.5 * h * L, 0.5 * L, 0.25 * h * L * L};
+}
+
+__device__ __forceinline__ void hxdrift_inv(St& s, double h, const HxConst& k, double inv) {
+    const double px = s.px, py = s.py;
+    const double P = px * inv, Q = py * inv;
+    const double QQ = Q * Q;
+    const double s2 = fma(P, P, QQ), d2 = fma(P, P, -QQ);
+    const double hx1 = fma(h, s.x, 1.0);
+    const double hL = hx1 * k.L;
+    s.x = fma(hL, P, fma(k.b, d2, s.x));
+    s.px = fma(-k.c, fma(P, px, Q * py), px);
+    s.y = fma(hL * Q, fma(px, k.c, 1.0), s.y);
+    s.z = fma(-hx1 * k.dd, s2, s.z);
+}
+
 // Horner over B only (bendMPole kicks carry no skew terms), order M
 template <int M>
 __device__ __forceinline__ void horner_b(const St& s, const double* B, double& re, double& im) {
@@ -194,9 +220,10 @@ __device__ __forceinline__ void bend_kick_core(St& s, const BkCoef& c, double re
 // The energy loss per kick D is tiny (|D/(1+delta)| ~ 1e-7), so the new inverse is the old one
 // times 1/(1-u), u = D/(1+delta), summed to u^3 (truncation below 1e-20 relative); a loss
 // above |u| = 1e-4 takes the exact reciprocal.
+// cradL = crad x L, the element's radiation constant times the kick's length.
 template <int M, int RAD, bool PURE>
 __device__ __forceinline__ double bend_kick_rad(St& s, const double* B, const BkCoef& c, double L,
-                                                double crad, double qec, double inv, double gauss) {
+                                                double cradL, double qec, double inv, double gauss) {
     double re, im;
     horner_b<M>(s, B, re, im);
     double x = s.x, y = s.y, y2 = y * y;
@@ -206,16 +233,23 @@ __device__ __forceinline__ double bend_kick_rad(St& s, const double* B, const Bk
         re = fma(y2, fma(c.cR2, x, c.cR1), re);
     }
     double hx1 = fma(x, c.h, 1.0);
-    double vq = fma(xpr, xpr, ypr * ypr);
-    double vn2 = rcp(fma(hx1, hx1, vq));
     double by = re + c.h, bx = im;
-    // with no imaginary field (M = 0, PURE) bx is exactly 0 and its terms are +0: left out
+    // with no imaginary field (M = 0, PURE) bx is exactly 0 and its terms are +0: left out, and
+    // |B x v|^2 = by^2 ((1+hx)^2 + x'^2) since the cross term by x' has no partner
     constexpr bool NOIM = (M == 0) && PURE;
-    double cr = NOIM ? -by * xpr : fma(bx, ypr, -by * xpr);
-    double b2p = (NOIM ? fma(by * hx1, by * hx1, cr * cr)
-                       : fma(by * hx1, by * hx1, fma(bx * hx1, bx * hx1, cr * cr))) * vn2;
+    double xx = xpr * xpr, yy = ypr * ypr;
+    double vq = xx + yy;
+    double b2p;
+    if constexpr (NOIM) {
+        double t = fma(hx1, hx1, xx);
+        b2p = (by * by) * t * rcp(t + yy);
+    } else {
+        double vn2 = rcp(fma(hx1, hx1, vq));
+        double cr = fma(bx, ypr, -by * xpr);
+        b2p = fma(by * hx1, by * hx1, fma(bx * hx1, bx * hx1, cr * cr)) * vn2;
+    }
     double opd = 1.0 + s.d;
-    double mean = crad * (opd * opd) * b2p * fma(0.5, vq, hx1) * L;
+    double mean = cradL * (opd * opd) * b2p * fma(0.5, vq, hx1);
     double loss;
     if (RAD == 1) {
         loss = mean;
@@ -270,25 +304,28 @@ __device__ __forceinline__ void bendmpole(St& s, const DevElem* __restrict__ e,
         }
     } else if (rad == 1) {
         const double crad = e->h[H_CRAD];
+        const double cK1 = crad * K1, cK2 = crad * K2;
+        const HxConst k1 = hx_const(L1, c.h), k2 = hx_const(L2, c.h);
         double inv = rcp(1.0 + s.d);
         for (int m = 0; m < ns; m++) {
-            hxdrift(s, c.h, hx_coef(L1, c.h, inv));
-            inv = bend_kick_rad<M, 1, PURE>(s, B, c, K1, crad, 0.0, inv, 0.0);
-            hxdrift(s, c.h, hx_coef(L2, c.h, inv));
-            inv = bend_kick_rad<M, 1, PURE>(s, B, c, K2, crad, 0.0, inv, 0.0);
-            hxdrift(s, c.h, hx_coef(L2, c.h, inv));
-            inv = bend_kick_rad<M, 1, PURE>(s, B, c, K1, crad, 0.0, inv, 0.0);
-            hxdrift(s, c.h, hx_coef(L1, c.h, inv));
+            hxdrift_inv(s, c.h, k1, inv);
+            inv = bend_kick_rad<M, 1, PURE>(s, B, c, K1, cK1, 0.0, inv, 0.0);
+            hxdrift_inv(s, c.h, k2, inv);
+            inv = bend_kick_rad<M, 1, PURE>(s, B, c, K2, cK2, 0.0, inv, 0.0);
+            hxdrift_inv(s, c.h, k2, inv);
+            inv = bend_kick_rad<M, 1, PURE>(s, B, c, K1, cK1, 0.0, inv, 0.0);
+            hxdrift_inv(s, c.h, k1, inv);
         }
     } else {
         const double crad = e->h[H_CRAD], qec = e->v[V_QECOEF], SL = e->v[V_SL];
-        const double hs = 0.5 * SL;
+        const HxConst kh = hx_const(0.5 * SL, c.h);
+        const double cSL = crad * SL;
         double inv = rcp(1.0 + s.d);
         for (int m = 0; m < ns; m++) {
-            hxdrift(s, c.h, hx_coef(hs, c.h, inv));
+            hxdrift_inv(s, c.h, kh, inv);
             double g = qe_normal(seed, pid, turn, (uint32_t)e->elem, (uint32_t)m);
-            inv = bend_kick_rad<M, 2, PURE>(s, B, c, SL, crad, qec, inv, g);
-            hxdrift(s, c.h, hx_coef(hs, c.h, inv));
+            inv = bend_kick_rad<M, 2, PURE>(s, B, c, SL, cSL, qec, inv, g);
+            hxdrift_inv(s, c.h, kh, inv);
         }
     }
     s.px = fma(s.x, psi2, s.px);

@@ -26,7 +26,7 @@ Bars, for every mode:
       fused mode: except on at most 1 % of them, each an orbit already sensitive before its loss;
       one of 614 on the config-2 grid, a particle whose y at the aperture is 62 mm in the
       reference and 39 mm in the fused run after a last turn that took px to 0.19).
-Measured on the full config-2 grid: the largest error / amp is 17 (fused) and 3.8 (plain,
+Measured on the full config-2 grid: the largest error / amp is 19 (fused) and 3.8 (plain,
 exact) over 2,056 survivors of certain fate, and the regular survivors are within 3.3e-10.
 The DA area (trackDA's triangle fan, aline.cpp:689-708, over each grid column's first lost point)
 is not held to a bar: at 1,000 turns it rests on chaotic points, and the reference's own runs
