@@ -91,6 +91,12 @@ struct accel_adjoint {
     int npe = 0;
     int chunk = 0;               // turns per block-Jacobian tape; 0: per-turn element reversal
     bool general = true;         // the tape needs the dual-number fallback (jtape_needs_general)
+    // no element of the line reads z or changes delta (and the tape is the explicit one): a
+    // reverse sweep seeded with zero z components never uses the unit Jacobians' z rows, so
+    // the tapes are written without them, and a seed with a z component has them re-taped
+    bool zrow_free = false;
+    bool tapes_zrow = true;      // the whole-run tapes of the last forward carry the z rows
+    DevBuf flag;
     bool all_turns = false;      // turn_tape holds every turn of the run, written by the forward
     // the Jacobian tape of every turn of the run fits the budget: the forward runs in chunks of
     // kForwardChunk turns and each chunk's tape is written on the second stream as soon as its
@@ -116,7 +122,7 @@ struct accel_adjoint {
         if (tape_stream) cudaStreamDestroy(tape_stream);
         if (fwd_stream) cudaStreamDestroy(fwd_stream);
         for (DevBuf* b : {&st, &lam, &aos, &tape, &ckpt, &turn_tape, &part, &meta, &final_x, &grad, &jt, &rt, &pel,
-                          &grow, &uzd, &sched})
+                          &grow, &uzd, &sched, &flag})
             b->release();
     }
 };
@@ -253,6 +259,8 @@ int accel_adjoint_create(accel_line* L, int N, int nturn, int every, const int32
         std::vector<int32_t> uz((size_t)J->npe + 1);
         jtape_unit_zd(L->host_tbl.data(), ne, J->pelem.data(), J->npe, uz.data());
         CK(cudaMemcpy(J->uzd.p, uz.data(), sizeof(int32_t) * uz.size(), cudaMemcpyHostToDevice));
+        J->zrow_free = !J->general && std::all_of(uz.begin(), uz.end(), [](int32_t z) { return z == 0; });
+        if ((s = J->flag.ensure(sizeof(int)))) return s;
         if (J->whole) {
             // the forward on the highest-priority stream: a chunk's blocks are placed ahead of
             // the tape blocks waiting for room, so the latency-bound forward is not held back
@@ -340,8 +348,9 @@ int accel_adjoint_forward(accel_adjoint* J, const double* r0, double* r_final) {
             CK(cudaStreamWaitEvent(J->tape_stream, J->chunk_ev[(size_t)c], 0));
             launch_adj_jtape(a, (const double*)J->turn_tape.p, t0, nt, nullptr, J->npe,
                              jt + (size_t)t0 * (J->npe + 1) * 36 * span, rt + (size_t)t0 * J->nparam * 6 * span,
-                             J->general, J->tape_stream, work + c, sm_fwd, C->sm_count);
+                             J->general, J->tape_stream, work + c, sm_fwd, C->sm_count, !J->zrow_free);
         }
+        J->tapes_zrow = !J->zrow_free;
         CK(cudaEventRecord(J->fwd_done, J->fwd_stream));
         CK(cudaEventRecord(J->tape_done, J->tape_stream));
         CK(cudaStreamWaitEvent(s, J->fwd_done, 0));
@@ -381,6 +390,29 @@ int accel_adjoint_backward(accel_adjoint* J, const double* g, double* dr0, doubl
     if (J->nparam > 0) CK(cudaMemsetAsync(J->part.p, 0, sizeof(double) * (size_t)nblk * J->nparam, s));
     AdjParams a = params_of(J);
     int64_t launches = 1;
+    // z rows are needed when the seed has a z component (or the line reads z)
+    bool zrow = !J->zrow_free;
+    if (!zrow && J->chunk > 0) {
+        int any = 0;
+        launch_any_nonzero((const double*)J->lam.p + 4 * (size_t)J->n, J->n, (int*)J->flag.p, s);
+        CK(cudaMemcpyAsync(&any, J->flag.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        zrow = any != 0;
+        launches++;
+    }
+    // the forward wrote every turn's tape, without z rows: a seed with a z component has them
+    // written again, with z rows, from the kept turn starts
+    if (J->whole && zrow && !J->tapes_zrow) {
+        const size_t span = (size_t)adj_tile_span(J->n);
+        for (int t0 = 0; t0 < J->nturn; t0 += kForwardChunk) {
+            const int nt = std::min(kForwardChunk, J->nturn - t0);
+            launch_adj_jtape(a, (const double*)J->turn_tape.p, t0, nt, (const double*)J->final_x.p, J->npe,
+                             (double*)J->jt.p + (size_t)t0 * (J->npe + 1) * 36 * span,
+                             (double*)J->rt.p + (size_t)t0 * J->nparam * 6 * span, J->general, s);
+            launches++;
+        }
+        J->tapes_zrow = true;
+    }
     // the forward wrote every turn's tape: one sweep over the whole run, last turn to first
     if (J->whole) {
         launch_adj_jsweep(a, J->nturn, (const double*)J->final_x.p, J->npe, (const int32_t*)J->pel.p,
@@ -402,7 +434,7 @@ int accel_adjoint_backward(accel_adjoint* J, const double* g, double* dr0, doubl
             for (int hi = nt; hi > 0; hi -= J->chunk) {
                 const int lo = std::max(0, hi - J->chunk);
                 launch_adj_jtape(a, tt, lo, hi - lo, (const double*)J->final_x.p, J->npe, (double*)J->jt.p,
-                                 (double*)J->rt.p, J->general, s);
+                                 (double*)J->rt.p, J->general, s, nullptr, nullptr, 0, zrow);
                 launch_adj_jsweep(a, hi - lo, (const double*)J->final_x.p, J->npe, (const int32_t*)J->pel.p,
                                   (const double*)J->jt.p, (const double*)J->rt.p, (double*)J->grow.p, s);
                 launches += 2;

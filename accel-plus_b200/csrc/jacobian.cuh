@@ -26,6 +26,9 @@
 // there the z column stays the unit vector e_z and the delta row stays e_delta, so the row
 // updates skip column z and a term "a * row(delta)" only adds a to column delta.  Adding a * 0
 // changes nothing, so this is the same arithmetic with the zero terms left out.
+// ZR = false (only with ZD = false) also leaves the z row at e_z.  In a line where no element
+// reads z, the adjoint of z is the seed's z component at every unit, so with a seed whose z
+// component is zero the z row is multiplied by zero in the reverse sweep and need not be formed.
 #pragma once
 #include "engine.h"
 #include "adjoint_params.h"
@@ -35,8 +38,9 @@ namespace jac {
 
 enum { X = 0, PX = 1, Y = 2, PY = 3, Z = 4, D = 5 };
 
-template <int NC, bool ZD = true>
+template <int NC, bool ZD = true, bool ZR = true>
 struct JS {
+    static_assert(ZR || !ZD, "the z row may be left out only where nothing reads z");
     double s[6];
     double m[6 * NC];
 };
@@ -44,8 +48,8 @@ struct JS {
 // columns the row updates touch
 __host__ __device__ constexpr bool live_col(bool zd, int k) { return zd || k != Z; }
 
-template <int NC, bool ZD>
-__device__ __forceinline__ void set_identity(JS<NC, ZD>& j) {
+template <int NC, bool ZD, bool ZR>
+__device__ __forceinline__ void set_identity(JS<NC, ZD, ZR>& j) {
 #pragma unroll
     for (int i = 0; i < 6 * NC; i++) j.m[i] = 0.0;
 #pragma unroll
@@ -53,23 +57,23 @@ __device__ __forceinline__ void set_identity(JS<NC, ZD>& j) {
 }
 
 // row[dst] += a * row[src]
-template <int NC, bool ZD>
-__device__ __forceinline__ void axpy(JS<NC, ZD>& j, int dst, int src, double a) {
+template <int NC, bool ZD, bool ZR>
+__device__ __forceinline__ void axpy(JS<NC, ZD, ZR>& j, int dst, int src, double a) {
 #pragma unroll
     for (int k = 0; k < NC; k++)
         if (live_col(ZD, k)) j.m[dst * NC + k] = fma(a, j.m[src * NC + k], j.m[dst * NC + k]);
 }
 
 // row[dst] += a * row[delta]
-template <int NC, bool ZD>
-__device__ __forceinline__ void dterm(JS<NC, ZD>& j, int dst, double a) {
+template <int NC, bool ZD, bool ZR>
+__device__ __forceinline__ void dterm(JS<NC, ZD, ZR>& j, int dst, double a) {
     if (ZD) axpy(j, dst, D, a);
     else j.m[dst * NC + D] += a;
 }
 
 // row[dst] += a * row[s1] + b * row[s2]
-template <int NC, bool ZD>
-__device__ __forceinline__ void add2(JS<NC, ZD>& j, int dst, int s1, double a, int s2, double b) {
+template <int NC, bool ZD, bool ZR>
+__device__ __forceinline__ void add2(JS<NC, ZD, ZR>& j, int dst, int s1, double a, int s2, double b) {
 #pragma unroll
     for (int k = 0; k < NC; k++)
         if (live_col(ZD, k))
@@ -77,8 +81,8 @@ __device__ __forceinline__ void add2(JS<NC, ZD>& j, int dst, int s1, double a, i
 }
 
 // row[dst] += a * row[s1] + b * row[s2] + e * row[s3]
-template <int NC, bool ZD>
-__device__ __forceinline__ void add3(JS<NC, ZD>& j, int dst, int s1, double a, int s2, double b, int s3, double e) {
+template <int NC, bool ZD, bool ZR>
+__device__ __forceinline__ void add3(JS<NC, ZD, ZR>& j, int dst, int s1, double a, int s2, double b, int s3, double e) {
 #pragma unroll
     for (int k = 0; k < NC; k++)
         if (live_col(ZD, k))
@@ -87,14 +91,14 @@ __device__ __forceinline__ void add3(JS<NC, ZD>& j, int dst, int s1, double a, i
 }
 
 // row[dst] = c * row[dst] + a * row[s1] (+ b * row[s2])
-template <int NC, bool ZD>
-__device__ __forceinline__ void scale_add1(JS<NC, ZD>& j, int dst, double c, int s1, double a) {
+template <int NC, bool ZD, bool ZR>
+__device__ __forceinline__ void scale_add1(JS<NC, ZD, ZR>& j, int dst, double c, int s1, double a) {
 #pragma unroll
     for (int k = 0; k < NC; k++)
         if (live_col(ZD, k)) j.m[dst * NC + k] = fma(a, j.m[s1 * NC + k], c * j.m[dst * NC + k]);
 }
-template <int NC, bool ZD>
-__device__ __forceinline__ void scale_add2(JS<NC, ZD>& j, int dst, double c, int s1, double a, int s2, double b) {
+template <int NC, bool ZD, bool ZR>
+__device__ __forceinline__ void scale_add2(JS<NC, ZD, ZR>& j, int dst, double c, int s1, double a, int s2, double b) {
 #pragma unroll
     for (int k = 0; k < NC; k++)
         if (live_col(ZD, k))
@@ -104,15 +108,17 @@ __device__ __forceinline__ void scale_add2(JS<NC, ZD>& j, int dst, double c, int
 __device__ __forceinline__ bool lost(const double* s) { return s[X] != s[X]; }
 
 // fastdrift with NormL = N = L * inv, inv = 1 / (1 + delta)
-template <int NC, bool ZD>
-__device__ __forceinline__ void drift(JS<NC, ZD>& j, double N, double inv) {
+template <int NC, bool ZD, bool ZR>
+__device__ __forceinline__ void drift(JS<NC, ZD, ZR>& j, double N, double inv) {
     double* s = j.s;
     const double px = s[PX], py = s[PY];
     const double q = fma(px, px, py * py);
     const double w = 0.5 * N * inv;
     // z first: it reads the px, py, delta rows only, like x and y
-    add2(j, Z, PX, -2.0 * w * px, PY, -2.0 * w * py);
-    dterm(j, Z, 2.0 * w * q * inv);
+    if constexpr (ZR) {
+        add2(j, Z, PX, -2.0 * w * px, PY, -2.0 * w * py);
+        dterm(j, Z, 2.0 * w * q * inv);
+    }
     axpy(j, X, PX, N);
     dterm(j, X, -N * inv * px);
     axpy(j, Y, PY, N);
@@ -147,8 +153,8 @@ __device__ __forceinline__ void poly(const double* __restrict__ A, const double*
 // thin kick of weight K; with NC = 7 and a parameter (kind PK_B / PK_A of order pn), its explicit
 // partial is added to column 6: d px/d B_n = -K Re z^n, d py/d B_n = K Im z^n,
 // d px/d A_n = K Im z^n, d py/d A_n = K Re z^n.
-template <int NC, bool ZD>
-__device__ __forceinline__ void kick(JS<NC, ZD>& j, const double* A, const double* B, int M, double K, int pkind,
+template <int NC, bool ZD, bool ZR>
+__device__ __forceinline__ void kick(JS<NC, ZD, ZR>& j, const double* A, const double* B, int M, double K, int pkind,
                                      int pn) {
     double* s = j.s;
     const double x = s[X], y = s[Y];
@@ -177,8 +183,8 @@ __device__ __forceinline__ void kick(JS<NC, ZD>& j, const double* A, const doubl
 }
 
 // StrMPole (accel.cpp:800-847), Yoshida slices; delta is constant inside the element
-template <int NC, bool ZD>
-__device__ __forceinline__ void strmpole(JS<NC, ZD>& j, const DevElem& e, int pkind, int pn) {
+template <int NC, bool ZD, bool ZR>
+__device__ __forceinline__ void strmpole(JS<NC, ZD, ZR>& j, const DevElem& e, int pkind, int pn) {
     const double* A = e.v + V_A;
     const double* B = e.v + V_B;
     const int M = e.order_eff;
@@ -198,8 +204,8 @@ __device__ __forceinline__ void strmpole(JS<NC, ZD>& j, const DevElem& e, int pk
 }
 
 // hx drift of length L with curvature h at fixed delta (inv = 1 / (1 + delta))
-template <bool ZD>
-__device__ __forceinline__ void hxdrift(JS<6, ZD>& j, double L, double h, double inv) {
+template <bool ZD, bool ZR>
+__device__ __forceinline__ void hxdrift(JS<6, ZD, ZR>& j, double L, double h, double inv) {
     double* s = j.s;
     const double px = s[PX], py = s[PY];
     const double a = inv * L, b = 0.25 * h * L * L * inv * inv, c = 0.5 * h * L * inv;
@@ -208,8 +214,10 @@ __device__ __forceinline__ void hxdrift(JS<6, ZD>& j, double L, double h, double
     const double hx1 = fma(h, s[X], 1.0);
     const double gp = fma(g, px, 1.0);
     // z and y read the old x, px, py, delta rows; x then reads old px, py; px last
-    add3(j, Z, X, -h * dd * q, PX, -2.0 * hx1 * dd * px, PY, -2.0 * hx1 * dd * py);
-    dterm(j, Z, 2.0 * inv * hx1 * dd * q);
+    if constexpr (ZR) {
+        add3(j, Z, X, -h * dd * q, PX, -2.0 * hx1 * dd * px, PY, -2.0 * hx1 * dd * py);
+        dterm(j, Z, 2.0 * inv * hx1 * dd * q);
+    }
     add3(j, Y, X, h * a * py * gp, PX, hx1 * a * py * g, PY, hx1 * a * gp);
     dterm(j, Y, -inv * hx1 * a * py * gp);
     scale_add2(j, X, fma(h * px, a, 1.0), PX, fma(2.0 * b, px, hx1 * a), PY, -2.0 * b * py);
@@ -223,8 +231,8 @@ __device__ __forceinline__ void hxdrift(JS<6, ZD>& j, double L, double h, double
 }
 
 // curved kick of weight L (atpass.cpp:199-235, no radiation), field B[0..M] (no skew terms)
-template <bool ZD>
-__device__ __forceinline__ void bend_kick(JS<6, ZD>& j, const double* B, int M, double h, double K1, double K2,
+template <bool ZD, bool ZR>
+__device__ __forceinline__ void bend_kick(JS<6, ZD, ZR>& j, const double* B, int M, double h, double K1, double K2,
                                           double L) {
     double* s = j.s;
     const double x = s[X], y = s[Y], x2 = x * x, y2 = y * y;
@@ -241,15 +249,15 @@ __device__ __forceinline__ void bend_kick(JS<6, ZD>& j, const double* B, int M, 
     add2(j, PX, X, -L * ax, Y, -L * ay);
     dterm(j, PX, -L * ad);
     add2(j, PY, X, L * fma(h, t2x, di), Y, L * fma(h, t2y, dr));
-    axpy(j, Z, X, -L * h);
+    if constexpr (ZR) axpy(j, Z, X, -L * h);
     s[PX] = fma(-L, av, s[PX]);
     s[PY] = fma(L, fma(h, t2, im), s[PY]);
     s[Z] = fma(-L * h, x, s[Z]);
 }
 
 // BendMPole without radiation (accel.cpp:649-705): edge, Yoshida slices, edge
-template <bool ZD>
-__device__ __forceinline__ void bendmpole(JS<6, ZD>& j, const DevElem& e) {
+template <bool ZD, bool ZR>
+__device__ __forceinline__ void bendmpole(JS<6, ZD, ZR>& j, const DevElem& e) {
     const double* B = e.v + V_B;
     const int M = e.order_eff;
     const double h = e.v[V_IRHO], K1b = e.v[V_BK1], K2b = e.v[V_BK2];
@@ -274,8 +282,8 @@ __device__ __forceinline__ void bendmpole(JS<6, ZD>& j, const DevElem& e) {
     j.s[PY] = fma(-j.s[Y], psi2, j.s[PY]);
 }
 
-template <int NC, bool ZD>
-__device__ __forceinline__ void drift_len(JS<NC, ZD>& j, double L) {
+template <int NC, bool ZD, bool ZR>
+__device__ __forceinline__ void drift_len(JS<NC, ZD, ZR>& j, double L) {
     const double inv = 1.0 / (1.0 + j.s[D]);
     drift(j, L * inv, inv);
 }

@@ -241,8 +241,8 @@ __device__ __noinline__ jac::JS<6> dual_elem(jac::JS<6> j, const DevElem* __rest
 // made and the kernel keeps the small register budget of the explicit maps.  ZD = false: the
 // unit has no element that reads z or changes delta (unit_zd, set by the host), so the cavity
 // case cannot occur in it.
-template <bool GENERAL, bool ZD>
-__device__ __forceinline__ void jac_elem(jac::JS<6, ZD>& j, const DevElem* __restrict__ e) {
+template <bool GENERAL, bool ZD, bool ZR>
+__device__ __forceinline__ void jac_elem(jac::JS<6, ZD, ZR>& j, const DevElem* __restrict__ e) {
     if (jac::lost(j.s)) return;
     switch (e->op) {
     case OP_NOP: return;
@@ -312,20 +312,20 @@ __device__ __noinline__ fast::St param_elem_dual(jac::JS<6> j, const DevElem* __
 // One unit: the plain elements [e0, e1), then parameter element pe (or none, pe < 0); stores the
 // unit's Jacobian at J and the parameter sensitivities at S (tiled, stride kTile per entry and
 // pstride per parameter) and advances the state s.
-template <bool GENERAL, bool ZD>
+template <bool GENERAL, bool ZD, bool ZR>
 __device__ __forceinline__ void jtape_unit(const AdjParams& a, double* s, int e0, int e1, int pe,
                                            double* __restrict__ J, double* __restrict__ S, int64_t pstride) {
-    jac::JS<6, ZD> j;
+    jac::JS<6, ZD, ZR> j;
 #pragma unroll
     for (int i = 0; i < 6; i++) j.s[i] = s[i];
     jac::set_identity(j);
-    for (int e = e0; e < e1; e++) jac_elem<GENERAL, ZD>(j, a.tbl + e);
+    for (int e = e0; e < e1; e++) jac_elem<GENERAL, ZD, ZR>(j, a.tbl + e);
     if (pe >= 0) {
         const DevElem* el = a.tbl + pe;
         const int np = a.pcount[pe], f = a.pfirst[pe], kind = a.pkind[f];
         if (np == 1 && (el->op == OP_STRMPOLE || el->op == OP_STRKICK) && (kind == adj::PK_B || kind == adj::PK_A) &&
             !jac::lost(j.s)) {
-            jac::JS<7, ZD> q;
+            jac::JS<7, ZD, ZR> q;
 #pragma unroll
             for (int i = 0; i < 6; i++) {
                 q.s[i] = j.s[i];
@@ -357,7 +357,9 @@ __device__ __forceinline__ void jtape_unit(const AdjParams& a, double* s, int e0
     }
 }
 
-template <bool GENERAL>
+// ZR = false: the z rows of the unit Jacobians are left at e_z (jacobian.cuh), for a line with no
+// element that reads z and a reverse sweep whose seed has no z component.
+template <bool GENERAL, bool ZR>
 __device__ __forceinline__ void jtape_one(const AdjParams& a, const double* turn_tape, int j0, int64_t gid,
                                           const double* final_x, int npe, double* jt, double* sens) {
     const int64_t n = a.n;
@@ -380,10 +382,10 @@ __device__ __forceinline__ void jtape_one(const AdjParams& a, const double* turn
         double* J = jt + ((((int64_t)t * (npe + 1) + c) * ntile + b) * 36) * kTile + l;
         double* S = pe >= 0 ? sens + ((((int64_t)t * a.nparam + a.pfirst[pe]) * ntile + b) * 6) * kTile + l : nullptr;
         if constexpr (GENERAL) {
-            jtape_unit<true, true>(a, s, e0, e1, pe, J, S, pstride);
+            jtape_unit<true, true, true>(a, s, e0, e1, pe, J, S, pstride);
         } else {
-            if (a.unit_zd[c]) jtape_unit<false, true>(a, s, e0, e1, pe, J, S, pstride);
-            else jtape_unit<false, false>(a, s, e0, e1, pe, J, S, pstride);
+            if (a.unit_zd[c]) jtape_unit<false, true, true>(a, s, e0, e1, pe, J, S, pstride);
+            else jtape_unit<false, false, ZR>(a, s, e0, e1, pe, J, S, pstride);
         }
         e0 = e1 + 1;
     }
@@ -397,14 +399,14 @@ __device__ __forceinline__ void jtape_one(const AdjParams& a, const double* turn
 //     leaves, so the latency-bound forward keeps its SMs to itself; block 0 never leaves, so
 //     every unit is taped whatever the placement.  Each pass of the loop takes one group or
 //     leaves, and the counter only grows, so the loop ends.
-template <bool GENERAL>
+template <bool GENERAL, bool ZR>
 __global__ void __launch_bounds__(128, GENERAL ? 1 : 3) k_adj_jtape(const AdjParams a, const double* turn_tape, int j0,
                                                                     int nt, const double* final_x, int npe, double* jt,
                                                                     double* sens, int* work, const int* sm_fwd) {
     const int64_t units = a.n * (int64_t)nt;
     if (!work) {
         const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-        if (gid < units) jtape_one<GENERAL>(a, turn_tape, j0, gid, final_x, npe, jt, sens);
+        if (gid < units) jtape_one<GENERAL, ZR>(a, turn_tape, j0, gid, final_x, npe, jt, sens);
         return;
     }
     const int64_t groups = (units + 127) / 128;
@@ -421,7 +423,7 @@ __global__ void __launch_bounds__(128, GENERAL ? 1 : 3) k_adj_jtape(const AdjPar
         __syncthreads();
         if (g < 0 || g >= groups) return;
         const int64_t gid = g * 128 + threadIdx.x;
-        if (gid < units) jtape_one<GENERAL>(a, turn_tape, j0, gid, final_x, npe, jt, sens);
+        if (gid < units) jtape_one<GENERAL, ZR>(a, turn_tape, j0, gid, final_x, npe, jt, sens);
     }
 }
 
@@ -529,6 +531,20 @@ __global__ void __launch_bounds__(kTile) k_adj_jsweep(const AdjParams a, int nt,
     }
 }
 
+// flag = 1 when any of v[0 .. n) is not zero (the flag is zeroed before the launch)
+__global__ void k_any_nonzero(const double* __restrict__ v, int64_t n, int* flag) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        if (v[i] != 0.0) {
+            *flag = 1;
+            return;
+        }
+}
+
+void launch_any_nonzero(const double* v, int64_t n, int* flag, cudaStream_t s) {
+    cudaMemsetAsync(flag, 0, sizeof(int), s);
+    k_any_nonzero<<<(unsigned)std::min<int64_t>(1024, (n + 255) / 256 + 1), 256, 0, s>>>(v, n, flag);
+}
+
 __global__ void k_adj_reduce(const double* part, int nblk, int nparam, double* out) {
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nparam; j += gridDim.x * blockDim.x) {
         double s = 0;
@@ -600,19 +616,17 @@ bool jtape_needs_general(const DevElem* t, int ne, const int32_t* pcount, const 
 
 void launch_adj_jtape(const AdjParams& a, const double* turn_tape, int j0, int nt, const double* final_x,
                       int npe, double* jt, double* sens, bool general, cudaStream_t s, int* work,
-                      const int* sm_fwd, int sm_count) {
+                      const int* sm_fwd, int sm_count, bool zrow) {
     const int64_t threads = a.n * (int64_t)nt;
     unsigned grid = (unsigned)((threads + 127) / 128);
+    // general lines always carry the z row
+    auto kern = general ? k_adj_jtape<true, true> : zrow ? k_adj_jtape<false, true> : k_adj_jtape<false, false>;
     if (work) {
         int per_sm = 0;
-        if (general) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_adj_jtape<true>, 128, 0);
-        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_adj_jtape<false>, 128, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, 0);
         grid = std::min<unsigned>(grid, (unsigned)std::max(1, per_sm * sm_count));
     }
-    if (general)
-        k_adj_jtape<true><<<grid, 128, 0, s>>>(a, turn_tape, j0, nt, final_x, npe, jt, sens, work, sm_fwd);
-    else
-        k_adj_jtape<false><<<grid, 128, 0, s>>>(a, turn_tape, j0, nt, final_x, npe, jt, sens, work, sm_fwd);
+    kern<<<grid, 128, 0, s>>>(a, turn_tape, j0, nt, final_x, npe, jt, sens, work, sm_fwd);
 }
 void launch_adj_jsweep(const AdjParams& a, int nt, const double* final_x, int npe, const int32_t* pelem,
                        const double* jt, const double* sens, double* grow, cudaStream_t s) {

@@ -152,11 +152,15 @@ void launch_adj_reduce(const double* part, int nblk, int nparam, double* out, cu
 // sweep over it (kern_adjoint.cu)
 // general: the line has elements or parameters outside the explicit-Jacobian maps
 // (jtape_needs_general)
+// *flag = 1 when any of v[0 .. n) is non-zero (the launcher zeroes it first, on s)
+void launch_any_nonzero(const double* v, int64_t n, int* flag, cudaStream_t s);
 // work: null (one unit per thread), or a zeroed counter: a grid of the resident blocks takes
-// groups of units from it, leaving the SMs sm_fwd marks (sm_count: the device's SMs)
+// groups of units from it, leaving the SMs sm_fwd marks (sm_count: the device's SMs).
+// zrow = false: the z rows of units with no element that reads z are left at e_z (valid for a
+// line with no such element swept with a seed whose z components are zero)
 void launch_adj_jtape(const AdjParams& a, const double* turn_tape, int j0, int nt, const double* final_x,
                       int npe, double* jt, double* sens, bool general, cudaStream_t s, int* work = nullptr,
-                      const int* sm_fwd = nullptr, int sm_count = 0);
+                      const int* sm_fwd = nullptr, int sm_count = 0, bool zrow = true);
 bool jtape_needs_general(const DevElem* host_tbl, int ne, const int32_t* pcount, const int32_t* pfirst,
                          const int32_t* pkind);
 // per tape unit (npe + 1 of them): 1 if any of its elements is not a drift, straight multipole,

@@ -322,7 +322,9 @@ int  accel_correct_chrom(accel_line* line, const int32_t* fam1, int n1, const in
  * a second stream behind the forward's own launches, and returns once it is written; the backward
  * is then one sweep.  Otherwise the backward tapes the Jacobians of a chunk of turns at once, as
  * many as fit the budget, or, when not even one turn fits, reverses turn by turn.  The ways give
- * the same gradient (the last to round-off).
+ * the same gradient (the last to round-off).  On a line where no element reads z (no cavity),
+ * the tapes leave out what only a z component of dL/dr_final would use; a backward call whose
+ * dl_drfinal has one writes the tapes again with it first (one more taping pass).
  */
 typedef struct accel_adjoint accel_adjoint;  /* holds its line (and context) until destroyed */
 int  accel_adjoint_create(accel_line* line, int N, int nturn, int ckpt_every,

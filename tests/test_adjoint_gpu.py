@@ -169,6 +169,48 @@ def test_tape_budget_paths_agree(A, ctx, LT):
     assert np.max(np.abs(p2 - p0)) < 1e-8 * np.max(np.abs(p0))
 
 
+def test_z_rows_taped_again_for_a_z_seed(A, ctx, LT):
+    """On a line where no element reads z (the 4D DBA), the forward writes the unit Jacobians
+    without their z rows, which a seed with zero z components multiplies by zero; a seed with a z
+    component has the tapes written again with them, from the kept turn starts, before its sweep.
+    The gradient is linear in the seed across the two kinds of tape, the z-free gradient is the
+    same bit for bit before and after the second taping, and the z part equals the one of the
+    checkpointed path (tapes chunk by chunk in the reverse pass)."""
+    ring = LT.config4_ring()
+    pairs = LT.sextupole_pairs(ring)
+    elems = sorted({i for p in pairs for i in p})[:6]
+    params = [(i, A.F_POLYNOMB, 2) for i in elems]
+    n, nturn, every = 64, 64, 16
+    r0 = LT.config4_particles(n, seed=3)
+    adj = A.Adjoint(A.Line(ctx, ring), n, nturn, every, params)
+    rf = adj.forward(r0)
+    assert not np.isnan(rf[:, 0]).any()
+    g = np.zeros_like(rf)
+    g[:, 0], g[:, 2] = 2 * rf[:, 0], 2 * rf[:, 2]
+    gz = np.zeros_like(rf)
+    gz[:, 4] = np.random.default_rng(5).normal(size=n)
+    d0, p0 = adj.backward(g)
+    dz, pz = adj.backward(gz)
+    d1, p1 = adj.backward(g)
+    df, pf = adj.backward(g + gz)
+    adj.close()
+    assert np.array_equal(d0, d1) and np.array_equal(p0, p1)
+    assert np.max(np.abs(dz)) > 0
+    assert np.max(np.abs(df - d0 - dz)) < 1e-12 * np.max(np.abs(df))
+    assert np.max(np.abs(pf - p0 - pz)) < 1e-12 * np.max(np.abs(pf))
+    # 170,000 bytes: above one turn's tapes (147,456), below the run's turn starts (196,608)
+    A.set_adjoint_tape_budget(170000)
+    try:
+        adj_c = A.Adjoint(A.Line(ctx, ring), n, nturn, every, params)
+        adj_c.forward(r0)
+        dzc, pzc = adj_c.backward(gz)
+        adj_c.close()
+    finally:
+        A.set_adjoint_tape_budget(None)
+    assert np.max(np.abs(dzc - dz)) < 1e-13 * np.max(np.abs(dz))
+    assert np.max(np.abs(pzc - pz)) < 1e-12 * np.max(np.abs(pz))
+
+
 def test_adjoint_one_turn_jacobian_is_exact(A, ctx, LT):
     """Six particles at the closed orbit (the origin of the 4D ring), seeded with unit adjoints:
     row i of the one-turn matrix is dL/dr0 of particle i for L = r_final[i]."""
