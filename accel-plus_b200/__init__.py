@@ -116,6 +116,7 @@ def lib() -> C.CDLL:
         "accel_autotune": (I, [P, I, P, P, C.c_int64, C.POINTER(I)]),
         "accel_set_tile": (I, [P, I, I, I]),
         "accel_get_tile": (I, [P, C.POINTER(I)]),
+        "accel_set_stage_wait": (I, [P, I]),
         "accel_m66": (I, [P, I, I, D, D, I, C.POINTER(D)]),
         "accel_m66_at": (I, [P, I, I, C.POINTER(D), I, D, C.POINTER(D)]),
         "accel_m66_knob": (I, [P, I, I, C.POINTER(D), I, P, P, P, C.POINTER(D), C.POINTER(D)]),
@@ -355,6 +356,10 @@ class Context:
 
     def set_tile(self, block=0, seg_turns=0, variant=-1):
         _check(lib().accel_set_tile(self.h, block, seg_turns, variant), "accel_set_tile")
+
+    def set_stage_wait(self, probes: int = 0):
+        """accel_set_stage_wait: the staged schedule's first-wait probes (0 default, < 0 none)."""
+        _check(lib().accel_set_stage_wait(self.h, int(probes)), "accel_set_stage_wait")
 
     def get_tile(self):
         t = (C.c_int * 3)()

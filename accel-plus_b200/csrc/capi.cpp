@@ -291,6 +291,7 @@ static int emit_part(accel_ctx* C, const CoreReq& q, int part, int turns, cudaSt
     P.err = cnt + 4;
     P.lost_flag = cnt + 5;
     P.tw_pair_passes = cnt + 6;
+    P.stage_wait = C->stage_wait;
     P.seed = L0->seed;
     P.rng_base = (int32_t*)L0->d_rng.p;
     P.turn0 = 0;
@@ -518,7 +519,17 @@ static int run_core(accel_ctx* C, const CoreReq& q, cudaStream_t user) {
         C->bps[qs.variant] = fused_blocks_per_sm(qs.variant);
         if (C->bps[qs.variant] <= 0) return fail(ACCEL_E_CUDA, "fused kernel cannot be resident");
     }
-    return run_core_plan(C, qs, user);
+    if (q.mode != ACCEL_MODE_FUSED || qs.sched != kSchedStaged) return run_core_plan(C, qs, user);
+    // the staged kernel's bulk copies are waited on with a bounded wait; a wait that ran out sets
+    // the error word (cnt[4]) and its block leaves, so the run is checked before returning
+    int32_t* err = (int32_t*)C->cnt.p + 4;
+    CK(cudaMemsetAsync(err, 0, sizeof(int32_t), C->stream));
+    if ((s = run_core_plan(C, qs, user))) return s;
+    int32_t h = 0;
+    CK(cudaMemcpyAsync(&h, err, sizeof h, cudaMemcpyDeviceToHost, C->stream));
+    CK(cudaStreamSynchronize(C->stream));
+    if (h) return fail(ACCEL_E_TIMEOUT, "a shared-memory staging copy did not complete in its bounded wait");
+    return ACCEL_OK;
 }
 
 // Issue a prepared request (buffers sized, schedule resolved): as graphs, or directly with events.
@@ -1166,6 +1177,14 @@ int accel_set_tile(accel_ctx* C, int block, int seg_turns, int variant) {
     C->tile_variant = variant;
     C->tile_seg = seg_turns;
     C->graphs.clear();
+    return ACCEL_OK;
+}
+
+int accel_set_stage_wait(accel_ctx* C, int probes) {
+    if (!C) return fail(ACCEL_E_INVALID, "NULL ctx");
+    std::lock_guard<std::mutex> lk(C->mu);
+    C->stage_wait = probes;
+    C->graphs.clear();  // the limit is a launch parameter of the captured graphs
     return ACCEL_OK;
 }
 

@@ -181,7 +181,8 @@ __global__ void __launch_bounds__(BS, MINB) k_fused_staged(const TrackParams P, 
                 mbar_expect_tx(ma, bytes);
                 asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
                              ::"r"(sa), "l"(src), "r"(bytes), "r"(ma) : "memory");
-                if (!mbar_wait(ma, phase, kStageWaitLimit)) {
+                const int first = P.stage_wait < 0 ? 0 : P.stage_wait == 0 ? kStageWaitLimit : P.stage_wait;
+                if (!mbar_wait(ma, phase, first)) {
                     s_fail = 1;
                     atomicExch(P.err, 1);
                     mbar_wait(ma, phase, kStageWaitLimit);  // the copy in flight, before leaving

@@ -29,6 +29,8 @@ struct TrackParams {
     const int32_t* rng_base; // device: QE turn base of the line (advanced per call)
     uint64_t seed;
     int32_t* tw_pair_passes; // transverse wake passes that fell back to the pair sum (may be null)
+    int stage_wait;          // staged schedule: try_wait probes of a stage's first wait (0: the
+                             // default limit; < 0: none, the wait counts as run out at once)
 };
 
 // ---- fused (kern_fused.cu) ----------------------------------------------------------------

@@ -57,6 +57,7 @@ struct accel_ctx {
         probe_state, tw_scratch, hot;  // hot: the element records' first lines (staged schedule)
     int tile_variant = -1;  // -1: tuned or default
     int tile_seg = 0;       // 0: tuned or default
+    int stage_wait = 0;     // staged schedule's first-wait probes (accel_set_stage_wait)
     int tile_sched = -1;    // -1: tuned or default
     int bps[accel::kNumFusedVariants] = {0};
     std::map<accel::GraphKey, std::unique_ptr<accel::GraphEntry>> graphs;

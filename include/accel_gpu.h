@@ -268,6 +268,12 @@ int  accel_autotune(accel_line* const* lines, int ninst, const int64_t* part_off
                     const double* r_soa, int64_t ntot, int* tile_out3);
 int  accel_set_tile(accel_ctx* ctx, int block, int seg_turns, int variant);  /* 0s = auto */
 int  accel_get_tile(accel_ctx* ctx, int* tile_out3);
+/* The staged schedule (mode 2) waits for each block's shared-memory copy with a bounded number
+ * of try_wait probes; a wait that runs out sets an error word, the block waits (bounded again)
+ * for its copy in flight and leaves, and the call returns ACCEL_E_TIMEOUT.  probes sets the
+ * first wait's limit: 0 the default (2^22), < 0 none (the wait runs out at once, which tests
+ * that path).  No counterpart in the reference. */
+int  accel_set_stage_wait(accel_ctx* ctx, int probes);
 
 /*
  * One-turn (or [st, ed)) 6x6 transfer matrix around the point (0,0,0,0,0,dpp) (row-major m[36]).

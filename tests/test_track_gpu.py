@@ -456,6 +456,43 @@ def test_crab_rfmult_wiggler_against_reference(A, ctx, mode):
             assert np.all(np.isfinite(ex)) and np.max(np.abs(ex - fd)) < 1e-6 * np.max(np.abs(fd)), name
 
 
+def test_staged_wait_that_runs_out_is_a_status(A, ctx, LT):
+    """The staged schedule waits for each block's shared-memory copy with a bounded number of
+    probes.  A wait that runs out (forced here: a first wait of zero probes) sets the error word;
+    the block then waits, bounded again, for its copy in flight and leaves, and the call returns
+    ACCEL_E_TIMEOUT instead of results.  The context stays usable: with the default limit the
+    next call tracks as the default schedule does, bit for bit."""
+    import torch
+    base = LT.config2_ring()
+    lines = [A.Line(ctx, LT.error_copy(base, k)) for k in (0, 1)]
+    grids = [LT.da_grid(11, 5), LT.da_grid(9, 7)]
+    off = np.zeros(3, dtype=np.int64)
+    off[1:] = np.cumsum([g.shape[0] for g in grids])
+    aos = np.concatenate(grids)
+
+    def run(tile):
+        ctx.set_tile(0, 8, tile)
+        soa = torch.tensor(aos.T.copy(), device="cuda").contiguous()
+        loss = torch.empty(len(aos), device="cuda", dtype=torch.int32)
+        A.track_batched(lines, off, soa, 16, loss=loss)
+        torch.cuda.synchronize()
+        return soa.cpu().numpy(), loss.cpu().numpy()
+
+    try:
+        ctx.set_stage_wait(-1)
+        with pytest.raises(A.AccelError) as err:
+            run(200)
+        assert err.value.status == A.E_TIMEOUT
+        ctx.set_stage_wait(0)
+        a, la = run(200)
+        b, lb = run(0)
+    finally:
+        ctx.set_stage_wait(0)
+        ctx.set_tile(0, 0, -1)
+    assert np.array_equal(la, lb)
+    assert same_bits(a, b)
+
+
 @pytest.mark.parametrize("variant", [0, 1, 2])
 def test_staged_schedule_equals_fused(A, ctx, LT, variant):
     """The instance-staged schedule (each block stages one instance's element hot lines in shared
