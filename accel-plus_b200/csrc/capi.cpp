@@ -1305,6 +1305,13 @@ int accel_line_setrfphase(accel_line* L, double* phis_out) {
 }
 
 // ---- beam statistics, peak probe, counters ---------------------------------------------------
+// sums `count` device doubles over the context's ranks (accel_beam_stat's exchange)
+static int stat_allreduce(void* ctx, double* buf, int count, cudaStream_t s) {
+    accel_ctx* C = (accel_ctx*)ctx;
+    const ncclResult_t r = nccl().AllReduce(buf, buf, (size_t)count, ncclFloat64, ncclSum, (ncclComm_t)C->comm, s);
+    return r == ncclSuccess ? 0 : nccl_fail("ncclAllReduce (beam moments)", r);
+}
+
 int accel_beam_stat(accel_ctx* C, const double* r, int layout, int N, double* mean, double* sigma,
                     double* cross, int* nlive) {
     if (!C || !r || N <= 0) return fail(ACCEL_E_INVALID, "bad argument");
@@ -1327,7 +1334,10 @@ int accel_beam_stat(accel_ctx* C, const double* r, int layout, int N, double* me
     if ((s = C->scratch.ensure(sizeof(double) * kScratchDoubles))) return s;
     double* part = (double*)C->scratch.p;
     double* out = part + 12 * (size_t)nblk + 32;
-    launch_beam_stat(soa, N, part, nblk, out, C->stream);
+    // a context with a communicator holds its rank's part of a bunch: the moments are the
+    // bunch's, the two passes' sums added over the ranks (every rank takes this call)
+    if ((s = launch_beam_stat(soa, N, part, nblk, out, C->stream, C->comm ? stat_allreduce : nullptr, C)))
+        return s;
     C->launches += 5;
     double h[19];
     CK(cudaMemcpyAsync(h, out, sizeof(h), cudaMemcpyDeviceToHost, C->stream));

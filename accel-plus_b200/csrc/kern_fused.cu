@@ -587,15 +587,20 @@ __global__ void k_stat_out(const double* s1, const double* s2, double* out) {
     }
 }
 
-void launch_beam_stat(const double* st, int64_t n, double* part, int nblk, double* out,
-                      cudaStream_t s) {
+int launch_beam_stat(const double* st, int64_t n, double* part, int nblk, double* out, cudaStream_t s,
+                     StatReduce reduce, void* rctx) {
     double* s1 = part + 12 * (size_t)nblk;
     double* s2 = s1 + 8;
     k_stat1<<<nblk, kStatThreads, 0, s>>>(st, n, part);
     k_stat_fin<<<1, 32, 0, s>>>(part, nblk, 7, s1);
+    int r = reduce ? reduce(rctx, s1, 7, s) : 0;  // the sums and live count of every rank
+    if (r) return r;
     k_stat2<<<nblk, kStatThreads, 0, s>>>(st, n, s1, part);
     k_stat_fin<<<1, 32, 0, s>>>(part, nblk, 12, s2);
+    r = reduce ? reduce(rctx, s2, 12, s) : 0;  // the centred second moments of every rank
+    if (r) return r;
     k_stat_out<<<1, 32, 0, s>>>(s1, s2, out);
+    return 0;
 }
 
 // ---- FP64 FMA throughput probe --------------------------------------------------------------

@@ -100,9 +100,13 @@ void launch_longwake_stage(int stage, const TrackParams& p, const LwParams& w, d
                            int32_t* counts, cudaStream_t s);
 // scratch[0..5] from the exchanged z range and count (kern_coll.cu)
 void launch_lw_regeom(double* scratch, int nbins, double charge_nc, cudaStream_t s);
-// moments of live particles: out[0..5] mean, [6..11] sigma, [12..17] cross, [18] nlive
-void launch_beam_stat(const double* st, int64_t n, double* partial, int nblk, double* out,
-                      cudaStream_t s);
+// moments of live particles: out[0..5] mean, [6..11] sigma, [12..17] cross, [18] nlive.
+// reduce (may be null) sums `count` device doubles over the ranks of a bunch spread over GPUs, in
+// place on stream s, between the passes (the sums and count, then the centred moments); it
+// returns a status, which the launcher returns (0: success)
+typedef int (*StatReduce)(void* ctx, double* buf, int count, cudaStream_t s);
+int launch_beam_stat(const double* st, int64_t n, double* partial, int nblk, double* out, cudaStream_t s,
+                     StatReduce reduce = nullptr, void* rctx = nullptr);
 int beam_stat_blocks(int64_t n);
 double fp64_peak_run(int sm_count, cudaStream_t s, float* ms_out, double* sm_mhz_out);
 

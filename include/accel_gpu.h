@@ -347,7 +347,9 @@ int  accel_adjoint_backward(accel_adjoint* adj, const double* dl_drfinal, double
 int  accel_set_adjoint_tape_budget(int64_t bytes);
 
 /* Beam moments of live particles (calc_beam_stat, utility.cpp:387-438): mean[6], sigma[6],
- * cross[6] = <xx'>,<yy'>,<x d>,<x' d>,<y z>,<y' z>; returns the live count in *nlive.       */
+ * cross[6] = <xx'>,<yy'>,<x d>,<x' d>,<y z>,<y' z>; returns the live count in *nlive.  On a
+ * context with a communicator (accel_ctx_set_comm) r is this rank's part of a bunch and the
+ * moments are the whole bunch's: every rank of the communicator makes the call.              */
 int  accel_beam_stat(accel_ctx* ctx, const double* r, int layout, int N, double* mean,
                      double* sigma, double* cross, int* nlive);
 

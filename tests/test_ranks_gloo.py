@@ -149,6 +149,26 @@ order = np.argsort(np.where(np.isnan(r[:, 0]), np.inf, r[:, 4]), kind="stable")
 half = order[: N // 2] if rank == 0 else order[N // 2:]
 mine = staged_wake(r[half].copy())
 res["contiguous_bit_exact"] = bool(np.array_equal(mine.view(np.int64), ref[half].view(np.int64)))
+# the bunch's moments from the two halves (accel_beam_stat with a communicator): the sums and
+# live count added over the ranks, then the centred second moments with the bunch's means
+mine = r[half]
+live = ~np.isnan(mine[:, 0])
+s1 = torch.tensor(np.append(mine[live].sum(axis=0), live.sum()), dtype=torch.float64)
+dist.all_reduce(s1, op=dist.ReduceOp.SUM)
+s1 = s1.numpy()
+mean = s1[:6] / s1[6]
+d = mine[live] - mean
+s2 = torch.tensor(np.concatenate([(d * d).sum(axis=0), [(d[:, 0] * d[:, 1]).sum(), (d[:, 2] * d[:, 3]).sum(),
+                  (d[:, 0] * d[:, 5]).sum(), (d[:, 1] * d[:, 5]).sum(), (d[:, 2] * d[:, 4]).sum(),
+                  (d[:, 3] * d[:, 4]).sum()]]), dtype=torch.float64)
+dist.all_reduce(s2, op=dist.ReduceOp.SUM)
+s2 = s2.numpy()
+m_ref, sig_ref, cross_ref, nl_ref = O.port_beam_stat(r)
+res["moments_count"] = bool(int(s1[6]) == nl_ref)
+sc = np.where(sig_ref > 0, sig_ref, 1.0)  # x', y and y' of this bunch are all zero
+res["moments_rel_err"] = float(max(np.max(np.abs(mean - m_ref) / sc),
+                                   np.max(np.abs(np.sqrt(s2[:6] / s1[6]) - sig_ref) / sc),
+                                   np.max(np.abs(s2[6:] / s1[6] - cross_ref)) / np.max(sig_ref) ** 2))
 dist.barrier()
 dist.destroy_process_group()
 print("RESULT " + json.dumps(res))
@@ -159,7 +179,10 @@ def test_two_gloo_ranks_split_bunch_wake():
     """The longitudinal wake of a bunch split over two ranks, exchanged as the engine does it
     (z range and live count by min / max / sum, then bin counts by sum): each rank's kicked
     particles equal, bit for bit, the one-rank wake of the whole bunch (integer counts and exact
-    min / max make the exchange exact)."""
+    min / max make the exchange exact).  The bunch's moments from the two halves, exchanged as
+    accel_beam_stat does with a communicator (first-pass sums and count, then centred second
+    moments, each summed over the ranks), equal the oracle's moments of the whole bunch to
+    1e-12."""
     pytest.importorskip("torch")
     port = free_port()
     procs = []
@@ -175,3 +198,6 @@ def test_two_gloo_ranks_split_bunch_wake():
         res.append(json.loads([l for l in out.splitlines() if l.startswith("RESULT ")][-1][7:]))
     for r in res:
         assert r["interleaved_bit_exact"] and r["contiguous_bit_exact"] and r["kicked"], r
+        # the moments of the split bunch against the oracle's moments of the whole bunch: the
+        # same sums in another order of additions
+        assert r["moments_count"] and r["moments_rel_err"] < 1e-12, r

@@ -84,3 +84,24 @@ def test_one_rank_exchange_reproduces_local_transverse_wake(A):
     a, b = out
     assert np.array_equal(a, b, equal_nan=True)
     assert not np.array_equal(a[:, 1], r0[:, 1])
+
+
+def test_one_rank_exchange_reproduces_local_beam_moments(A):
+    """accel_beam_stat on a context with a communicator gives the moments of the whole bunch: the
+    first pass's sums and live count, then the centred second moments, summed over the ranks
+    between the passes.  With one rank the sums are the rank's own, so the moments must equal the
+    local ones bit for bit, lost particles left out."""
+    rng = np.random.default_rng(14)
+    n = 30000
+    r = rng.normal(0, 1e-3, (n, 6))
+    r[::97, 0] = np.nan
+    out = []
+    for with_comm in (False, True):
+        ctx = A.Context(0)
+        if with_comm:
+            ctx.set_comm(A.nccl_unique_id(), 1, 0)
+        out.append(ctx.beam_stat(r.copy()))
+        ctx.close()
+    (m0, s0, c0, n0), (m1, s1, c1, n1) = out
+    assert n0 == n1 == n - len(range(0, n, 97))
+    assert np.array_equal(m0, m1) and np.array_equal(s0, s1) and np.array_equal(c0, c1)
