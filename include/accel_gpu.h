@@ -371,7 +371,8 @@ int  accel_beam_stat(accel_ctx* ctx, const double* r, int layout, int N, double*
  * address via cudaGetSymbolAddress, and the kernels loaded) with that device current; make that
  * first call before beginning any stream capture.  A failed set-up is retried by the next call.
  * A CUDA error already pending from earlier work is reported (ACCEL_E_CUDA) and left pending,
- * and nothing is launched.                                                                     */
+ * and nothing is launched.  It takes no context, so the moments are those of r alone, with no
+ * exchange over a communicator.                                                                */
 #define ACCEL_NOALLOC_STAT_MAX_N 4194304
 int  accel_beam_stat_noalloc(const double* r, int layout, int64_t N, double* out, void* stream);
 
