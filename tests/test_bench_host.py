@@ -45,4 +45,28 @@ def test_reference_arm_maps_no_engine_library(O):
     assert line["cpu_baseline"]["kind"] == "reference"
     assert "extrapolated" in line["cpu_baseline"]["sample"]
     assert line["process_maps_engine_library"] is False
+    assert line["native_so_loaded"] == ["oracle/_ref/libaccel_ref.so"]
     assert line["value"] > 0
+
+
+def test_nudge_growth_and_tangent_picks():
+    """The full-size gradient check's helpers: the growth of a 1e-12 nudge relative to each
+    coordinate's RMS (inf for a particle lost in either run), and the particles the forward-mode
+    check takes (the most sensitive with growth up to 1e4, and quiet ones drawn with a seed)."""
+    import numpy as np
+    sys.path.insert(0, ROOT)
+    import bench
+    rng = np.random.default_rng(0)
+    base = rng.normal(size=(200, 6))
+    nudged = base.copy()
+    nudged[:, 0] += 1e-12 * np.sqrt(np.mean(base[:, 0] ** 2)) * np.arange(200)
+    nudged[7, 0] = np.nan
+    g = bench.nudge_growth(base, nudged)
+    assert np.isinf(g[7])
+    assert np.allclose(g[[0, 1, 50]], [0.0, 1.0, 50.0], atol=1e-3)
+    growth = np.concatenate([np.linspace(0, 20, 100), [5e3, 2e4, 9e3, 3e3, 1e5, np.inf]])
+    pick = bench.tangent_picks(growth, 2, 3, seed=1)
+    assert list(pick[-2:]) == [100, 102]            # 5e3 and 9e3: the largest up to 1e4
+    quiet = [p for p in pick if p < 100]
+    assert len(quiet) == 3 and all(growth[p] <= 10 for p in quiet)
+    assert np.array_equal(pick, bench.tangent_picks(growth, 2, 3, seed=1))
