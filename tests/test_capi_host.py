@@ -198,8 +198,9 @@ def test_no_device_is_an_error_not_a_fallback(A):
     assert ei.value.status == A.E_NODEVICE
 
 
-def test_model_flops_match_survey_formula(A, LT):
-    """Config-1 FODO: 32 x [2 quads (m=1) + 2 sextupoles (m=2) + 2 bends (m=0) + 4 drifts]."""
+def test_model_flops_match_cost_formula(A, LT):
+    """The flop model (StrMPole slice 52 + 3(8m + 4), BendMPole slice 4*46 + 3(44 + 7m), drift
+    14) on the 32-cell FODO: 32 x [2 quads (m=1) + 2 sextupoles (m=2) + 2 bends (m=0) + 4 drifts]."""
     ring = LT.config1_ring()
     per_cell = 2 * 10 * (52 + 3 * 12) + 2 * 10 * (52 + 3 * 20) + 2 * (10 * (184 + 3 * 44) + 8) + 4 * 14
     assert LT.flops_per_turn(ring) == 32 * per_cell
