@@ -111,11 +111,11 @@ def load_golden(name: str) -> list:
     return A.read_lattice(path)
 
 
-def config1_ring() -> list:
+def fodo_ring() -> list:
     return load_golden("fodo32.lat")
 
 
-def config2_ring() -> list:
+def dba_ring() -> list:
     """DBA with the RF phase from setrfphase; radiation (classical) and cavity on."""
     ring = load_golden("dba18.lat")
     for d in ring:
@@ -126,8 +126,8 @@ def config2_ring() -> list:
     return ring
 
 
-def config4_ring() -> list:
-    """Config-2 ring without the cavity, radiation off (4D)."""
+def dba_4d_ring() -> list:
+    """The 18-cell DBA without its cavity, radiation off (4D)."""
     ring = [d for d in load_golden("dba18.lat") if d.type != A.CAVITY]
     for d in ring:
         if d.type == A.BENDMPOLE:
@@ -200,7 +200,7 @@ def error_copy(base: Sequence, seed: int, dk_rel: float = 1e-3, sigma_off: float
 
 def error_copy_text(seed: int, base_text: str | None = None, dk_rel: float = 1e-3,
                     sigma_off: float = 30e-6) -> str:
-    """The lattice file of error_copy(config2_ring(), seed), made from the text of dba18.lat in
+    """The lattice file of error_copy(dba_ring(), seed), made from the text of dba18.lat in
     pure Python (no engine library): the same draws in the same order, each StrMPole's two
     coefficient lines rewritten with 17 significant digits, every other line kept.  The result
     equals accel_lattice_write of the descriptor copy, character for character (the lattice
@@ -241,7 +241,7 @@ def da_grid(nx: int, ny: int, x0=-0.025, x1=0.025, y0=0.0, y1=0.012) -> np.ndarr
     return r.reshape(-1, 6).copy()
 
 
-def config1_particles(n: int = 1024, seed: int = 0) -> np.ndarray:
+def fodo_particles(n: int = 1024, seed: int = 0) -> np.ndarray:
     rng = np.random.default_rng(seed)
     r = np.zeros((n, 6))
     r[:, 0] = rng.uniform(-5e-3, 5e-3, n)
@@ -249,15 +249,15 @@ def config1_particles(n: int = 1024, seed: int = 0) -> np.ndarray:
     return r
 
 
-def config3_sizes(ncopy: int = 256, seed: int = 12345) -> list[tuple[int, int]]:
+def copy_grid_sizes(ncopy: int = 256, seed: int = 12345) -> list[tuple[int, int]]:
     rng = np.random.default_rng(seed)
     return [(int(rng.integers(21, 82)), int(rng.integers(11, 42))) for _ in range(ncopy)]
 
 
-def config3(ncopy: int = 256, seed: int = 12345):
+def batched_da_workload(ncopy: int = 256, seed: int = 12345):
     """(rings, part_off, AoS particles) for the batched uneven-DA workload."""
-    base = config2_ring()
-    sizes = config3_sizes(ncopy, seed)
+    base = dba_ring()
+    sizes = copy_grid_sizes(ncopy, seed)
     rings = [error_copy(base, k) for k in range(ncopy)]
     grids = [da_grid(nx, ny) for nx, ny in sizes]
     off = np.zeros(ncopy + 1, dtype=np.int64)
@@ -265,7 +265,7 @@ def config3(ncopy: int = 256, seed: int = 12345):
     return rings, off, np.concatenate(grids, axis=0)
 
 
-def config4_particles(n: int = 4096, seed: int = 1) -> np.ndarray:
+def gaussian_4d_particles(n: int = 4096, seed: int = 1) -> np.ndarray:
     rng = np.random.default_rng(seed)
     r = np.zeros((n, 6))
     r[:, 0] = rng.normal(0, 1e-3, n)
@@ -288,7 +288,7 @@ def twiss_from_m66(m: np.ndarray):
     return out
 
 
-def config5_particles(n: int, m66: np.ndarray, seed: int = 5, ex=10e-9, ey=10e-12, sz=3e-3,
+def matched_bunch_particles(n: int, m66: np.ndarray, seed: int = 5, ex=10e-9, ey=10e-12, sz=3e-3,
                       sd=1e-3) -> np.ndarray:
     """Gaussian bunch matched to the ring-entrance Twiss of m66."""
     rng = np.random.default_rng(seed)

@@ -125,7 +125,7 @@ def workload_shape(copies: int, rank: int):
     """(per-copy grid sizes, particle offsets, AoS particles) of the batched DA workload; pure
     numpy, no engine library."""
     LT = importlib.import_module("accel-plus_b200.lattices")
-    sizes = LT.config3_sizes(copies, seed=12345 + rank)
+    sizes = LT.copy_grid_sizes(copies, seed=12345 + rank)
     grids = [LT.da_grid(nx, ny) for nx, ny in sizes]
     off = np.zeros(copies + 1, dtype=np.int64)
     off[1:] = np.cumsum([g.shape[0] for g in grids])
@@ -134,7 +134,7 @@ def workload_shape(copies: int, rank: int):
 
 def workload(copies: int, rank: int):
     LT = importlib.import_module("accel-plus_b200.lattices")
-    base = LT.config2_ring()
+    base = LT.dba_ring()
     sizes, off, aos = workload_shape(copies, rank)
     rings = [LT.error_copy(base, rank * copies + k) for k in range(copies)]
     return rings, off, aos, sizes
@@ -170,7 +170,7 @@ def cpu_reference_rate(sizes, off, aos, rank: int = 0, turns_goal: float = 15.0,
     copies = len(sizes)
     picks = reference_copies(sizes, count)
     if kind == "port":  # the C restatement takes descriptors (the engine's host-only reader)
-        base = LT.config2_ring()
+        base = LT.dba_ring()
 
     def run(k, nturn):
         r = aos[off[k]:off[k + 1]].copy()
@@ -285,14 +285,14 @@ def adjoint_leg(A, LT, ctx, steps: int = 3, ranks=None, check: bool = True) -> d
     differences per scalar
     input 2 x (6 x 4096 + 36); batched over the independent particles (one coordinate of every
     particle at once) 2 x (6 + 36)."""
-    ring = LT.config4_ring()
+    ring = LT.dba_4d_ring()
     line = A.Line(ctx, ring)
     pairs = LT.sextupole_pairs(ring)
     elems = sorted({i for p in pairs for i in p})
     params = [(i, A.F_POLYNOMB, 2) for i in elems]
     n, nturn, every = 4096, 512, 64
     rank = ranks.rank if ranks else 0
-    r0 = LT.config4_particles(n, seed=1 + rank)
+    r0 = LT.gaussian_4d_particles(n, seed=1 + rank)
     adj = A.Adjoint(line, n, nturn, every, params)
 
     def gradient():
@@ -397,7 +397,7 @@ def adjoint_fd_check(A, LT, ctx, adj, r0, nturn, pairs, elems, knob_steps=(3e-6,
     against the only derivative the reference itself can give, its own tracking differenced."""
     import torch
     n = len(r0)
-    ring = LT.config4_ring()
+    ring = LT.dba_4d_ring()
     scale = np.sqrt(np.mean(r0 ** 2, axis=0))
     nudged = r0.copy()
     nudged[:, 0] *= 1 + 1e-12
@@ -528,7 +528,7 @@ def adjoint_tangent_check(A, LT, ctx, adj, r0, nturn, pick, pairs, elems, hk=1e-
     the whole run no longer converge.  Relative errors: dL/dr0 per particle, the largest
     |adjoint - tangent| over the coordinates over the largest |tangent|; the knobs, over the
     particles together, the largest |adjoint - tangent| over the largest |tangent|."""
-    ring = LT.config4_ring()
+    ring = LT.dba_4d_ring()
     line = A.Line(ctx, ring)
     kr = []
     for ea, eb in pairs:
@@ -913,13 +913,13 @@ def wake_leg(A, LT, ctx, nturn: int = 200, n: int = 1 << 20) -> dict:
     sigma_delta 1e-3, 10 nm / 10 pm).  The state stays on the device (SoA); timed with CUDA events
     on the launching stream after a warm-up, over `nturn` turns of the 10,000 the full run takes."""
     import torch
-    ring = LT.config2_ring()
+    ring = LT.dba_ring()
     m = A.Line(ctx, ring).m66()
     wring = ring + [LT.longwake_elem()]
     line = A.Line(ctx, wring)
     line.set_flags(rad=A.RAD_RADQE, cavity=1, wake=1)
     line.set_seed(2024)
-    r = LT.config5_particles(n, m, seed=5)
+    r = LT.matched_bunch_particles(n, m, seed=5)
     st = torch.tensor(np.ascontiguousarray(r.T), device="cuda", dtype=torch.float64).contiguous()
     s = torch.cuda.current_stream()
     line.track(st, 5, layout=A.LAYOUT_SOA, stream=s.cuda_stream)

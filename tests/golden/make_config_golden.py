@@ -10,10 +10,10 @@ oracle/_ref/libaccel_ref.so):
 Cases (every input is regenerated from its seed by accel-plus_b200/lattices.py):
   c1      the 32-cell FODO (fodo32.lat), 1,024 particles x uniform in +-5 mm, y in +-2 mm
           (default_rng(0)), 1,000 turns, radiation, cavity and wake off
-  c2      the 18-cell DBA with radiation and RF on (config2_ring), a 101 x 51 grid over x in
+  c2      the 18-cell DBA with radiation and RF on (dba_ring), a 101 x 51 grid over x in
           [-25, 25] mm, y in [0, 12] mm, 1,024 turns
   c3_<k>  error-seeded copy k of that DBA (error_copy(base, k)) on its full grid from
-          config3_sizes(256, 12345)[k], 1,000 turns; four copies spanning the grid-size range
+          copy_grid_sizes(256, 12345)[k], 1,000 turns; four copies spanning the grid-size range
 
 Each case is tracked by the reference's ALine::pass one turn at a time with the per-turn NaN
 scan of trackDA (aline.cpp:646-659), OpenMP over all host threads (bit-identical to one thread
@@ -185,15 +185,15 @@ def main():
 
     if not only or "c1" in only:
         print("c1: FODO, 1024 particles, 1000 turns", flush=True)
-        line = ref_line(LT.config1_ring(), rad=0, cavity=0)
-        store("c1", classify(line, LT.config1_particles(), 1000, threads))
+        line = ref_line(LT.fodo_ring(), rad=0, cavity=0)
+        store("c1", classify(line, LT.fodo_particles(), 1000, threads))
     if not only or "c2" in only:
         print("c2: DBA, 101 x 51 grid, 1024 turns", flush=True)
-        line = ref_line(LT.config2_ring(), rad=1, cavity=1)
+        line = ref_line(LT.dba_ring(), rad=1, cavity=1)
         store("c2", classify(line, LT.da_grid(101, 51), 1024, threads, shape=(101, 51)))
     if not only or "c3" in only:
-        sizes = LT.config3_sizes(256, 12345)
-        base = LT.config2_ring()
+        sizes = LT.copy_grid_sizes(256, 12345)
+        base = LT.dba_ring()
         picks = c3_copies(sizes)
         out["c3_copies"] = np.array(picks, dtype=np.int32)
         for k in picks:

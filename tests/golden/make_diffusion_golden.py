@@ -38,7 +38,7 @@ def main():
     LT = importlib.import_module("accel-plus_b200.lattices")
     fd, path = tempfile.mkstemp(suffix=".lat")
     os.close(fd)
-    A.write_lattice(path, LT.config4_ring())
+    A.write_lattice(path, LT.dba_4d_ring())
     line = O.RefLine(path)
     os.unlink(path)
     O.ref().ref_set_threads(1)

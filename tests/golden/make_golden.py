@@ -149,9 +149,9 @@ def main():
         line.track(r, 1)
         out[f"elem_{name}"] = r
 
-    # config 1: FODO, 64 of the 1024 config-1 particles, 1 and 100 turns; one-turn matrix
+    # the 32-cell FODO: 64 of its 1,024 uniform particles, 1 and 100 turns; one-turn matrix
     rf = O.RefLine(fodo)
-    p = LT.config1_particles()[:64].copy()
+    p = LT.fodo_particles()[:64].copy()
     out["fodo_in"] = p.copy()
     r1 = p.copy()
     rf.track(r1, 1)
@@ -163,7 +163,7 @@ def main():
     out["fodo_tune"] = np.array(rf.tune())
     out["fodo_chrom"] = np.array(rf.chrom())
 
-    # config 2: DBA, radiation + cavity on, a coarse DA grid with loss turns over 200 turns
+    # the 18-cell DBA, radiation + cavity on, a coarse DA grid with loss turns over 200 turns
     rd = O.RefLine(dba)
     rd.set_flags(rad=0, cavity=0)
     out["dba_m66"] = rd.m66()
@@ -179,8 +179,8 @@ def main():
     rp = O.RefLine(dba)
     out["dba_phis"] = np.array([rp.setrfphase()])  # on the committed (sextupole-corrected) ring
 
-    # config 3: two error-seeded copies (feed-down), small grids, 100 turns
-    base = LT.config2_ring()
+    # two error-seeded copies of the DBA (feed-down), small grids, 100 turns
+    base = LT.dba_ring()
     for k in (0, 1):
         ring = LT.error_copy(base, k)
         rr = ref_of(ring)

@@ -36,7 +36,7 @@ def main():
         recs.append(x)
         lows.append(0.0)
         his.append(0.5)
-    ring = LT.config1_ring()
+    ring = LT.fodo_ring()
     r = np.zeros((2, 6))
     r[:, 0] = [1e-3, 4e-3]
     r[:, 2] = [5e-4, 1e-3]

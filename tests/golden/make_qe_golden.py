@@ -89,9 +89,9 @@ def moments(r):
 def equilibrium(A, LT, path, batch=0):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
-    ring = LT.config2_ring()
+    ring = LT.dba_ring()
     m66 = entrance_m66(A, O, ring)
-    r0 = LT.config5_particles(PROCS * EQ_PER, m66, seed=EQ_SEED + batch)
+    r0 = LT.matched_bunch_particles(PROCS * EQ_PER, m66, seed=EQ_SEED + batch)
     jobs = [(2000 + 100 * batch + k, path, r0[k * EQ_PER:(k + 1) * EQ_PER].copy()) for k in range(PROCS)]
     with mp.get_context("spawn").Pool(PROCS) as pool:
         parts = pool.map(worker_eq, jobs)
@@ -113,7 +113,7 @@ def main():
     LT = importlib.import_module("accel-plus_b200.lattices")
     fd, path = tempfile.mkstemp(suffix=".lat")
     os.close(fd)
-    A.write_lattice(path, LT.config2_ring())
+    A.write_lattice(path, LT.dba_ring())
     if len(sys.argv) > 1 and sys.argv[1] == "equilibrium":
         equilibrium(A, LT, path, int(sys.argv[2]) if len(sys.argv) > 2 else 0)
         os.unlink(path)

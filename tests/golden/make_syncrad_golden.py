@@ -31,7 +31,7 @@ SYNCRAD_F = [3000.0, 0.9, 1.3, 1.0, 2e-9, 2e-11, 1e-3, 5.0, 3.0]
 
 def ring(A, LT):
     """The 4D DBA with the lumped radiation element at its end (radiation flag set by the caller)."""
-    return LT.config4_ring() + [A.elem(A.SYNCRAD, "SR", 0.2, f=SYNCRAD_F)]
+    return LT.dba_4d_ring() + [A.elem(A.SYNCRAD, "SR", 0.2, f=SYNCRAD_F)]
 
 
 def moments(r):

@@ -64,21 +64,21 @@ def ring_and_params(A, LT, ringname):
     elements with a corrector and a matrix (element kinds the tape takes on dual numbers, and a
     Quad K parameter)."""
     if ringname == "fodo":
-        ring, nturn, every = LT.config1_ring(), 24, 8
+        ring, nturn, every = LT.fodo_ring(), 24, 8
     elif ringname == "dba4d":
-        ring, nturn, every = LT.config4_ring(), 40, 16  # 40 = 2 x 16 + 8: a short last segment
+        ring, nturn, every = LT.dba_4d_ring(), 40, 16  # 40 = 2 x 16 + 8: a short last segment
     elif ringname == "dba6d":
-        ring, nturn, every = LT.config2_ring(), 40, 16
+        ring, nturn, every = LT.dba_ring(), 40, 16
         for d in ring:
             if d.type == A.BENDMPOLE:
                 d.flags = A.RAD_OFF
             if d.type == A.CAVITY:
                 d.f[2] = 0.0  # without radiation the synchronous phase is 0
     elif ringname == "dba4d_single":
-        ring, nturn, every = LT.config4_ring(), 40, 16
+        ring, nturn, every = LT.dba_4d_ring(), 40, 16
     else:  # "fodo_quad"
         ring, nturn, every = [], 24, 8
-        for d in LT.config1_ring():
+        for d in LT.fodo_ring():
             if d.type == A.STRMPOLE and d.poly_b[2] == 0 and d.poly_b[1] != 0 and d.len > 0:
                 ring.append(A.elem(A.QUAD, d.name, d.len, f=[d.poly_b[1]]))
             else:
@@ -176,12 +176,12 @@ def test_z_rows_taped_again_for_a_z_seed(A, ctx, LT):
     The gradient is linear in the seed across the two kinds of tape, the z-free gradient is the
     same bit for bit before and after the second taping, and the z part equals the one of the
     checkpointed path (tapes chunk by chunk in the reverse pass)."""
-    ring = LT.config4_ring()
+    ring = LT.dba_4d_ring()
     pairs = LT.sextupole_pairs(ring)
     elems = sorted({i for p in pairs for i in p})[:6]
     params = [(i, A.F_POLYNOMB, 2) for i in elems]
     n, nturn, every = 64, 64, 16
-    r0 = LT.config4_particles(n, seed=3)
+    r0 = LT.gaussian_4d_particles(n, seed=3)
     adj = A.Adjoint(A.Line(ctx, ring), n, nturn, every, params)
     rf = adj.forward(r0)
     assert not np.isnan(rf[:, 0]).any()
@@ -214,7 +214,7 @@ def test_z_rows_taped_again_for_a_z_seed(A, ctx, LT):
 def test_adjoint_one_turn_jacobian_is_exact(A, ctx, LT):
     """Six particles at the closed orbit (the origin of the 4D ring), seeded with unit adjoints:
     row i of the one-turn matrix is dL/dr0 of particle i for L = r_final[i]."""
-    ring = LT.config4_ring()
+    ring = LT.dba_4d_ring()
     line = A.Line(ctx, ring)
     r0 = np.zeros((6, 6))
     adj = A.Adjoint(line, 6, 1, 1, [])
@@ -227,13 +227,13 @@ def test_adjoint_one_turn_jacobian_is_exact(A, ctx, LT):
 
 
 def test_adjoint_rejects_radiation_and_bad_params(A, ctx, LT):
-    ring = LT.config2_ring()  # radiation on
+    ring = LT.dba_ring()  # radiation on
     line = A.Line(ctx, ring)
     with pytest.raises(A.AccelError) as ei:
         A.Adjoint(line, 4, 2, 1, [])
     assert ei.value.status == A.E_UNSUPPORTED
-    line4 = A.Line(ctx, LT.config4_ring())
-    drift = [i for i, d in enumerate(LT.config4_ring()) if d.type == A.DRIFT][0]
+    line4 = A.Line(ctx, LT.dba_4d_ring())
+    drift = [i for i, d in enumerate(LT.dba_4d_ring()) if d.type == A.DRIFT][0]
     with pytest.raises(A.AccelError) as ei:
         A.Adjoint(line4, 4, 2, 1, [(drift, A.F_POLYNOMB, 2)])
     assert ei.value.status == A.E_UNSUPPORTED
@@ -246,7 +246,7 @@ def test_handles_released_in_any_order(A, ctx, LT):
     L = A.lib()
     c = C.c_void_p()
     assert L.accel_ctx_create(0, C.byref(c)) == 0
-    ring = LT.config4_ring()
+    ring = LT.dba_4d_ring()
     arr = (A.ElemDesc * len(ring))(*ring)
     ln = C.c_void_p()
     assert L.accel_line_create(c, arr, len(ring), C.byref(ln)) == 0
@@ -269,7 +269,7 @@ def test_autograd_function_over_the_adjoint_pair(A, ctx, LT):
     on a torch expression of the tracked coordinates returns the adjoint's gradients with respect
     to the initial coordinates and the sextupole strengths."""
     torch = pytest.importorskip("torch")
-    ring = LT.config4_ring()
+    ring = LT.dba_4d_ring()
     sx = [i for i, d in enumerate(ring) if d.type == A.STRMPOLE and d.poly_b[2] != 0][:4]
     line = A.Line(ctx, ring)
     n, nturn = 64, 32
@@ -298,7 +298,7 @@ def test_autograd_function_over_the_adjoint_pair(A, ctx, LT):
     assert np.allclose(k2.grad.numpy(), dp, rtol=1e-14, atol=0)
 
 
-def test_config4_gradient_full_size(A, ctx, LT):
+def test_gradient_4096_particles_512_turns(A, ctx, LT):
     """The gradient at the stated size: 4,096 Gaussian particles (seed 1) through 512 turns of the
     4D DBA, checkpoints every 64 turns, with respect to every particle's initial coordinates and
     the 36 sextupole knobs (the 72 sextupoles in mirror pairs).
@@ -317,13 +317,13 @@ def test_config4_gradient_full_size(A, ctx, LT):
     differences of the fused maps grow with the orbit's sensitivity; measured below 7e-11 x
     growth), the knob gradients of the 16 within 1e-6 (measured 5e-8)."""
     import bench
-    ring = LT.config4_ring()
+    ring = LT.dba_4d_ring()
     line = A.Line(ctx, ring)
     pairs = LT.sextupole_pairs(ring)
     assert len(pairs) == 36
     elems = sorted({i for p in pairs for i in p})
     params = [(i, A.F_POLYNOMB, 2) for i in elems]
-    r0 = LT.config4_particles(4096, seed=1)
+    r0 = LT.gaussian_4d_particles(4096, seed=1)
     adj = A.Adjoint(line, 4096, 512, 64, params)
     rf = adj.forward(r0)
     assert not np.isnan(rf[:, 0]).any()

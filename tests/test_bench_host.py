@@ -24,7 +24,7 @@ def test_error_copy_text_equals_library_writer(A, LT, seed):
     fd, path = tempfile.mkstemp(suffix=".lat")
     os.close(fd)
     try:
-        A.write_lattice(path, LT.error_copy(LT.config2_ring(), seed))
+        A.write_lattice(path, LT.error_copy(LT.dba_ring(), seed))
         with open(path) as f:
             want = f.read()
     finally:

@@ -26,7 +26,7 @@ def test_status_strings(A):
 
 
 def test_lattice_roundtrip_bit_exact(A, LT, tmp_path):
-    for ring in (LT.config1_ring(), LT.config2_ring()):
+    for ring in (LT.fodo_ring(), LT.dba_ring()):
         p = str(tmp_path / "x.lat")
         A.write_lattice(p, ring)
         back = A.read_lattice(p)
@@ -201,7 +201,7 @@ def test_no_device_is_an_error_not_a_fallback(A):
 def test_model_flops_match_cost_formula(A, LT):
     """The flop model (StrMPole slice 52 + 3(8m + 4), BendMPole slice 4*46 + 3(44 + 7m), drift
     14) on the 32-cell FODO: 32 x [2 quads (m=1) + 2 sextupoles (m=2) + 2 bends (m=0) + 4 drifts]."""
-    ring = LT.config1_ring()
+    ring = LT.fodo_ring()
     per_cell = 2 * 10 * (52 + 3 * 12) + 2 * 10 * (52 + 3 * 20) + 2 * (10 * (184 + 3 * 44) + 8) + 4 * 14
     assert LT.flops_per_turn(ring) == 32 * per_cell
 

@@ -24,9 +24,9 @@ Bars, for every mode:
       keep the reference's operation order;
   the aperture code of each particle lost in the reference's turn equal to the reference's (the
       fused mode: except on at most 1 % of them, each an orbit already sensitive before its loss;
-      one of 614 on the config-2 grid, a particle whose y at the aperture is 62 mm in the
+      one of 614 on the DBA's 101 x 51 grid, a particle whose y at the aperture is 62 mm in the
       reference and 39 mm in the fused run after a last turn that took px to 0.19).
-Measured on the full config-2 grid: the largest error / amp is 19 (fused) and 3.8 (plain,
+Measured on the DBA's full 101 x 51 grid: the largest error / amp is 19 (fused) and 3.8 (plain,
 exact) over 2,056 survivors of certain fate, and the regular survivors are within 3.3e-10.
 The DA area (trackDA's triangle fan, aline.cpp:689-708, over each grid column's first lost point)
 is not held to a bar: at 1,000 turns it rests on chaotic points, and the reference's own runs
@@ -100,22 +100,22 @@ def check_case(c, r, lt, mode, bit_exact=False):
 
 
 @pytest.mark.parametrize("mode", ["fused", "plain", "exact"])
-def test_config1_full_size(A, ctx, LT, CG, mode):
+def test_fodo_1024_particles_1000_turns(A, ctx, LT, CG, mode):
     """The FODO, 1,024 particles, 1,000 turns: no transcendental on the path, so the plain and
     exact modes equal the reference bit for bit; the fused mode is within 1e-9."""
     c = case(CG, "c1")
-    line = A.Line(ctx, LT.config1_ring())
-    r = LT.config1_particles()
+    line = A.Line(ctx, LT.fodo_ring())
+    r = LT.fodo_particles()
     lt = np.empty(len(r), dtype=np.int32)
     line.track(r, 1000, loss=lt, mode=MODES[mode])
     check_case(c, r, lt, mode, bit_exact=mode != "fused")
 
 
 @pytest.mark.parametrize("mode", ["fused", "plain", "exact"])
-def test_config2_full_grid(A, ctx, LT, CG, mode):
+def test_dba_101x51_grid_1024_turns(A, ctx, LT, CG, mode):
     """The DBA with radiation and RF, its full 101 x 51 DA grid for 1,024 turns."""
     c = case(CG, "c2")
-    line = A.Line(ctx, LT.config2_ring())
+    line = A.Line(ctx, LT.dba_ring())
     r = LT.da_grid(101, 51)
     lt = np.empty(len(r), dtype=np.int32)
     line.track(r, 1024, loss=lt, mode=MODES[mode])
@@ -123,12 +123,12 @@ def test_config2_full_grid(A, ctx, LT, CG, mode):
 
 
 @pytest.mark.parametrize("mode", ["fused", "plain", "exact"])
-def test_config3_copies_full_grids(A, ctx, LT, CG, mode):
+def test_error_copies_full_grids_1000_turns(A, ctx, LT, CG, mode):
     """Four error-seeded copies of the batched workload on their full grids, tracked together in
     one batched call with host arrays (staged inside the call) for 1,000 turns."""
     picks = [int(k) for k in CG["c3_copies"]]
-    sizes = LT.config3_sizes(256, 12345)
-    base = LT.config2_ring()
+    sizes = LT.copy_grid_sizes(256, 12345)
+    base = LT.dba_ring()
     lines = [A.Line(ctx, LT.error_copy(base, k)) for k in picks]
     grids = [LT.da_grid(*sizes[k]) for k in picks]
     off = np.zeros(len(picks) + 1, dtype=np.int64)

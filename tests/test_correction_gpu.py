@@ -39,7 +39,7 @@ def exact_chrom(line):
 
 @pytest.mark.parametrize("fam,order", [("QF1", 1), ("SF", 2), ("SD", 2)])
 def test_knob_derivative_matches_differences(A, ctx, LT, fam, order):
-    ring = LT.config4_ring()
+    ring = LT.dba_4d_ring()
     idx = family(ring, A, fam)
     knob = [(i, A.F_POLYNOMB, order) for i in idx]
     line = A.Line(ctx, ring)
@@ -90,7 +90,7 @@ def _with_coeffs(ring, A, coeffs, order):
 
 
 def test_tune_correction_newton_against_reference_fit(A, ctx, LT, O):
-    ring = LT.config4_ring()
+    ring = LT.dba_4d_ring()
     target = (0.19, 0.36)
     line = A.Line(ctx, ring)
     tx, ty, it = line.correct_tune(family(ring, A, "QF1"), family(ring, A, "QD1"), *target, method=0)
@@ -110,7 +110,7 @@ def test_tune_correction_newton_against_reference_fit(A, ctx, LT, O):
 
 
 def test_chrom_correction_newton_against_reference_fit(A, ctx, LT, O):
-    ring = LT.config4_ring()
+    ring = LT.dba_4d_ring()
     target = (1.0, 1.5)
     line = A.Line(ctx, ring)
     cx, cy, it = line.correct_chrom(family(ring, A, "SF"), family(ring, A, "SD"), *target, method=0)

@@ -30,7 +30,7 @@ def DG():
 
 
 def test_track_diffusion_against_reference(A, ctx, LT, DG):
-    line = A.Line(ctx, LT.config4_ring())
+    line = A.Line(ctx, LT.dba_4d_ring())
     nturn = int(DG["nturn"][0])
     nux, nuy, dif, tot = line.track_diffusion(nturn, DG["x0"], DG["y0"], mode=A.MODE_EXACT)
     lost_ref = np.isnan(DG["dif"])
@@ -57,7 +57,7 @@ def test_track_diffusion_against_reference(A, ctx, LT, DG):
 
 
 def test_track_tune_against_reference(A, ctx, LT, DG):
-    line = A.Line(ctx, LT.config4_ring())
+    line = A.Line(ctx, LT.dba_4d_ring())
     nturn = int(DG["nturn"][0])
     for (x, y), (tx, ty) in zip(DG["tune_pts"], DG["tunes"]):
         gx, gy = line.track_tune(nturn, float(x), float(y), mode=A.MODE_EXACT)

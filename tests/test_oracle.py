@@ -31,7 +31,7 @@ def test_port_elements_match_golden(A, O, G, MG):
 
 
 def test_port_fodo_matches_golden(O, G, LT):
-    ring = LT.config1_ring()
+    ring = LT.fodo_ring()
     for turns, key in ((1, "fodo_t1"), (100, "fodo_t100")):
         r = G["fodo_in"].copy()
         O.port_track(ring, r, turns, loss=False)
@@ -41,7 +41,7 @@ def test_port_fodo_matches_golden(O, G, LT):
 
 def test_port_openmp_blocks_bit_identical(O, G, LT):
     """ALine::pass splits particles into per-thread blocks; results do not depend on it."""
-    ring = LT.config1_ring()
+    ring = LT.fodo_ring()
     r1 = G["fodo_in"].copy()
     r8 = G["fodo_in"].copy()
     O.port_track(ring, r1, 20, loss=False, nthreads=1)
@@ -50,7 +50,7 @@ def test_port_openmp_blocks_bit_identical(O, G, LT):
 
 
 def test_port_dba_loss_turns_match_golden(O, G, LT):
-    ring = LT.config2_ring()
+    ring = LT.dba_ring()
     r = G["dba_grid_in"].copy()
     lt = O.port_track(ring, r, 200)
     assert np.array_equal(lt, G["dba_grid_loss"])
@@ -59,7 +59,7 @@ def test_port_dba_loss_turns_match_golden(O, G, LT):
 
 
 def test_port_error_copies_match_golden(O, G, LT):
-    base = LT.config2_ring()
+    base = LT.dba_ring()
     for k in (0, 1):
         ring = LT.error_copy(base, k)
         r = G[f"c3_{k}_in"].copy()
@@ -69,7 +69,7 @@ def test_port_error_copies_match_golden(O, G, LT):
 
 
 def test_port_m66_dba(O, G, LT):
-    ring = LT.config2_ring()
+    ring = LT.dba_ring()
     O.port_set_flags(ring, rad=0, cavity=0)
     assert same_bits(O.port_m66(ring), G["dba_m66"])
     O.port_set_flags(ring, rad=1, cavity=1)

@@ -43,7 +43,7 @@ def test_full_batched_job_equals_copies_tracked_alone(A, ctx):
 
 
 def test_edge_cases(A, ctx, LT):
-    line = A.Line(ctx, LT.config2_ring())
+    line = A.Line(ctx, LT.dba_ring())
     rng = np.random.default_rng(4)
     r0 = np.zeros((64, 6))
     r0[:, 0] = rng.uniform(-0.02, 0.02, 64)

@@ -29,7 +29,7 @@ def moments(r):
 def test_quantum_excitation_statistics(A, ctx, LT):
     ref = np.load(os.path.join(GOLDEN, "qe_moments.npz"))
     n_ref, turns = int(ref["n"][0]), int(ref["turns"][0])
-    line = A.Line(ctx, LT.config2_ring())
+    line = A.Line(ctx, LT.dba_ring())
     line.set_flags(rad=A.RAD_RADQE, cavity=1)
     line.set_seed(20240611)
     n = 262144
@@ -54,7 +54,7 @@ def test_quantum_excitation_statistics(A, ctx, LT):
 
 def test_quantum_excitation_is_reproducible_and_seeded(A, ctx, LT):
     """Counter-based deviates: the same seed gives the same bits, another seed other bits."""
-    line = A.Line(ctx, LT.config2_ring())
+    line = A.Line(ctx, LT.dba_ring())
     line.set_flags(rad=A.RAD_RADQE, cavity=1)
     runs = []
     for seed in (7, 7, 8):
@@ -105,8 +105,8 @@ def test_quantum_excitation_equilibrium(A, ctx, LT):
     turns = files[0]["turns"]
     ref, n_ref = pooled(files, len(turns) - 1)
     n = 131072
-    r = LT.config5_particles(n, files[0]["m66"], seed=777)
-    line = A.Line(ctx, LT.config2_ring())
+    r = LT.matched_bunch_particles(n, files[0]["m66"], seed=777)
+    line = A.Line(ctx, LT.dba_ring())
     line.set_flags(rad=A.RAD_RADQE, cavity=1)
     line.set_seed(97531)
     line.track(r, int(turns[-1]))

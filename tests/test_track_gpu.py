@@ -58,7 +58,7 @@ def test_elements_against_reference(A, ctx, G, MG, mode):
 
 @pytest.mark.parametrize("mode", ["plain", "exact"])
 def test_plain_fodo_bit_exact(A, ctx, G, LT, mode):
-    line = A.Line(ctx, LT.config1_ring())
+    line = A.Line(ctx, LT.fodo_ring())
     for turns, key in ((1, "fodo_t1"), (100, "fodo_t100")):
         r = G["fodo_in"].copy()
         line.track(r, turns, mode=MODES[mode])
@@ -88,7 +88,7 @@ def test_exact_mode_is_the_plain_kernel_bit_for_bit(A, ctx, G, LT):
     radiation and RF (the DA grid of the DBA, 200 turns, particles lost all along), with quantum
     excitation (the same counter-based normals), over error-seeded copies in one batch, and on a
     line whose longitudinal wake splits every turn into ranges."""
-    base = LT.config2_ring()
+    base = LT.dba_ring()
     # radiation + RF, losses
     line = A.Line(ctx, base)
     g = G["dba_grid_in"]
@@ -97,7 +97,7 @@ def test_exact_mode_is_the_plain_kernel_bit_for_bit(A, ctx, G, LT):
     # quantum excitation
     qline = A.Line(ctx, base)
     qline.set_flags(rad=A.RAD_RADQE)
-    r0 = LT.config5_particles(2048, line.m66(), seed=3)
+    r0 = LT.matched_bunch_particles(2048, line.m66(), seed=3)
     (rp, lp), (re, le) = _exact_vs_plain(A, [qline], np.array([0, 2048]), r0, 40)
     assert same_bits(re, rp) and np.array_equal(le, lp)
     # error copies, one batch
@@ -115,7 +115,7 @@ def test_exact_mode_is_the_plain_kernel_bit_for_bit(A, ctx, G, LT):
 
 
 def test_fused_fodo_tolerance(A, ctx, G, LT):
-    line = A.Line(ctx, LT.config1_ring())
+    line = A.Line(ctx, LT.fodo_ring())
     r = G["fodo_in"].copy()
     line.track(r, 1)
     assert rel_err(r, G["fodo_t1"]) < 1e-12
@@ -124,10 +124,10 @@ def test_fused_fodo_tolerance(A, ctx, G, LT):
     assert rel_err(r, G["fodo_t100"]) < 1e-10
 
 
-def test_fused_config1_1000_turns(A, ctx, O, LT):
-    """Config 1 (FODO, uniform x in +-5 mm, y in +-2 mm), 1,000 turns: fused GPU vs the oracle."""
-    ring = LT.config1_ring()
-    p = LT.config1_particles()[:256].copy()
+def test_fused_fodo_1000_turns(A, ctx, O, LT):
+    """The 32-cell FODO (uniform x in +-5 mm, y in +-2 mm), 1,000 turns: fused GPU vs the oracle."""
+    ring = LT.fodo_ring()
+    p = LT.fodo_particles()[:256].copy()
     ref = p.copy()
     lt_ref = O.port_track(ring, ref, 1000, nthreads=8)
     line = A.Line(ctx, ring)
@@ -140,9 +140,9 @@ def test_fused_config1_1000_turns(A, ctx, O, LT):
 
 @pytest.mark.parametrize("mode", ["plain", "fused"])
 def test_dba_grid_loss_turns(A, ctx, O, G, LT, mode):
-    """Config 2 ring (radiation + cavity on): loss turns of a DA grid against the reference."""
+    """The 18-cell DBA (radiation + cavity on): loss turns of a DA grid against the reference."""
     m = A.MODE_PLAIN if mode == "plain" else A.MODE_FUSED
-    ring = LT.config2_ring()
+    ring = LT.dba_ring()
     sv = Sensitivity(O, ring, G["dba_grid_in"], 200, 13, 7)
     ref_lt = sv.lt
     assert np.array_equal(ref_lt, G["dba_grid_loss"])  # the oracle is the reference here
@@ -163,10 +163,10 @@ def test_dba_grid_loss_turns(A, ctx, O, G, LT, mode):
 
 @pytest.mark.parametrize("mode", ["plain", "fused"])
 def test_batched_error_copies(A, ctx, O, G, LT, mode):
-    """Config-3 style: error-seeded copies with uneven grids tracked in one batched launch."""
+    """Error-seeded copies of the DBA with uneven grids tracked in one batched launch."""
     import torch
     m = A.MODE_PLAIN if mode == "plain" else A.MODE_FUSED
-    base = LT.config2_ring()
+    base = LT.dba_ring()
     rings = [LT.error_copy(base, k) for k in (0, 1, 7)]
     shapes = [(9, 5), (9, 5), (7, 3)]
     grids = [G["c3_0_in"], G["c3_1_in"], LT.da_grid(7, 3)]
@@ -192,7 +192,7 @@ def test_batched_error_copies(A, ctx, O, G, LT, mode):
 
 
 def test_m66_fd_matches_getm66_and_exact_is_close(A, ctx, G, LT):
-    line = A.Line(ctx, LT.config1_ring())
+    line = A.Line(ctx, LT.fodo_ring())
     fd = line.m66(method=1, delta=1e-8)
     assert same_bits(fd, G["fodo_m66"])  # the FD path is the reference's getm66 on the GPU
     ex = line.m66(method=0)
@@ -214,7 +214,7 @@ def test_setrfphase_matches_reference(A, ctx, G, LT):
 def test_range_pass_and_layouts(A, ctx, O, G, LT):
     """pass(r, N, st, ed) on a sub-range, AoS and SoA, host and device pointers."""
     import torch
-    ring = LT.config1_ring()
+    ring = LT.fodo_ring()
     line = A.Line(ctx, ring)
     p = G["fodo_in"].copy()
     ref = p.copy()
@@ -236,7 +236,7 @@ def test_range_pass_other_modes(A, ctx, O, G, LT, mode):
     """pass(r, N, st, ed) in the fused and exact modes: a sub-range against the reference's
     pass_line (1e-12 fused, bit for bit exact), and a turn tracked as two ranges equal to the
     turn in one call (each element's arithmetic does not depend on where a call starts)."""
-    ring = LT.config1_ring()
+    ring = LT.fodo_ring()
     line = A.Line(ctx, ring)
     p = G["fodo_in"].copy()
     ref = p.copy()
@@ -324,10 +324,10 @@ def test_transverse_wake_ring_fused_matches_plain(A, ctx, LT):
     z-sorted prefix sums, the order in z changing from turn to turn) against the plain mode (the
     reference's operation order and pair sum) at the 1000-turn regular-orbit tolerance; and the
     wake does act (the same ring without it ends elsewhere)."""
-    ring = LT.config4_ring()
+    ring = LT.dba_4d_ring()
     m = A.Line(ctx, ring).m66()
     tw = A.elem(A.TRANSWAKE, "TW", 0.0, f=[3000, 2.0, 5000.0, 10.0, 1.5, 4000.0, 12.0, 2.0], flags=1)
-    r0 = LT.config5_particles(2048, m, seed=9)
+    r0 = LT.matched_bunch_particles(2048, m, seed=9)
     line = A.Line(ctx, ring + [tw])
     a, b, c = r0.copy(), r0.copy(), r0.copy()
     line.track(a, 100, mode=A.MODE_PLAIN)
@@ -358,9 +358,9 @@ def test_device_memory_limit_fails_cleanly(A, LT):
     r0[:, 0] = rng.uniform(-2e-3, 2e-3, 3000)
     r0[:, 2] = rng.uniform(-1e-3, 1e-3, 3000)
     ref = r0.copy()
-    A.Line(A.Context(0), LT.config1_ring()).track(ref, 20)
+    A.Line(A.Context(0), LT.fodo_ring()).track(ref, 20)
     c2 = A.Context(0)
-    line = A.Line(c2, LT.config1_ring())
+    line = A.Line(c2, LT.fodo_ring())
     held = A.device_memory_held()
     try:
         A.set_device_memory_limit(held)  # no new buffer fits
@@ -381,7 +381,7 @@ def test_device_memory_limit_fails_cleanly(A, LT):
 
 def test_autotune_and_launch_count(A, ctx, LT):
     import torch
-    base = LT.config2_ring()
+    base = LT.dba_ring()
     rings = [LT.error_copy(base, k) for k in range(3)]
     grids = [LT.da_grid(11, 5), LT.da_grid(13, 7), LT.da_grid(9, 9)]
     lines = [A.Line(ctx, r) for r in rings]
@@ -463,7 +463,7 @@ def test_staged_wait_that_runs_out_is_a_status(A, ctx, LT):
     ACCEL_E_TIMEOUT instead of results.  The context stays usable: with the default limit the
     next call tracks as the default schedule does, bit for bit."""
     import torch
-    base = LT.config2_ring()
+    base = LT.dba_ring()
     lines = [A.Line(ctx, LT.error_copy(base, k)) for k in (0, 1)]
     grids = [LT.da_grid(11, 5), LT.da_grid(9, 7)]
     off = np.zeros(3, dtype=np.int64)
@@ -501,7 +501,7 @@ def test_staged_schedule_equals_fused(A, ctx, LT, variant):
     loss turns bit for bit as the default schedule, including at tasks that straddle two
     instances (their lanes read the other instance's records from global memory)."""
     import torch
-    base = LT.config2_ring()
+    base = LT.dba_ring()
     rings = [LT.error_copy(base, k) for k in (0, 1, 7, 9)]
     lines = [A.Line(ctx, r) for r in rings]
     for l in lines:

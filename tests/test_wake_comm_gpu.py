@@ -16,7 +16,7 @@ pytestmark = pytest.mark.gpu
 
 
 def ring_with_wake(A, LT):
-    ring = LT.config2_ring()
+    ring = LT.dba_ring()
     return ring[:-1] + [LT.longwake_elem()] + ring[-1:]  # wake before the aperture
 
 
@@ -45,7 +45,7 @@ def test_one_rank_exchange_reproduces_local_wake(A, LT):
     assert np.array_equal(a, b, equal_nan=True)
     # the wake did act: the same ring without it ends elsewhere
     ctx = A.Context(0)
-    line = A.Line(ctx, LT.config2_ring())
+    line = A.Line(ctx, LT.dba_ring())
     c = r0.copy()
     line.track(c, 30)
     assert not np.array_equal(a, c, equal_nan=True)
