@@ -8,7 +8,7 @@ import os
 import numpy as np
 import pytest
 
-from conftest import same_bits
+from conftest import GOLDEN, same_bits
 
 
 def _flags(O, A, name, elems):
@@ -150,3 +150,24 @@ def test_naff_matches_reference(A):
     g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "naff.npz"))
     for x, lo, hi, nu in zip(g["records"], g["xlow"], g["xhi"], g["nu"]):
         assert abs(A.naff(x, lo, hi) - nu) <= 1e-8 * abs(nu), (A.naff(x, lo, hi), nu)
+
+
+def test_port_reproduces_full_size_fixture_subset(O, LT):
+    """The reference outputs committed for the full-size parity tests (config_golden.npz, made by
+    the reference library) against the C restatement on a subset of the same particles: the
+    FODO's first 256 particles and the whole grid of the smallest error-seeded DBA copy (24 x 11,
+    radiation and cavity on), 1,000 turns each: loss turns equal and final coordinates bit for
+    bit."""
+    cg = np.load(os.path.join(GOLDEN, "config_golden.npz"))
+    threads = os.cpu_count() or 1
+    r = LT.fodo_particles()[:256].copy()
+    lt = O.port_track(LT.fodo_ring(), r, 1000, nthreads=threads)
+    assert np.array_equal(lt, cg["c1_loss"][:256])
+    assert same_bits(r, cg["c1_out"][:256])
+    k = int(cg["c3_copies"][0])
+    nx, ny = (int(v) for v in cg[f"c3_{k}_shape"])
+    assert nx * ny == 264
+    r = LT.da_grid(nx, ny)
+    lt = O.port_track(LT.error_copy(LT.dba_ring(), k), r, 1000, nthreads=threads)
+    assert np.array_equal(lt, cg[f"c3_{k}_loss"])
+    assert same_bits(r, cg[f"c3_{k}_out"])
