@@ -52,6 +52,9 @@ def parse():
                     help="only the adjoint leg, printed as its own JSON line (profiling runs)")
     ap.add_argument("--no-fd-check", action="store_true",
                     help="skip the adjoint's finite-difference check (profiling runs)")
+    ap.add_argument("--adjoint-turns", type=int, default=512,
+                    help="turns of the adjoint leg (fewer: a small case for profiling; the tapes "
+                         "take about 100 MB per turn)")
     ap.add_argument("--wake-only", action="store_true",
                     help="time the bunch workload with its per-turn wake (2^20 particles) and exit")
     ap.add_argument("--wake-turns", type=int, default=200)
@@ -273,8 +276,8 @@ def config_dict(args, off, aos):
             "seeds": "copy k of rank r: error seed r*copies+k; grid sizes default_rng(12345+r)"}
 
 
-def adjoint_leg(A, LT, ctx, steps: int = 3, ranks=None, check: bool = True) -> dict:
-    """Gradient of L = sum over particles of (x^2 + y^2) after 512 turns of the 4D DBA (no cavity,
+def adjoint_leg(A, LT, ctx, steps: int = 3, ranks=None, check: bool = True, nturn: int = 512) -> dict:
+    """Gradient of L = sum over particles of (x^2 + y^2) after nturn (512) turns of the 4D DBA (no cavity,
     radiation off), 4,096 Gaussian particles (seed 1), with respect to the 6 x 4,096 initial
     coordinates and the 36 sextupole knobs (mirror pairs of the 72 sextupoles), checkpointed every
     64 turns.  Under torchrun each rank takes its own 4,096 particles (seed 1 + rank) and the knob
@@ -290,7 +293,7 @@ def adjoint_leg(A, LT, ctx, steps: int = 3, ranks=None, check: bool = True) -> d
     pairs = LT.sextupole_pairs(ring)
     elems = sorted({i for p in pairs for i in p})
     params = [(i, A.F_POLYNOMB, 2) for i in elems]
-    n, nturn, every = 4096, 512, 64
+    n, every = 4096, 64
     rank = ranks.rank if ranks else 0
     r0 = LT.gaussian_4d_particles(n, seed=1 + rank)
     adj = A.Adjoint(line, n, nturn, every, params)
@@ -354,7 +357,7 @@ def adjoint_leg(A, LT, ctx, steps: int = 3, ranks=None, check: bool = True) -> d
     naive, batched = 2 * n_in, 2 * (6 + len(pairs))
     adj.close()
     line.close()
-    return {"workload": "4D DBA, 4096 particles, 512 turns, checkpoints every 64, 36 sextupole knobs",
+    return {"workload": f"4D DBA, 4096 particles, {nturn} turns, checkpoints every 64, 36 sextupole knobs",
             "gradients_per_s": 1.0 / t_adj, "gradient_components_per_s": n_in / t_adj,
             "ms_per_gradient": 1e3 * t_adj, "ms_forward": 1e3 * t_fwd, "ms_backward": 1e3 * (t_adj - t_fwd),
             "ms_forward_alone": 1e3 * t_fwd_alone,
@@ -871,7 +874,7 @@ def engine_arm(args):
 
     adjoint = None
     if not args.no_adjoint:
-        adjoint = adjoint_leg(A, LT, ctx, ranks=ranks, check=not args.no_fd_check)
+        adjoint = adjoint_leg(A, LT, ctx, ranks=ranks, check=not args.no_fd_check, nturn=args.adjoint_turns)
 
     # the collective workloads: a 2^20-particle bunch with its per-turn longitudinal wake, and the
     # transverse wake's sorted sum against the pair sum (each rank on its own GPU)
@@ -1005,18 +1008,18 @@ def wake_only(turns: int, variant: int = -1):
     ctx.close()
 
 
-def adjoint_only(check: bool = True):
+def adjoint_only(check: bool = True, nturn: int = 512):
     A = importlib.import_module("accel-plus_b200")
     LT = importlib.import_module("accel-plus_b200.lattices")
     ctx = A.Context(0)
-    print(json.dumps({"adjoint": adjoint_leg(A, LT, ctx, check=check)}), flush=True)
+    print(json.dumps({"adjoint": adjoint_leg(A, LT, ctx, check=check, nturn=nturn)}), flush=True)
     ctx.close()
 
 
 def main():
     args = parse()
     if args.adjoint_only:
-        adjoint_only(check=not args.no_fd_check)
+        adjoint_only(check=not args.no_fd_check, nturn=args.adjoint_turns)
         return
     if args.wake_only:
         wake_only(args.wake_turns, args.variant)
